@@ -1,0 +1,14 @@
+"""Shared pytest configuration: the ``gpu`` marker and import paths."""
+
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for sub in ("", "pencil-rs_b200", "oracle"):
+    path = os.path.join(ROOT, sub) if sub else ROOT
+    if path not in sys.path:
+        sys.path.insert(0, path)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
