@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Headline benchmark: 512^3 R2C f32 forward + normalised inverse on a 4x8
+virtual pencil grid with the pencil transposes fused into the FFT passes.
+
+One step = R2cPlan.forward then R2cPlan.inverse over the whole field, inputs
+resident in HBM.  value = algorithmic HBM bytes of all steps on all GPUs /
+max-over-ranks device time (GB/s); ms_per_step is the forward+inverse time.
+Each GPU runs its own full transform (replicas; the on-device virtual ranks
+need no inter-GPU exchange).  ``--impl reference`` times the CPU oracle port
+of the reference algorithm instead (rank 0 only).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pencil-rs_b200"))
+
+METRIC = "512³ R2C fwd+inv ms & HBM GB/s (% peak); ragged batch vs per-grid, same accuracy"
+SHAPE = (512, 512, 512)
+GRID = (4, 8)
+CPU_SAMPLE_SHAPE = (512, 512, 64)
+
+
+def algorithmic_bytes(shape, real_bytes=4):
+    """Pass model per direction: the R2C pass reads the real field and writes
+    the half spectrum; each C2C pass reads and writes the half spectrum."""
+    n_real = 1
+    for s in shape:
+        n_real *= s
+    n_cplx = n_real // shape[-1] * (shape[-1] // 2 + 1)
+    r2c = n_real * real_bytes + n_cplx * 2 * real_bytes
+    c2c = 2 * n_cplx * 2 * real_bytes
+    per_pass = [r2c] + [c2c] * (len(shape) - 1)
+    return 2 * sum(per_pass), per_pass
+
+
+def flops(shape):
+    n = 1
+    for s in shape:
+        n *= s
+    return 2 * 5 * n * math.log2(n)  # 5 N log2 N per direction, forward + inverse
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(device_id)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if sm:
+            sm.sort()
+            out.update(sm_mhz=sm[len(sm) // 2], sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+def cpu_baseline(steps=1, warmup=0, sample=CPU_SAMPLE_SHAPE):
+    """The oracle port (numpy/scipy restatement of the reference algorithm:
+    per-rank local line FFTs + segment-layout pack / Alltoallv / unpack) on the
+    host cores, on a bounded sample of the workload."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pencil_oracle as po
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    po.set_workers(cores)
+    topo = po.Topology(GRID)
+    route = po.r2c_route(topo, sample)
+    x = np.random.default_rng(1).uniform(-1.0, 1.0, sample).astype(np.float32)
+    locs = po.scatter(route.input_pencil, x[None], (1,))
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        spec = po.execute_forward(route, locs)
+        po.execute_reverse(route, spec, True, np.float32)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    t = sorted(times)[len(times) // 2]
+    bytes_, _ = algorithmic_bytes(sample)
+    return {"value": bytes_ / t / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": f"R2C f32 {list(sample)} forward+inverse on the {GRID[0]}x{GRID[1]} virtual grid "
+                      f"(1/8 of the 512^3 field), median of {len(times)}; {t * 1e3:.1f} ms per forward+inverse"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    base = cpu_baseline(steps=args.steps, warmup=args.warmup)
+    bytes_, _ = algorithmic_bytes(CPU_SAMPLE_SHAPE)
+    ms = bytes_ / (base["value"] * 1e9) * 1e3
+    line = {"metric": METRIC, "value": base["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic: uniform(-1,1), numpy default_rng(1)",
+            "impl": "reference",
+            "config": {"workload": f"R2C f32 {list(CPU_SAMPLE_SHAPE)} forward+inverse, {GRID[0]}x{GRID[1]} "
+                                   "virtual ranks (bounded sample of the 512^3 workload)",
+                       "grid": list(GRID), "shape": list(CPU_SAMPLE_SHAPE)},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def b200_arm(args):
+    import torch
+    import pencil_b200 as pb
+    from pencil_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    shape = tuple(args.shape)
+    topo = pb.MpiTopology(GRID)
+    plan = pb.R2cPlan.from_shape(topo, shape, (), dtype=torch.float32)
+    ws = plan.allocate_workspace(dev)
+    # field A: uniform(-1,1) from numpy default_rng(1), global layout -> input layout
+    import numpy as np
+    rng = np.random.default_rng(1)
+    xa_host = rng.uniform(-1.0, 1.0, shape).astype(np.float32)
+    x = plan.input_pencil.scatter(torch.from_numpy(xa_host).to(dev)).contiguous()
+    spec = plan.allocate_output(dev)
+    back = plan.allocate_input(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = pb.plans._stream_ptr(stream)
+    lib = L.load()
+    hx, hs, hb, hw = (pb.plans._ptr(t) for t in (x, spec, back, ws))
+
+    def step():
+        L.check(lib.pb_execute(plan._h, L.FORWARD, hx, hs, hw, sp), "forward")
+        L.check(lib.pb_execute(plan._h, L.INVERSE, hs, hb, hw, sp), "inverse")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    L.check(lib.pb_execute_status(plan._h, hw, sp), "spectrum")
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms)
+    bytes_step, per_pass = algorithmic_bytes(shape)
+    value = bytes_step * world / (ms * 1e-3) / 1e9
+
+    # per-launch device times of the same steps (roofline of the pass kernel)
+    fwd_t, inv_t = [], []
+    for _ in range(max(3, min(args.steps, 10))):
+        fwd_t.append(plan.execute_timed(L.FORWARD, x, spec, ws, stream))
+        inv_t.append(plan.execute_timed(L.INVERSE, spec, back, ws, stream))
+    n_fwd = len(fwd_t[0])
+    n_inv = len(inv_t[0])  # passes plus one spectrum check
+    pass_ms = sum(sum(t) for t in fwd_t) + sum(sum(t[1:]) for t in inv_t)
+    pass_bytes = len(fwd_t) * sum(per_pass) * 2
+    launches = len(fwd_t) * (n_fwd + n_inv - 1)
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    check_ms = sum(t[0] for t in inv_t) / len(inv_t)
+
+    # accuracy: round trip of field A and the known spectrum of field B
+    L.check(lib.pb_execute_status(plan._h, hw, sp), "spectrum")
+    lg = math.log2(shape[0] * shape[1] * shape[2])
+    rt = float(torch.linalg.vector_norm((back - x).double()) / torch.linalg.vector_norm(x.double()))
+    kvec = torch.from_numpy(rng.integers(0, shape[0] // 2, size=(16, 3))).to(dev)
+    phase = torch.from_numpy(rng.uniform(0.0, 2 * math.pi, 16)).to(dev)
+    axes = [torch.arange(n, device=dev, dtype=torch.float64) for n in shape]
+    fb = torch.zeros(shape, dtype=torch.float64, device=dev)
+    for m in range(16):
+        th = (2 * math.pi * kvec[m, 0] / shape[0] * axes[0])[:, None, None] + \
+             (2 * math.pi * kvec[m, 1] / shape[1] * axes[1])[None, :, None] + \
+             (2 * math.pi * kvec[m, 2] / shape[2] * axes[2])[None, None, :]
+        fb += torch.cos(th + phase[m])
+    xb = plan.input_pencil.scatter(fb.float()).contiguous()
+    del fb, th
+    plan.forward(xb, spec, ws)
+    got = plan.output_pencil.gather(spec)[0]
+    exp = torch.zeros_like(got)
+    ntot = shape[0] * shape[1] * shape[2]
+    for m in range(16):
+        k = [int(v) for v in kvec[m]]
+        ph = float(phase[m])
+        exp[k[0], k[1], k[2]] += (ntot / 2) * complex(math.cos(ph), math.sin(ph))
+        mk = ((-k[0]) % shape[0], (-k[1]) % shape[1], (-k[2]) % shape[2])
+        if mk[2] <= shape[2] // 2:
+            exp[mk] += (ntot / 2) * complex(math.cos(ph), -math.sin(ph))
+    kb = float(torch.linalg.vector_norm((got - exp).to(torch.complex128)) /
+               torch.linalg.vector_norm(exp.to(torch.complex128)))
+    del got, exp, xb
+
+    # e2e through the C-ABI with pinned host buffers holding the concatenated
+    # virtual-rank arrays (the reference's local arrays): H2D, forward, inverse
+    # with the spectrum check, D2H -- every step
+    h_in = x.cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    g_in = torch.empty_like(x)
+
+    def e2e_step():
+        g_in.copy_(h_in, non_blocking=True)
+        plan.forward(g_in, spec, ws)
+        plan.inverse(spec, back, ws)  # syncs to report R2cError::InvalidSpectrum like the reference
+        h_out.copy_(back, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 5))
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    t_start = time.perf_counter()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1) / e2e_steps)
+    e2e_wall_ms = (time.perf_counter() - t_start) * 1e3 / e2e_steps
+    h2d = h_in.numel() * h_in.element_size()
+    d2h = h_out.numel() * h_out.element_size()
+    e2e_err = float(torch.linalg.vector_norm((h_out - h_in).double()) / torch.linalg.vector_norm(h_in.double()))
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline()
+
+    if rank == 0:
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic_pass_kernel_512cube.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f).get("bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: field A uniform(-1,1) numpy default_rng(1); field B 16 random-phase cosines",
+            "config": {"workload": "R2C f32 [512,512,512] -> [512,512,257], 4x8 virtual pencil grid, fused "
+                                   "transpose-in-pass, forward + normalised inverse",
+                       "grid": list(GRID), "shape": list(shape),
+                       "l2": "no flush: every pass streams >= 512 MiB, larger than the 126 MB L2",
+                       "parallelism": f"replicas x{world} (each GPU runs the full field)"},
+            "gflops": flops(shape) / (ms * 1e-3) / 1e9 * world,
+            "accuracy": {"roundtrip_rel_l2": rt, "field_b_rel_l2": kb, "bound": 1e-6 * lg,
+                         "e2e_roundtrip_rel_l2": e2e_err},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "pb::pass_kernel<float>", "bytes_per_launch": per_pass,
+                         "launch_ms_avg": pass_ms / launches, "spectrum_check_ms": check_ms},
+            "e2e": {"value": bytes_step / (e2e_ms * 1e-3) / 1e9 * world, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "wall_ms_per_step": e2e_wall_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * (plan.info.passes_forward + plan.info.passes_inverse + 2),
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "cpu_baseline": base,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    ok = rt <= 1e-6 * lg and kb <= 1e-6 * lg
+    return 0 if ok else 3
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

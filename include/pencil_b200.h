@@ -1,0 +1,225 @@
+/*
+ * pencil_b200.h - C-ABI of the B200 (sm_100a) pencil FFT library.
+ *
+ * Drop-in boundary for the pencil FFT hot path of nogaki/pencil-rs.  Every
+ * entry point names the reference item it replaces (paths relative to the
+ * reference workspace root).  Plain pointers and sizes only: no CUDA or torch
+ * types in the signatures (streams are `void*` holding a cudaStream_t).
+ *
+ * Data model.  The reference runs one MPI rank per process; here a P_0 x ... x
+ * P_{M-1} Cartesian grid of *virtual ranks* lives on one GPU.  Virtual rank r
+ * has row-major Cartesian coordinates (topology.rs:25-46, reorder=false) and
+ * owns the reference's local array: row-major [extra..., permuted spatial...]
+ * (crates/pencil-array/src/lib.rs:12-19) over its floor-partition ranges
+ * (geometry.rs:9-59).  A device buffer argument is the concatenation of all
+ * virtual ranks' local arrays in rank order, so each rank's bytes equal the
+ * reference's local array on that rank.  pb_pencil_local() gives each rank's
+ * offset and memory shape.
+ *
+ * Errors: every entry point returns a pb_status.  Preflight errors return
+ * before any device work and leave every buffer unchanged (the reference's
+ * collective preflight contract, crates/pencil-fft/src/lib.rs:97-117).
+ * Execution is asynchronous on the given stream; an inverse/backward C2R
+ * spectrum rejection (R2cError::InvalidSpectrum) is recorded in the workspace
+ * and reported by pb_execute_status(); when rejected, the destination is left
+ * unchanged, as in the reference.
+ */
+#ifndef PENCIL_B200_H
+#define PENCIL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_MAX_DIMS 8
+#define PB_MAX_GRID 4
+
+/* Status codes; names follow FftError (crates/pencil-fft/src/distributed.rs:340-420),
+ * R2cError (442-457), TransposeError (crates/pencil-array/src/transpose.rs:113-176),
+ * SpatialRemapError (crates/pencil-array/src/spatial_remap.rs:35-110). */
+typedef enum pb_status {
+  PB_OK = 0,
+  PB_EINVALID_DIMENSIONS = 1,        /* FftError::InvalidDimensions (N<2, M==0, M>=N, empty selection) */
+  PB_EZERO_EXTENT = 2,               /* PencilError::ZeroGlobalExtent */
+  PB_EINVALID_DECOMPOSITION = 3,     /* PencilError::InvalidDecomposition */
+  PB_EINVALID_PERMUTATION = 4,       /* PencilError::InvalidPermutation */
+  PB_EINVALID_LENGTH = 5,            /* Local*Error::InvalidLength (e.g. DCT-I of length 1) */
+  PB_EINVALID_GRAPH = 6,             /* MixedError::InvalidGraph */
+  PB_EINPUT_LAYOUT_MISMATCH = 7,     /* FftError::InputLayoutMismatch (C2R real length) */
+  PB_EUNSUPPORTED_DECOMPOSITION_CHANGE = 8, /* TransposeError::UnsupportedDecompositionChange */
+  PB_ECOUNT_OVERFLOW = 9,            /* TransposeError::CountOverflow (i32 MPI counts) */
+  PB_ESHAPE_MISMATCH = 10,           /* SpatialRemapError::ShapeMismatch / layout mismatch */
+  PB_EINVALID_SIGN = 11,             /* SpatialRemapError::InvalidSign */
+  PB_EINVALID_SPECTRUM = 12,         /* R2cError::InvalidSpectrum */
+  PB_ETIMEOUT = 13,                  /* a bounded device wait gave up */
+  PB_ENULL = 14,                     /* null handle or pointer */
+  PB_EUNSUPPORTED = 15,              /* valid for the reference, not (yet) for this library */
+  PB_ECUDA = 16,                     /* CUDA runtime error */
+  PB_EINVALID_ARGUMENT = 17,
+  PB_EWRONG_PLAN = 18                /* workspace/batch does not belong to this plan */
+} pb_status;
+
+typedef enum pb_precision { PB_F32 = 0, PB_F64 = 1 } pb_precision;
+
+/* Operations.  FORWARD/INVERSE/BACKWARD are the reference's forward, normalised
+ * inverse and raw backward (distributed.rs:1448-1500).  The VJP_* operations are
+ * the adjoints (vector-Jacobian products) of those three maps: they take a
+ * cotangent in the operation's output layout and return one in its input
+ * layout.  The reference has no adjoints. */
+typedef enum pb_op {
+  PB_FORWARD = 0,
+  PB_INVERSE = 1,
+  PB_BACKWARD = 2,
+  PB_VJP_FORWARD = 3,
+  PB_VJP_INVERSE = 4,
+  PB_VJP_BACKWARD = 5
+} pb_op;
+
+/* Per-axis transform codes: AxisTransform (distributed/mixed.rs:92-101),
+ * R2rKind (r2r.rs:18-35, FFTW REDFT/RODFT names) and AxisR2rKind::Dht. */
+typedef enum pb_axis_kind {
+  PB_AXIS_NONE = 0,
+  PB_AXIS_FFT = 1,
+  PB_AXIS_RFFT = 2,
+  PB_AXIS_DCT1 = 10, /* REDFT00 */
+  PB_AXIS_DCT2 = 11, /* REDFT10 */
+  PB_AXIS_DCT3 = 12, /* REDFT01 */
+  PB_AXIS_DCT4 = 13, /* REDFT11 */
+  PB_AXIS_DST1 = 14, /* RODFT00 */
+  PB_AXIS_DST2 = 15, /* RODFT10 */
+  PB_AXIS_DST3 = 16, /* RODFT01 */
+  PB_AXIS_DST4 = 17, /* RODFT11 */
+  PB_AXIS_DHT = 18
+} pb_axis_kind;
+
+/* Plan geometry: MpiTopology<M> process grid + global shape + ExtraShape +
+ * DistributedLayout::permute_dims (distributed.rs:517-524, 1192-1300). */
+typedef struct pb_geom {
+  int32_t ndim;                    /* N, spatial dimensions */
+  int32_t ngrid;                   /* M, process-grid dimensions (1 <= M < N) */
+  int64_t shape[PB_MAX_DIMS];      /* global spatial shape, logical axis order */
+  int32_t grid[PB_MAX_GRID];       /* process-grid extents P_0..P_{M-1} */
+  int32_t extra_ndim;              /* ExtraShape dimensions (0 = scalar) */
+  int64_t extra[PB_MAX_DIMS];
+  int32_t permute_dims;            /* 1 = reference default (stage axis last in memory) */
+} pb_geom;
+
+/* One pencil layout (Pencil::new_permuted, crates/pencil-array/src/pencil.rs:69-112). */
+typedef struct pb_pencil_desc {
+  int32_t ndim;
+  int32_t ngrid;
+  int64_t shape[PB_MAX_DIMS];
+  int32_t grid[PB_MAX_GRID];
+  int32_t decomposition[PB_MAX_GRID]; /* spatial axis split by each grid axis */
+  int32_t permutation[PB_MAX_DIMS];   /* logical axes in memory order */
+} pb_pencil_desc;
+
+typedef struct pb_plan_info {
+  int64_t input_elems;     /* all virtual ranks, extra included */
+  int64_t output_elems;
+  int32_t input_complex;   /* element of the FORWARD input: 1 complex, 0 real */
+  int32_t output_complex;
+  int32_t real_bytes;      /* 4 (f32) or 8 (f64) */
+  int32_t nranks;
+  int64_t workspace_bytes; /* bytes of the caller-owned workspace */
+  int32_t passes_forward;  /* kernel launches of one FORWARD */
+  int32_t passes_inverse;
+} pb_plan_info;
+
+typedef struct pb_plan pb_plan;
+typedef struct pb_transpose pb_transpose;
+typedef struct pb_remap pb_remap;
+typedef struct pb_batch pb_batch;
+
+/* ---- library ---------------------------------------------------------- */
+const char* pb_version(void);
+const char* pb_status_string(int status);
+
+/* ---- host geometry (no device work) ----------------------------------- */
+/* Local ranges/shape of one virtual rank: local_ranges_for + Pencil local
+ * shapes (geometry.rs:33-59, pencil.rs:97-100).  start/shape_logical/shape_memory
+ * have ndim entries; *offset is the rank's element offset in a concatenated
+ * buffer holding extra_count blocks per rank. */
+int pb_pencil_local(const pb_pencil_desc* pencil, int32_t rank, int64_t extra_count, int64_t* start,
+                    int64_t* shape_logical, int64_t* shape_memory, int64_t* local_len, int64_t* offset);
+/* Canonical route stage `stage` (build_route, distributed.rs:2306-2382). */
+int pb_route_stage(const pb_geom* geom, int32_t stage, pb_pencil_desc* out, int32_t* distributed_edge);
+
+/* ---- plans (C2cPlan / R2cPlan / C2rPlan / R2rPlan / DhtPlan / Mixed*) -- */
+/* C2cPlan::from_shape_with_selection_and_layout (distributed.rs:1259-1282) and
+ * from_shape_with_fft_directions (1689-1718).  selection/positive: N bytes or NULL
+ * (NULL selection = AxisSelection::all(); positive[a]=1 = FourierDirection::Backward). */
+int pb_plan_create_c2c(const pb_geom* geom, int32_t precision, const uint8_t* selection,
+                       const uint8_t* positive, pb_plan** plan);
+/* R2cPlan::from_shape_with_selection_and_layout (distributed/r2c.rs:518-628,1204-1448). */
+int pb_plan_create_r2c(const pb_geom* geom, int32_t precision, const uint8_t* selection, pb_plan** plan);
+/* C2rPlan::from_shape_with_selection_and_layout (distributed/c2r.rs:167-191);
+ * geom->shape is the reduced complex shape. */
+int pb_plan_create_c2r(const pb_geom* geom, int64_t real_len, int32_t precision, const uint8_t* selection,
+                       pb_plan** plan);
+/* R2rPlan::from_shape (distributed/r2r.rs:1080-1093; kinds[a] = PB_AXIS_NONE or a
+ * DCT/DST kind) and DhtPlan (distributed/r2r.rs:83-86; PB_AXIS_DHT).  Real
+ * (complex_values=0) or componentwise complex (1) values. */
+int pb_plan_create_r2r(const pb_geom* geom, int32_t precision, int32_t complex_values, const int32_t* kinds,
+                       pb_plan** plan);
+/* MixedC2cPlan (distributed/mixed.rs:392-440): transforms[a] in {NONE, FFT, DCT*, DST*, DHT}. */
+int pb_plan_create_mixed_c2c(const pb_geom* geom, int32_t precision, const int32_t* transforms,
+                             const uint8_t* positive, pb_plan** plan);
+/* MixedR2cPlan (distributed/mixed.rs:441-470, validate_r2c_graph 1602-1626). */
+int pb_plan_create_mixed_r2c(const pb_geom* geom, int32_t precision, const int32_t* transforms, pb_plan** plan);
+int pb_plan_destroy(pb_plan* plan);
+int pb_plan_get_info(const pb_plan* plan, pb_plan_info* info);
+/* which: 0 = FORWARD input pencil, 1 = FORWARD output pencil (input_pencil /
+ * output_pencil, distributed.rs:1317-1330). */
+int pb_plan_pencil(const pb_plan* plan, int32_t which, pb_pencil_desc* out);
+
+/* forward / inverse / backward (distributed.rs:1448-1500) and their adjoints.
+ * in/out/workspace: device pointers (workspace of info.workspace_bytes, one per
+ * concurrent stream); stream: cudaStream_t or NULL. Out-of-place; `in` is
+ * preserved. */
+int pb_execute(pb_plan* plan, int32_t op, const void* in, void* out, void* workspace, void* stream);
+/* Waits for `stream` and reports the spectrum check of the last C2R-bearing
+ * execution that used `workspace`: PB_OK or PB_EINVALID_SPECTRUM. */
+int pb_execute_status(pb_plan* plan, void* workspace, void* stream);
+/* forward_with_timing & co. (distributed.rs:1545-1600, TransformTiming 290-325):
+ * synchronous; stage_ms[i] = device time of kernel launch i (pass or check),
+ * *count = number of launches. */
+int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void* workspace, void* stream,
+                     float* stage_ms, int32_t capacity, int32_t* count);
+
+/* ---- transposes ------------------------------------------------------- */
+/* AllToAllvTransposePlan::new (crates/pencil-array/src/alltoallv_transpose.rs:65-72). */
+int pb_transpose_create_alltoallv(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,
+                                  int32_t elem_bytes, pb_transpose** plan);
+/* LocalTransposePlan::new (crates/pencil-array/src/local_transpose.rs:48-72). */
+int pb_transpose_create_local(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,
+                              int32_t elem_bytes, pb_transpose** plan);
+/* workspace_requirements (transpose.rs:684-721), summed over virtual ranks. */
+int pb_transpose_workspace(const pb_transpose* plan, int64_t* send_elems, int64_t* receive_elems);
+/* execute_views (alltoallv_transpose.rs:204-254, local_transpose.rs:87-132): one fused pass. */
+int pb_transpose_execute(pb_transpose* plan, const void* src, void* dst, void* stream);
+/* The unfused steps with the reference's segment layout: pack_source
+ * (transpose.rs:1126-1176), the MPI_Alltoallv of every sub-communicator
+ * (alltoallv_transpose.rs:324-367), unpack_destination (transpose.rs:1233-1281). */
+int pb_transpose_pack(pb_transpose* plan, const void* src, void* send, void* stream);
+int pb_transpose_exchange(pb_transpose* plan, const void* send, void* receive, void* stream);
+int pb_transpose_unpack(pb_transpose* plan, const void* receive, void* dst, void* stream);
+int pb_transpose_destroy(pb_transpose* plan);
+
+/* ---- affine remap ----------------------------------------------------- */
+/* SpatialRemapPlan::prepare (spatial_remap.rs:221-338); offsets are i64 (the
+ * reference takes i128; every offset is first reduced mod the extent). */
+int pb_remap_create(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count, int32_t elem_bytes,
+                    const int8_t* signs, const int64_t* offsets, pb_remap** plan);
+/* SpatialRemapPlan::apply_views (spatial_remap.rs:349-404). */
+int pb_remap_apply(pb_remap* plan, const void* src, void* dst, void* stream);
+int pb_remap_destroy(pb_remap* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PENCIL_B200_H */

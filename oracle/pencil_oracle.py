@@ -42,6 +42,25 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
+# Host threads for the local line transforms (scipy.fft's pocketfft with
+# ``workers``); 1 keeps numpy's single-threaded FFT.  Only the timed CPU
+# baseline raises it.
+WORKERS = 1
+
+
+def set_workers(n: int) -> None:
+    global WORKERS
+    WORKERS = max(1, int(n))
+
+
+def _fft(x, axis, inverse=False):
+    if WORKERS > 1:
+        import scipy.fft as sf
+        return (sf.ifft(x, axis=axis, workers=WORKERS) * x.shape[axis]) if inverse else sf.fft(
+            x, axis=axis, workers=WORKERS)
+    return (np.fft.ifft(x, axis=axis) * x.shape[axis]) if inverse else np.fft.fft(x, axis=axis)
+
+
 # ---------------------------------------------------------------------------
 # errors (mirroring the reference error enums by name)
 # ---------------------------------------------------------------------------
@@ -441,12 +460,15 @@ def c2c_lines(x: np.ndarray, axis: int, positive: bool, scale: float = 1.0) -> n
     crates/pencil-fft/src/lib.rs:498-550; inverse = backward * 1/n."""
     x = np.asarray(x, dtype=np.complex128)
     n = x.shape[axis]
-    y = np.fft.ifft(x, axis=axis) * n if positive else np.fft.fft(x, axis=axis)
+    y = _fft(x, axis, inverse=positive)
     return y * scale if scale != 1.0 else y
 
 
 def r2c_lines(x: np.ndarray, axis: int) -> np.ndarray:
     """LocalR2cPlan::forward, crates/pencil-fft/src/r2c.rs:428-448."""
+    if WORKERS > 1:
+        import scipy.fft as sf
+        return sf.rfft(np.asarray(x, dtype=np.float64), axis=axis, workers=WORKERS)
     return np.fft.rfft(np.asarray(x, dtype=np.float64), axis=axis)
 
 
@@ -461,7 +483,11 @@ def c2r_lines(x: np.ndarray, axis: int, n: int, scale: float = 1.0, check=True) 
             raise NonzeroEndpoint()
         if n % 2 == 0 and np.any(np.take(x, n // 2, axis=axis).imag != 0):
             raise NonzeroEndpoint()
-    y = np.fft.irfft(x, n=n, axis=axis) * n
+    if WORKERS > 1:
+        import scipy.fft as sf
+        y = sf.irfft(x, n=n, axis=axis, workers=WORKERS) * n
+    else:
+        y = np.fft.irfft(x, n=n, axis=axis) * n
     return y * scale if scale != 1.0 else y
 
 

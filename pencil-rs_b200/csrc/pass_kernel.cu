@@ -1,0 +1,706 @@
+// Fused pencil pass: gather L lines of the transform axis from the source
+// pencil layout, run the local 1-D transform in shared memory, scatter the
+// results straight into the destination pencil layout.
+//
+// One launch replaces, for one route stage, the reference's per-line RustFFT
+// loop (crates/pencil-fft/src/lib.rs:591-603, r2c.rs:428-465, r2r.rs:681-778,
+// dht.rs:253-302) AND the following transition's pack -> MPI_Alltoallv ->
+// unpack (crates/pencil-array/src/transpose.rs:1126-1281,
+// alltoallv_transpose.rs:204-367): each element is written once, directly to
+// the address its destination virtual rank's local array has for it.
+//
+// FFT core: Stockham autosort, mixed radix 2/3/4/5/7/8 with compile-time
+// butterflies plus an O(R) generic radix for other primes, twiddles from a
+// table of m-th roots of unity generated on the host in extended precision
+// and rounded once to the plan type.  R2C/C2R use the two-real-lines-in-one-
+// complex-FFT split; DCT/DST II/III use Makhoul's n-point reordering with
+// pre/post twiddles; DCT/DST IV use an n/2-point complex FFT (even n); type I
+// kinds use the symmetric/antisymmetric extension of a line pair; the DHT is
+// the Hartley combination of a pair's FFT.  Every real-valued kind processes
+// two real lines (or the two components of one complex line) per complex FFT.
+#include <cuda_runtime.h>
+
+#include "pb_device.cuh"
+
+namespace pb {
+
+template <typename R>
+struct Cx;
+template <>
+struct Cx<float> {
+  using T = float2;
+};
+template <>
+struct Cx<double> {
+  using T = double2;
+};
+
+template <typename C, typename R>
+__device__ __forceinline__ C mk(R x, R y) {
+  C c;
+  c.x = x;
+  c.y = y;
+  return c;
+}
+template <typename C>
+__device__ __forceinline__ C add(C a, C b) {
+  a.x += b.x;
+  a.y += b.y;
+  return a;
+}
+template <typename C>
+__device__ __forceinline__ C sub(C a, C b) {
+  a.x -= b.x;
+  a.y -= b.y;
+  return a;
+}
+template <typename C, typename R>
+__device__ __forceinline__ C scl(C a, R s) {
+  a.x *= s;
+  a.y *= s;
+  return a;
+}
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C c;
+  c.x = a.x * b.x - a.y * b.y;
+  c.y = a.x * b.y + a.y * b.x;
+  return c;
+}
+// multiply by e^{-i pi/2} (forward) or e^{+i pi/2} (inverse)
+template <bool INV, typename C>
+__device__ __forceinline__ C rot(C a) {
+  C c;
+  if (INV) {
+    c.x = -a.y;
+    c.y = a.x;
+  } else {
+    c.x = a.y;
+    c.y = -a.x;
+  }
+  return c;
+}
+// v * w (forward) or v * conj(w) (inverse)
+template <bool INV, typename C>
+__device__ __forceinline__ C twmul(C v, C w) {
+  C c;
+  if (INV) {
+    c.x = v.x * w.x + v.y * w.y;
+    c.y = v.y * w.x - v.x * w.y;
+  } else {
+    c.x = v.x * w.x - v.y * w.y;
+    c.y = v.x * w.y + v.y * w.x;
+  }
+  return c;
+}
+
+// cos(2 pi i / R), sin(2 pi i / R) for the odd small radices (exact doubles).
+__host__ __device__ constexpr double kcos(int R, int i) {
+  return R == 3 ? (i == 0 ? 1.0 : -0.5)
+         : R == 5 ? (i == 0 ? 1.0 : (i == 1 || i == 4) ? 0.30901699437494745 : -0.8090169943749475)
+                  : (i == 0 ? 1.0
+                     : (i == 1 || i == 6) ? 0.6234898018587335
+                     : (i == 2 || i == 5) ? -0.2225209339563144
+                                          : -0.9009688679024191);
+}
+__host__ __device__ constexpr double ksin(int R, int i) {
+  return R == 3 ? (i == 0 ? 0.0 : i == 1 ? 0.8660254037844386 : -0.8660254037844386)
+         : R == 5 ? (i == 0   ? 0.0
+                     : i == 1 ? 0.9510565162951535
+                     : i == 2 ? 0.5877852522924731
+                     : i == 3 ? -0.5877852522924731
+                              : -0.9510565162951535)
+                  : (i == 0   ? 0.0
+                     : i == 1 ? 0.7818314824680298
+                     : i == 2 ? 0.9749279121818236
+                     : i == 3 ? 0.4338837391175581
+                     : i == 4 ? -0.4338837391175581
+                     : i == 5 ? -0.9749279121818236
+                              : -0.7818314824680298);
+}
+
+template <typename C, int RAD, bool INV>
+struct Bfly;
+
+template <typename C, bool INV>
+struct Bfly<C, 2, INV> {
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0];
+    v[0] = add(a, v[1]);
+    v[1] = sub(a, v[1]);
+  }
+};
+
+template <typename C, bool INV>
+struct Bfly<C, 4, INV> {
+  static __device__ __forceinline__ void run(C* v) {
+    C t0 = add(v[0], v[2]), t1 = sub(v[0], v[2]);
+    C t2 = add(v[1], v[3]), t3 = rot<INV>(sub(v[1], v[3]));
+    v[0] = add(t0, t2);
+    v[2] = sub(t0, t2);
+    v[1] = add(t1, t3);
+    v[3] = sub(t1, t3);
+  }
+};
+
+template <typename C, bool INV>
+struct Bfly<C, 8, INV> {
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(v[0].x);
+    const R h = R(0.7071067811865476);
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    Bfly<C, 4, INV>::run(e);
+    Bfly<C, 4, INV>::run(o);
+    C w1 = scl(add(o[1], rot<INV>(o[1])), h);
+    C w2 = rot<INV>(o[2]);
+    C w3 = scl(sub(rot<INV>(o[3]), o[3]), h);
+    v[0] = add(e[0], o[0]);
+    v[4] = sub(e[0], o[0]);
+    v[1] = add(e[1], w1);
+    v[5] = sub(e[1], w1);
+    v[2] = add(e[2], w2);
+    v[6] = sub(e[2], w2);
+    v[3] = add(e[3], w3);
+    v[7] = sub(e[3], w3);
+  }
+};
+
+// Odd prime radix: X_q = v0 + sum_p a_p cos(2 pi pq/R) -/+ i sum_p b_p sin(2 pi pq/R)
+template <typename C, int RAD, bool INV>
+struct BflyOdd {
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(v[0].x);
+    constexpr int H = (RAD - 1) / 2;
+    C a[H], b[H];
+#pragma unroll
+    for (int p = 1; p <= H; ++p) {
+      a[p - 1] = add(v[p], v[RAD - p]);
+      b[p - 1] = sub(v[p], v[RAD - p]);
+    }
+    C out[RAD];
+    C s0 = v[0];
+#pragma unroll
+    for (int p = 0; p < H; ++p) s0 = add(s0, a[p]);
+    out[0] = s0;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      C A = v[0];
+      C B = mk<C, R>(R(0), R(0));
+#pragma unroll
+      for (int p = 1; p <= H; ++p) {
+        const int i = (p * q) % RAD;
+        A = add(A, scl(a[p - 1], R(kcos(RAD, i))));
+        B = add(B, scl(b[p - 1], R(ksin(RAD, i))));
+      }
+      C rB = rot<INV>(B);
+      out[q] = add(A, rB);
+      out[RAD - q] = sub(A, rB);
+    }
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) v[q] = out[q];
+  }
+};
+template <typename C, bool INV>
+struct Bfly<C, 3, INV> : BflyOdd<C, 3, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 5, INV> : BflyOdd<C, 5, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 7, INV> : BflyOdd<C, 7, INV> {};
+
+// One Stockham stage: input index j + r*m/R, output (j - j%Ns)*R + j%Ns + r*Ns.
+template <typename C, int RAD, bool INV>
+__device__ __forceinline__ void fft_stage(const C* __restrict__ in, C* __restrict__ out, int nseq, int m,
+                                          int ld, int Ns, const C* __restrict__ W) {
+  const int nb = m / RAD;
+  const int total = nseq * nb;
+  const int tw = m / (Ns * RAD);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int s = t / nb;
+    const int j = t - s * nb;
+    const C* src = in + s * ld;
+    C* dst = out + s * ld;
+    const int k = j % Ns;
+    C v[RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) v[r] = src[j + r * nb];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < RAD; ++r) v[r] = twmul<INV>(v[r], W[k * tw * r]);
+    }
+    Bfly<C, RAD, INV>::run(v);
+    const int base = (j - k) * RAD + k;
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) dst[base + r * Ns] = v[r];
+  }
+}
+
+// Generic radix (any R): direct O(R^2) butterfly reading the stage input from
+// shared memory.
+template <typename C, bool INV>
+__device__ void fft_stage_generic(const C* __restrict__ in, C* __restrict__ out, int nseq, int m, int ld,
+                                  int Ns, int RAD, const C* __restrict__ W) {
+  using R = decltype(W[0].x);
+  const int nb = m / RAD;
+  const int total = nseq * nb;
+  const int tw = m / (Ns * RAD);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int s = t / nb;
+    const int j = t - s * nb;
+    const C* src = in + s * ld;
+    C* dst = out + s * ld;
+    const int k = j % Ns;
+    const int base = (j - k) * RAD + k;
+    for (int q = 0; q < RAD; ++q) {
+      C acc = mk<C, R>(R(0), R(0));
+      int idx = 0;  // (p*q) mod RAD
+      for (int p = 0; p < RAD; ++p) {
+        C v = src[j + p * nb];
+        if (Ns > 1 && p > 0) v = twmul<INV>(v, W[k * tw * p]);
+        acc = add(acc, twmul<INV>(v, W[idx * nb]));
+        idx += q;
+        if (idx >= RAD) idx -= RAD;
+      }
+      dst[base + q * Ns] = acc;
+    }
+  }
+}
+
+template <typename C, bool INV>
+__device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const PassArgs& A) {
+  C* in = b0;
+  C* out = b1;
+  int Ns = 1;
+  for (int s = 0; s < A.nstages; ++s) {
+    const int R = A.radix[s];
+    switch (R) {
+      case 2: fft_stage<C, 2, INV>(in, out, nseq, m, ld, Ns, W); break;
+      case 3: fft_stage<C, 3, INV>(in, out, nseq, m, ld, Ns, W); break;
+      case 4: fft_stage<C, 4, INV>(in, out, nseq, m, ld, Ns, W); break;
+      case 5: fft_stage<C, 5, INV>(in, out, nseq, m, ld, Ns, W); break;
+      case 7: fft_stage<C, 7, INV>(in, out, nseq, m, ld, Ns, W); break;
+      case 8: fft_stage<C, 8, INV>(in, out, nseq, m, ld, Ns, W); break;
+      default: fft_stage_generic<C, INV>(in, out, nseq, m, ld, Ns, R, W); break;
+    }
+    __syncthreads();
+    C* t = in;
+    in = out;
+    out = t;
+    Ns *= R;
+  }
+  return in;
+}
+
+__device__ __forceinline__ bool weight_hit(int mode, int idx, int n) {
+  switch (mode) {
+    case W_FIRST: return idx == 0;
+    case W_LAST: return idx == n - 1;
+    case W_INTERIOR: return idx > 0 && idx < n - 1;
+    case W_HALF_INTERIOR: return idx != 0 && !((n & 1) == 0 && idx == n / 2);
+    default: return false;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) pass_kernel(const PassArgs A) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (A.gate != nullptr && *A.gate != 0) return;
+
+  // ---- tile decode: (extra, outer coordinates, chunk of the tile axis)
+  long long t = blockIdx.x;
+  const int ci = (int)(t % A.nchunks);
+  long long outer = t / A.nchunks;
+  const int2 ch = A.chunks[ci];
+  int g[MAXN];
+#pragma unroll
+  for (int x = 0; x < MAXN; ++x) g[x] = 0;
+  for (int i = A.nouter_axes - 1; i >= 0; --i) {
+    g[A.outer_axis[i]] = (int)(outer % A.outer_ext[i]);
+    outer /= A.outer_ext[i];
+  }
+  const long long e = outer;
+  g[A.b] = ch.x;
+  const int L = ch.y;
+
+  // ---- shared memory carve-up
+  const int nin = A.n_in, nout = A.n_out, m = A.m, ld = A.ld;
+  long long* sA = reinterpret_cast<long long*>(smem);
+  long long* dA = sA + nin;
+  int* sS = reinterpret_cast<int*>(dA + nout);
+  int* dS = sS + nin;
+  size_t off = ((size_t)(nin + nout) * 12 + 15) & ~size_t(15);
+  C* W = reinterpret_cast<C*>(smem + off);
+  C* buf0 = W + ((m + 1) & ~1);
+  C* buf1 = buf0 + A.buf_elems;
+
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k = tid; k < nin; k += nt) {
+    int gg[MAXN];
+#pragma unroll
+    for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
+    gg[A.a] = k;
+    int sb;
+    sA[k] = locate(A.src, e, gg, A.b, &sb);
+    sS[k] = sb;
+  }
+  for (int k = tid; k < nout; k += nt) {
+    int gg[MAXN];
+#pragma unroll
+    for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
+    gg[A.a] = k;
+    int sb;
+    dA[k] = locate(A.dst, e, gg, A.b, &sb);
+    dS[k] = sb;
+  }
+  const C* Wg = reinterpret_cast<const C*>(A.twiddle);
+  if (Wg != nullptr)
+    for (int i = tid; i < m; i += nt) W[i] = Wg[i];
+  __syncthreads();
+
+  const int total_in = L * nin;
+  const bool c2c = A.kind == P_C2C;
+  // ---- load: global (source layout) -> shared
+  if (A.in_complex) {
+    const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+    C* st = c2c ? buf0 : buf1;
+    const int row = c2c ? ld : nin;
+    if (A.src_k_contig) {
+      for (int i = tid; i < total_in; i += nt) {
+        const int j = i / nin, k = i - j * nin;
+        st[j * row + k] = in[sA[k] + (long long)j * sS[k]];
+      }
+    } else {
+      for (int i = tid; i < total_in; i += nt) {
+        const int k = i / L, j = i - k * L;
+        st[j * row + k] = in[sA[k] + (long long)j * sS[k]];
+      }
+    }
+  } else {
+    const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+    R* st = reinterpret_cast<R*>(buf1);
+    if (A.src_k_contig) {
+      for (int i = tid; i < total_in; i += nt) {
+        const int j = i / nin, k = i - j * nin;
+        st[j * nin + k] = in[sA[k] + (long long)j * sS[k]];
+      }
+    } else {
+      for (int i = tid; i < total_in; i += nt) {
+        const int k = i / L, j = i - k * L;
+        st[j * nin + k] = in[sA[k] + (long long)j * sS[k]];
+      }
+    }
+  }
+  __syncthreads();
+
+  const int n = A.n;
+  const R* str = reinterpret_cast<const R*>(buf1);  // real staging
+  const C* stc = buf1;                              // complex staging
+  const C* aux0 = reinterpret_cast<const C*>(A.aux0);
+  const C* aux1 = reinterpret_cast<const C*>(A.aux1);
+  const R pre_f = R(A.pre_factor);
+  const R zero = R(0);
+
+  // value of component c (0: first real line / real part, 1: second / imag) of pair p at index q
+  auto getv = [&](int p, int c, int q) -> R {
+    R v;
+    if (A.in_complex) {
+      const C z = stc[p * nin + q];
+      v = c ? z.y : z.x;
+    } else {
+      const int l = 2 * p + c;
+      v = (l < L) ? str[l * nin + q] : zero;
+    }
+    if (A.pre_mode != W_NONE && weight_hit(A.pre_mode, q, n)) v *= pre_f;
+    return v;
+  };
+
+  int nseq = L;
+  const int pairs = (A.kind == P_R2R && A.in_complex) ? L : (L + 1) / 2;
+  // ---- pre-process: staging -> FFT input sequences in buf0
+  if (A.kind == P_R2C) {
+    nseq = pairs;
+    for (int i = tid; i < nseq * m; i += nt) {
+      const int s = i / m, q = i - s * m;
+      buf0[s * ld + q] = mk<C, R>(getv(s, 0, q), getv(s, 1, q));
+    }
+  } else if (A.kind == P_C2R) {
+    nseq = pairs;
+    const int h = n / 2 + 1;
+    for (int i = tid; i < nseq * m; i += nt) {
+      const int s = i / m, q = i - s * m;
+      const int hq = q < h ? q : n - q;
+      const bool edge = (hq == 0) || ((n & 1) == 0 && hq == n / 2);
+      R w = R(1);
+      if (A.pre_mode == W_HALF_INTERIOR && !edge) w = pre_f;
+      C X = mk<C, R>(zero, zero), Y = mk<C, R>(zero, zero);
+      const int l0 = 2 * s, l1 = 2 * s + 1;
+      X = stc[l0 * nin + hq];
+      if (l1 < L) Y = stc[l1 * nin + hq];
+      if (q >= h) {
+        X.y = -X.y;
+        Y.y = -Y.y;
+      }
+      if (edge) {
+        X.y = zero;
+        Y.y = zero;
+      }
+      buf0[s * ld + q] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
+    }
+  } else if (A.kind == P_R2R) {
+    const int sub = A.sub;
+    const bool iv4 = (sub == S_DCT4 || sub == S_DST4);
+    nseq = iv4 ? 2 * pairs : pairs;
+    for (int i = tid; i < nseq * m; i += nt) {
+      const int s = i / m, q = i - s * m;
+      C z;
+      switch (sub) {
+        case S_DCT2:
+        case S_DST2: {
+          const int idx = (2 * q < n) ? 2 * q : 2 * (n - 1 - q) + 1;
+          R x = getv(s, 0, idx), y = getv(s, 1, idx);
+          if (sub == S_DST2 && (idx & 1)) {
+            x = -x;
+            y = -y;
+          }
+          z = mk<C, R>(x, y);
+        } break;
+        case S_DCT3:
+        case S_DST3: {
+          const int i0 = (sub == S_DST3) ? n - 1 - q : q;
+          R ux = getv(s, 0, i0), uy = getv(s, 1, i0);
+          R vx = zero, vy = zero;
+          if (q > 0) {
+            const int i1 = (sub == S_DST3) ? q - 1 : n - q;
+            vx = getv(s, 0, i1);
+            vy = getv(s, 1, i1);
+          }
+          const C w = aux0[q];
+          const C Vx = cmul(w, mk<C, R>(ux, -vx));
+          const C Vy = cmul(w, mk<C, R>(uy, -vy));
+          z = mk<C, R>(Vx.x - Vy.y, Vx.y + Vy.x);
+        } break;
+        case S_DCT4:
+        case S_DST4: {
+          const int p = s >> 1, c = s & 1;
+          if ((n & 1) == 0) {
+            const int i0 = 2 * q, i1 = n - 1 - 2 * q;
+            const int j0 = (sub == S_DST4) ? n - 1 - i0 : i0;
+            const int j1 = (sub == S_DST4) ? n - 1 - i1 : i1;
+            z = cmul(mk<C, R>(getv(p, c, j0), getv(p, c, j1)), aux0[q]);
+          } else {
+            if (q < n) {
+              const int j0 = (sub == S_DST4) ? n - 1 - q : q;
+              z = scl(aux0[q], getv(p, c, j0));
+            } else {
+              z = mk<C, R>(zero, zero);
+            }
+          }
+        } break;
+        case S_DCT1: {
+          const int idx = q <= n - 1 ? q : m - q;
+          z = mk<C, R>(getv(s, 0, idx), getv(s, 1, idx));
+        } break;
+        case S_DST1: {
+          if (q == 0 || q == n + 1) {
+            z = mk<C, R>(zero, zero);
+          } else if (q <= n) {
+            z = mk<C, R>(getv(s, 0, q - 1), getv(s, 1, q - 1));
+          } else {
+            z = mk<C, R>(-getv(s, 0, m - q - 1), -getv(s, 1, m - q - 1));
+          }
+        } break;
+        default: {  // DHT
+          z = mk<C, R>(getv(s, 0, q), getv(s, 1, q));
+        } break;
+      }
+      buf0[s * ld + q] = z;
+    }
+  }
+  __syncthreads();
+
+  // ---- FFT
+  C* res = buf0;
+  if (A.kind != P_COPY) {
+    if (A.inv)
+      res = fft_run<C, true>(buf0, buf1, nseq, m, ld, W, A);
+    else
+      res = fft_run<C, false>(buf0, buf1, nseq, m, ld, W, A);
+  }
+  C* other = (res == buf0) ? buf1 : buf0;
+  const R post_f = R(A.post_factor);
+  const R sc = R(A.scale);
+
+  // ---- post-process: FFT output -> output staging
+  if (A.kind == P_R2C) {
+    const int h = n / 2 + 1;
+    for (int i = tid; i < L * h; i += nt) {
+      const int l = i / h, k = i - l * h;
+      const int p = l >> 1;
+      const C a = res[p * ld + k];
+      const C b = res[p * ld + (k == 0 ? 0 : n - k)];
+      C v = (l & 1) ? mk<C, R>((a.y + b.y) * R(0.5), (b.x - a.x) * R(0.5))
+                    : mk<C, R>((a.x + b.x) * R(0.5), (a.y - b.y) * R(0.5));
+      R f = sc;
+      if (A.post_mode != W_NONE && weight_hit(A.post_mode, k, n)) f *= post_f;
+      other[l * nout + k] = scl(v, f);
+    }
+  } else if (A.kind == P_C2R) {
+    R* o = reinterpret_cast<R*>(other);
+    for (int i = tid; i < L * n; i += nt) {
+      const int l = i / n, q = i - l * n;
+      const C z = res[(l >> 1) * ld + q];
+      o[l * nout + q] = ((l & 1) ? z.y : z.x) * sc;
+    }
+  } else if (A.kind == P_R2R) {
+    const int sub = A.sub;
+    R* orl = reinterpret_cast<R*>(other);
+    for (int i = tid; i < pairs * 2 * n; i += nt) {
+      const int p = i / (2 * n);
+      const int rem = i - p * 2 * n;
+      const int c = rem / n, k = rem - c * n;
+      if (!A.out_complex && 2 * p + c >= L) continue;
+      R v;
+      switch (sub) {
+        case S_DCT2:
+        case S_DST2: {
+          const int kk = (sub == S_DST2) ? n - 1 - k : k;
+          const C a = res[p * ld + kk];
+          const C b = res[p * ld + (kk == 0 ? 0 : n - kk)];
+          const C V = c ? mk<C, R>((a.y + b.y) * R(0.5), (b.x - a.x) * R(0.5))
+                        : mk<C, R>((a.x + b.x) * R(0.5), (a.y - b.y) * R(0.5));
+          const C w = aux0[kk];
+          v = R(2) * (w.x * V.x - w.y * V.y);
+        } break;
+        case S_DCT3:
+        case S_DST3: {
+          const int idx = (k & 1) ? n - 1 - (k >> 1) : (k >> 1);
+          const C z = res[p * ld + idx];
+          v = c ? z.y : z.x;
+          if (sub == S_DST3 && (k & 1)) v = -v;
+        } break;
+        case S_DCT4:
+        case S_DST4: {
+          const C* U = res + (2 * p + c) * ld;
+          if ((n & 1) == 0) {
+            if ((k & 1) == 0) {
+              const int kk = k >> 1;
+              v = R(2) * cmul(U[kk], aux1[kk]).x;
+            } else {
+              const int kk = (n - 1 - k) >> 1;
+              v = R(-2) * cmul(U[kk], aux1[kk]).y;
+            }
+          } else {
+            v = R(2) * cmul(U[k], aux1[k]).x;
+          }
+          if (sub == S_DST4 && (k & 1)) v = -v;
+        } break;
+        case S_DCT1: {
+          const C z = res[p * ld + k];
+          v = c ? z.y : z.x;
+        } break;
+        case S_DST1: {
+          const C z = res[p * ld + k + 1];
+          v = c ? z.x : -z.y;
+        } break;
+        default: {  // DHT
+          const C a = res[p * ld + k];
+          const C b = res[p * ld + (k == 0 ? 0 : n - k)];
+          const C V = c ? mk<C, R>((a.y + b.y) * R(0.5), (b.x - a.x) * R(0.5))
+                        : mk<C, R>((a.x + b.x) * R(0.5), (a.y - b.y) * R(0.5));
+          v = V.x - V.y;
+        } break;
+      }
+      R f = sc;
+      if (A.post_mode != W_NONE && weight_hit(A.post_mode, k, n)) f *= post_f;
+      v *= f;
+      if (A.out_complex) {
+        if (c)
+          other[p * nout + k].y = v;
+        else
+          other[p * nout + k].x = v;
+      } else {
+        orl[(2 * p + c) * nout + k] = v;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- store: shared -> global (destination layout)
+  const int total_out = L * nout;
+  if (A.out_complex) {
+    C* __restrict__ out = reinterpret_cast<C*>(A.out);
+    const C* src;
+    int row;
+    bool scale_here = false;
+    if (A.kind == P_C2C) {
+      src = res;
+      row = ld;
+      scale_here = true;
+    } else if (A.kind == P_COPY) {
+      src = buf1;
+      row = nin;
+    } else {
+      src = other;
+      row = nout;
+    }
+    if (A.dst_k_contig) {
+      for (int i = tid; i < total_out; i += nt) {
+        const int j = i / nout, k = i - j * nout;
+        C v = src[j * row + k];
+        if (scale_here) v = scl(v, sc);
+        out[dA[k] + (long long)j * dS[k]] = v;
+      }
+    } else {
+      for (int i = tid; i < total_out; i += nt) {
+        const int k = i / L, j = i - k * L;
+        C v = src[j * row + k];
+        if (scale_here) v = scl(v, sc);
+        out[dA[k] + (long long)j * dS[k]] = v;
+      }
+    }
+  } else {
+    R* __restrict__ out = reinterpret_cast<R*>(A.out);
+    const R* src = (A.kind == P_COPY) ? reinterpret_cast<const R*>(buf1) : reinterpret_cast<const R*>(other);
+    const int row = (A.kind == P_COPY) ? nin : nout;
+    if (A.dst_k_contig) {
+      for (int i = tid; i < total_out; i += nt) {
+        const int j = i / nout, k = i - j * nout;
+        out[dA[k] + (long long)j * dS[k]] = src[j * row + k];
+      }
+    } else {
+      for (int i = tid; i < total_out; i += nt) {
+        const int k = i / L, j = i - k * L;
+        out[dA[k] + (long long)j * dS[k]] = src[j * row + k];
+      }
+    }
+  }
+}
+
+size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
+  const size_t cbytes = 2 * (size_t)real_bytes;
+  size_t off = ((size_t)(A.n_in + A.n_out) * 12 + 15) & ~size_t(15);
+  off += (size_t)((A.m + 1) & ~1) * cbytes;
+  off += 2 * (size_t)A.buf_elems * cbytes;
+  return off;
+}
+
+cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  const size_t smem = pass_smem_bytes(A, real_bytes);
+  if (A.ntiles <= 0) return cudaSuccess;
+  if (A.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)A.ntiles);
+  if (real_bytes == 4) {
+    cudaError_t err = cudaFuncSetAttribute(pass_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    pass_kernel<float><<<grid, 256, smem, stream>>>(A);
+  } else {
+    cudaError_t err =
+        cudaFuncSetAttribute(pass_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    pass_kernel<double><<<grid, 256, smem, stream>>>(A);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pb

@@ -1,0 +1,61 @@
+// Argument blocks and launchers of the auxiliary kernels (aux_kernels.cu) and
+// the pass kernel (pass_kernel.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pb_internal.hpp"
+
+namespace pb {
+
+struct RemapArgs {
+  DevPencil src;
+  DevPencil dst;
+  const void* in;
+  void* out;
+  long long total;  // destination elements over all ranks and extras
+  int elem_bytes;
+  int sign[MAXN];
+  long long offset[MAXN];  // reduced into [0, n)
+};
+
+// One contiguous segment of a staging buffer: `extra` blocks of `len`
+// elements, each the region [start, start+ext) in global row-major order.
+struct SegDesc {
+  long long buf_off;
+  long long len;
+  int start[MAXN];
+  int ext[MAXN];
+};
+
+struct SegArgs {
+  DevPencil pen;
+  const SegDesc* segs;
+  int nseg;
+  long long total;
+  int elem_bytes;
+  int to_buffer;  // 1: pack pencil -> buffer, 0: unpack buffer -> pencil
+  const void* pencil_data;
+  void* pencil_out;
+  const void* buffer_in;
+  void* buffer;
+};
+
+struct ExchArgs {
+  const long long* recv_off;  // sorted receive-segment offsets
+  const long long* send_off;  // matching send-segment offsets
+  int nseg;
+  long long total;
+  int elem_bytes;
+  const void* send;
+  void* recv;
+};
+
+cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream);
+size_t pass_smem_bytes(const PassArgs& A, int real_bytes);
+cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream);
+cudaError_t launch_remap(const RemapArgs& A, cudaStream_t stream);
+cudaError_t launch_segments(const SegArgs& A, cudaStream_t stream);
+cudaError_t launch_exchange(const ExchArgs& A, cudaStream_t stream);
+
+}  // namespace pb

@@ -1,0 +1,129 @@
+// Internal types shared by the host plan builder and the CUDA kernels.
+//
+// Data model: a "virtual rank" r of a P_0 x ... x P_{M-1} process grid owns a
+// row-major array [extra..., permuted spatial...] exactly as one MPI rank of
+// the reference does (crates/pencil-array/src/lib.rs:12-19).  A device buffer
+// holds all virtual ranks' arrays concatenated in rank order, so every rank's
+// bytes are identical to the reference's local array on that rank.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <vector_types.h>
+
+#ifdef __CUDACC__
+#define PB_HD __host__ __device__
+#else
+#define PB_HD
+#endif
+
+namespace pb {
+
+constexpr int MAXN = 8;  // spatial dimensions
+constexpr int MAXM = 4;  // process-grid dimensions
+constexpr int MAXSTAGES = 24;
+constexpr int MAXCHUNKS = 4096;
+
+// Local line operation of one pass.
+enum PassKind : int {
+  P_COPY = 0,  // identity stage: layout change only
+  P_C2C = 1,
+  P_R2C = 2,
+  P_C2R = 3,
+  P_R2R = 4,  // sub-kind selects DCT/DST I-IV or DHT
+};
+
+enum R2rSub : int {
+  S_DCT1 = 0, S_DCT2 = 1, S_DCT3 = 2, S_DCT4 = 3,
+  S_DST1 = 4, S_DST2 = 5, S_DST3 = 6, S_DST4 = 7,
+  S_DHT = 8,
+};
+
+// Weight modes: diagonal factors applied to line inputs (pre) or outputs
+// (post); used by the adjoint (VJP) variants.
+enum WeightMode : int {
+  W_NONE = 0,
+  W_FIRST = 1,     // index 0
+  W_LAST = 2,      // index n-1
+  W_INTERIOR = 3,  // indices 1..n-2
+  W_HALF_INTERIOR = 4,  // half-spectrum bins other than DC and (even n) Nyquist
+};
+
+// Device view of one pencil layout over all virtual ranks.
+struct DevPencil {
+  int N;
+  int M;
+  int shape[MAXN];
+  int split[MAXN];        // grid axis splitting spatial axis x, or -1
+  int gdim[MAXM];
+  int rstride[MAXM];      // rank stride of each grid axis (row-major ranks)
+  int perm[MAXN];         // logical axes in memory order
+  int nranks;
+  const long long* info;  // per rank: base, len, start[N], stride[N], extent[N]
+};
+
+PB_HD constexpr int info_words(int N) { return 2 + 3 * N; }
+
+struct PassArgs {
+  int kind;
+  int sub;
+  int n;       // logical line length (real length for R2C/C2R)
+  int n_in;    // elements per input line
+  int n_out;   // elements per output line
+  int m;       // FFT length
+  int a;       // transform axis
+  int b;       // tile axis (lines of one tile differ only in this coordinate)
+  int inv;     // FFT sign: 0 = negative exponent, 1 = positive exponent
+  int in_complex;
+  int out_complex;
+  int nseq_per_line2;  // R2R/R2C/C2R: sequences per two lines (pair model)
+  int pre_mode;
+  int post_mode;
+  double pre_factor;
+  double post_factor;
+  double scale;
+  int src_k_contig;  // transform axis has unit stride in the source
+  int dst_k_contig;  // transform axis has unit stride in the destination
+  int nstages;
+  int radix[MAXSTAGES];
+  int ld;          // leading dimension (complex units) of a sequence in smem
+  int buf_elems;   // complex units per smem ping-pong buffer
+  int lines;       // lines per tile (max)
+  // tile enumeration
+  int nchunks;
+  const int2* chunks;  // (b0, count) chunks along the tile axis
+  int nouter_axes;
+  int outer_axis[MAXN];
+  int outer_ext[MAXN];
+  long long extra;
+  long long ntiles;
+  DevPencil src;
+  DevPencil dst;
+  const void* in;
+  void* out;
+  const void* twiddle;  // m roots exp(-2 pi i q/m), rounded to the plan type
+  const void* aux0;     // kind-specific pre/post twiddles
+  const void* aux1;
+  const int* gate;      // if non-null and nonzero: spectrum rejected, write nothing
+};
+
+// Endpoint statistics of the C2R boundary (distributed/r2c.rs:4709-4807).
+struct StatsArgs {
+  DevPencil pen;
+  const void* data;  // complex plane data in pencil layout
+  int red_axis;
+  int real_len;
+  int nplanes;       // 1 (odd n) or 2
+  long long extra;
+  long long plane_points;  // product of the other axes' extents
+  int other_axes[MAXN];
+  int other_ext[MAXN];
+  int nother;
+  double* acc;       // per (batch, plane): [max_all, max_im, sum_re, sum_im]
+  int* status;       // [0]: 1 if any plane rejected; [1]: 1 if a value was not finite
+  double relative;
+  double absolute;
+};
+
+}  // namespace pb

@@ -1,0 +1,1838 @@
+// Host side of the library: pencil geometry, canonical routes, plan families,
+// per-operation pass programs, device tables and the C-ABI entry points.
+//
+// Geometry and routes restate the reference (nogaki/pencil-rs):
+//   floor partition           crates/pencil-array/src/geometry.rs:9-59
+//   pencil local shapes       crates/pencil-array/src/pencil.rs:69-112, axis.rs:104-115
+//   rank <-> coordinates      crates/pencil-array/src/topology.rs:25-46 (reorder=false)
+//   canonical route           crates/pencil-fft/src/distributed.rs:2306-2382
+//   R2C / C2R stage lists     crates/pencil-fft/src/distributed/r2c.rs:1204-1535,
+//                             crates/pencil-fft/src/distributed/c2r.rs:193-222
+//   mixed graphs              crates/pencil-fft/src/distributed/mixed.rs:1602-1626
+//   endpoint thresholds       crates/pencil-fft/src/distributed/r2c.rs:4841-4878 and
+//                             the MixedR2cPlan contract (distributed/mixed.rs:350-380)
+// Each stage becomes one fused pass (pass_kernel.cu) that writes straight into
+// the layout of the next transforming stage; identity stages cost nothing
+// beyond the composed layout change.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pb_aux.hpp"
+#include "pencil_b200.h"
+
+namespace pb {
+
+struct PbError {
+  int code;
+};
+[[noreturn]] static void fail(int code) { throw PbError{code}; }
+static void cuda_ok(cudaError_t e) {
+  if (e != cudaSuccess) fail(PB_ECUDA);
+}
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+struct Pencil {
+  int N = 0, M = 0;
+  long long shape[MAXN] = {};
+  int grid[MAXM] = {};
+  int dec[MAXM] = {};
+  int perm[MAXN] = {};
+
+  int nranks() const {
+    int s = 1;
+    for (int t = 0; t < M; ++t) s *= grid[t];
+    return s;
+  }
+  void coords(int r, int* c) const {
+    for (int t = M - 1; t >= 0; --t) {
+      c[t] = r % grid[t];
+      r /= grid[t];
+    }
+  }
+  int split_of(int axis) const {
+    for (int t = 0; t < M; ++t)
+      if (dec[t] == axis) return t;
+    return -1;
+  }
+  int mem_pos(int axis) const {
+    for (int q = 0; q < N; ++q)
+      if (perm[q] == axis) return q;
+    return -1;
+  }
+  static long long part(long long n, long long P, long long c) { return (n * c) / P; }
+  void local(int r, long long* lo, long long* ext) const {
+    int c[MAXM];
+    coords(r, c);
+    for (int x = 0; x < N; ++x) {
+      lo[x] = 0;
+      ext[x] = shape[x];
+    }
+    for (int t = 0; t < M; ++t) {
+      const int ax = dec[t];
+      lo[ax] = part(shape[ax], grid[t], c[t]);
+      ext[ax] = part(shape[ax], grid[t], c[t] + 1) - lo[ax];
+    }
+  }
+  long long local_len(int r) const {
+    long long lo[MAXN], ext[MAXN];
+    local(r, lo, ext);
+    long long s = 1;
+    for (int x = 0; x < N; ++x) s *= ext[x];
+    return s;
+  }
+  long long total(long long extra) const {
+    long long s = 0;
+    for (int r = 0; r < nranks(); ++r) s += local_len(r) * extra;
+    return s;
+  }
+  bool same_distribution(const Pencil& o) const {
+    if (N != o.N || M != o.M) return false;
+    for (int x = 0; x < N; ++x)
+      if (shape[x] != o.shape[x]) return false;
+    for (int t = 0; t < M; ++t)
+      if (grid[t] != o.grid[t] || dec[t] != o.dec[t]) return false;
+    return true;
+  }
+  bool same_layout(const Pencil& o) const {
+    if (!same_distribution(o)) return false;
+    for (int x = 0; x < N; ++x)
+      if (perm[x] != o.perm[x]) return false;
+    return true;
+  }
+};
+
+static void validate_pencil(const Pencil& p) {
+  if (p.N < 1 || p.N > MAXN || p.M < 1 || p.M > MAXM || p.M > p.N) fail(PB_EINVALID_DIMENSIONS);
+  for (int x = 0; x < p.N; ++x) {
+    if (p.shape[x] <= 0) fail(PB_EZERO_EXTENT);
+    if (p.shape[x] > INT_MAX / 2) fail(PB_EUNSUPPORTED);
+  }
+  long long ranks = 1;
+  for (int t = 0; t < p.M; ++t) {
+    if (p.grid[t] <= 0) fail(PB_EINVALID_ARGUMENT);
+    ranks *= p.grid[t];
+    if (ranks > (1 << 20)) fail(PB_EUNSUPPORTED);
+  }
+  bool seen[MAXN] = {};
+  for (int t = 0; t < p.M; ++t) {
+    if (p.dec[t] < 0 || p.dec[t] >= p.N || seen[p.dec[t]]) fail(PB_EINVALID_DECOMPOSITION);
+    seen[p.dec[t]] = true;
+  }
+  bool pseen[MAXN] = {};
+  for (int q = 0; q < p.N; ++q) {
+    if (p.perm[q] < 0 || p.perm[q] >= p.N || pseen[p.perm[q]]) fail(PB_EINVALID_PERMUTATION);
+    pseen[p.perm[q]] = true;
+  }
+}
+
+static Pencil pencil_from_desc(const pb_pencil_desc* d) {
+  if (!d) fail(PB_ENULL);
+  Pencil p;
+  p.N = d->ndim;
+  p.M = d->ngrid;
+  if (p.N < 1 || p.N > MAXN || p.M < 1 || p.M > MAXM) fail(PB_EINVALID_DIMENSIONS);
+  for (int x = 0; x < p.N; ++x) {
+    p.shape[x] = d->shape[x];
+    p.perm[x] = d->permutation[x];
+  }
+  for (int t = 0; t < p.M; ++t) {
+    p.grid[t] = d->grid[t];
+    p.dec[t] = d->decomposition[t];
+  }
+  validate_pencil(p);
+  return p;
+}
+
+static void pencil_to_desc(const Pencil& p, pb_pencil_desc* d) {
+  std::memset(d, 0, sizeof(*d));
+  d->ndim = p.N;
+  d->ngrid = p.M;
+  for (int x = 0; x < p.N; ++x) {
+    d->shape[x] = p.shape[x];
+    d->permutation[x] = p.perm[x];
+  }
+  for (int t = 0; t < p.M; ++t) {
+    d->grid[t] = p.grid[t];
+    d->decomposition[t] = p.dec[t];
+  }
+}
+
+// Canonical input pencil: decomposition [0..M), identity memory order.
+static Pencil canonical(const pb_geom* g, const int64_t* shape) {
+  Pencil p;
+  p.N = g->ndim;
+  p.M = g->ngrid;
+  for (int x = 0; x < p.N; ++x) {
+    p.shape[x] = shape[x];
+    p.perm[x] = x;
+  }
+  for (int t = 0; t < p.M; ++t) {
+    p.grid[t] = g->grid[t];
+    p.dec[t] = t;
+  }
+  return p;
+}
+
+// build_route (distributed.rs:2306-2382) with advance_decomposition (2375-2382).
+static std::vector<Pencil> build_route(const Pencil& input, bool permute, std::vector<int>* distributed) {
+  const int N = input.N;
+  std::vector<Pencil> stages{input};
+  Pencil cur = input;
+  for (int axis = N - 2; axis >= 0; --axis) {
+    Pencil nxt = cur;
+    int pos = 0;
+    for (int q = 0; q < N; ++q)
+      if (cur.perm[q] != axis) nxt.perm[pos++] = cur.perm[q];
+    nxt.perm[N - 1] = axis;
+    bool dist = false;
+    for (int t = 0; t < cur.M; ++t)
+      if (cur.dec[t] == axis) {
+        nxt.dec[t] = axis + 1;
+        dist = true;
+      }
+    if (!permute)
+      for (int q = 0; q < N; ++q) nxt.perm[q] = q;
+    if (distributed) distributed->push_back(dist ? 1 : 0);
+    stages.push_back(nxt);
+    cur = nxt;
+  }
+  return stages;
+}
+
+static void validate_geom(const pb_geom* g) {
+  if (!g) fail(PB_ENULL);
+  if (g->ndim < 2 || g->ndim > MAXN || g->ngrid < 1 || g->ngrid >= g->ndim || g->ngrid > MAXM)
+    fail(PB_EINVALID_DIMENSIONS);
+  for (int x = 0; x < g->ndim; ++x) {
+    if (g->shape[x] <= 0) fail(PB_EZERO_EXTENT);
+    if (g->shape[x] > INT_MAX / 2) fail(PB_EUNSUPPORTED);
+  }
+  for (int t = 0; t < g->ngrid; ++t)
+    if (g->grid[t] <= 0) fail(PB_EINVALID_ARGUMENT);
+  if (g->extra_ndim < 0 || g->extra_ndim > MAXN) fail(PB_EINVALID_ARGUMENT);
+  for (int i = 0; i < g->extra_ndim; ++i)
+    if (g->extra[i] < 0) fail(PB_EINVALID_ARGUMENT);
+}
+
+static long long extra_count(const pb_geom* g) {
+  long long e = 1;
+  for (int i = 0; i < g->extra_ndim; ++i) {
+    e *= g->extra[i];
+    if (e > (1LL << 40)) fail(PB_EUNSUPPORTED);
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// stages and plans
+// ---------------------------------------------------------------------------
+enum StageKind { SK_ID = 0, SK_C2C = 1, SK_R2C = 2, SK_R2R = 3 };
+
+struct Stage {
+  int axis = 0;
+  Pencil in, out;
+  int kind = SK_ID;
+  int sub = 0;  // R2rSub for SK_R2R (DHT included)
+  bool positive = false;
+  bool real_in = false;
+  bool real_out = false;
+};
+
+// Internal program modes.  F/B/I are the reference's forward / raw backward /
+// normalised inverse; FS is forward with the inverse's per-axis normalisation
+// (C2rPlan::inverse); A* are the adjoints of F, FS, B, I.
+enum Mode { M_F = 0, M_FS, M_B, M_I, M_AF, M_AFS, M_AB, M_AI, M_COUNT };
+
+struct Step {
+  int type = 0;  // 0 pass, 1 endpoint statistics
+  PassArgs pa{};
+  StatsArgs sa{};
+  int src_slot = 0;  // -1 caller input, -2 caller output, 0/1 workspace buffers
+  int dst_slot = 0;
+};
+
+struct Program {
+  std::vector<Step> steps;
+  bool has_stats = false;
+};
+
+struct HostArena {
+  std::vector<unsigned char> bytes;
+  size_t add(const void* data, size_t n) {
+    size_t off = (bytes.size() + 255) & ~size_t(255);
+    bytes.resize(off + n);
+    if (n) std::memcpy(bytes.data() + off, data, n);
+    return off;
+  }
+};
+
+// pointers inside PassArgs/StatsArgs are stored as (arena offset + 1) until upload
+static const void* enc(size_t off) { return reinterpret_cast<const void*>(off + 1); }
+
+}  // namespace pb
+
+struct pb_plan {
+  int real_bytes = 4;
+  bool c2r_family = false;
+  std::vector<pb::Stage> stages;
+  int boundary = -1;
+  long long real_len = 0;
+  std::vector<std::array<double, 3>> terms;  // complex-suffix (E_a, allowance_a, factor_a)
+  long long extra = 1;
+  pb::Pencil fin, fout;
+  bool fin_complex = true, fout_complex = true;
+  pb::Program prog[pb::M_COUNT];
+  pb::HostArena host;
+  std::map<std::string, size_t> cache;
+  void* arena = nullptr;
+  size_t buf_bytes = 0;
+  size_t status_off = 0, acc_off = 0, ws_bytes = 0;
+  int max_smem = 227 * 1024;
+  ~pb_plan() {
+    if (arena) cudaFree(arena);
+  }
+};
+
+namespace pb {
+
+static std::string pencil_key(const Pencil& p, long long extra) {
+  std::string k = "P";
+  for (int x = 0; x < p.N; ++x) k += std::to_string(p.shape[x]) + "," + std::to_string(p.perm[x]) + ";";
+  for (int t = 0; t < p.M; ++t) k += std::to_string(p.grid[t]) + "," + std::to_string(p.dec[t]) + ";";
+  return k + "e" + std::to_string(extra);
+}
+
+// DevPencil with its rank table (base, len, start, stride, extent per rank).
+static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size_t>& cache, const Pencil& p,
+                            long long extra) {
+  DevPencil d{};
+  d.N = p.N;
+  d.M = p.M;
+  for (int x = 0; x < p.N; ++x) {
+    d.shape[x] = (int)p.shape[x];
+    d.split[x] = p.split_of(x);
+    d.perm[x] = p.perm[x];
+  }
+  int rs = 1;
+  for (int t = p.M - 1; t >= 0; --t) {
+    d.gdim[t] = p.grid[t];
+    d.rstride[t] = rs;
+    rs *= p.grid[t];
+  }
+  d.nranks = p.nranks();
+  const std::string key = pencil_key(p, extra);
+  auto it = cache.find(key);
+  size_t off;
+  if (it != cache.end()) {
+    off = it->second;
+  } else {
+    const int w = info_words(p.N);
+    std::vector<long long> info((size_t)d.nranks * w);
+    long long base = 0;
+    for (int r = 0; r < d.nranks; ++r) {
+      long long lo[MAXN], ext[MAXN];
+      p.local(r, lo, ext);
+      long long len = 1;
+      for (int x = 0; x < p.N; ++x) len *= ext[x];
+      long long* row = &info[(size_t)r * w];
+      row[0] = base;
+      row[1] = len;
+      long long stride = 1;
+      for (int q = p.N - 1; q >= 0; --q) {
+        const int ax = p.perm[q];
+        row[2 + p.N + ax] = stride;
+        stride *= ext[ax];
+      }
+      for (int x = 0; x < p.N; ++x) {
+        row[2 + x] = lo[x];
+        row[2 + 2 * p.N + x] = ext[x];
+        if (row[2 + p.N + x] > INT_MAX) fail(PB_EUNSUPPORTED);
+      }
+      base += len * extra;
+    }
+    off = A.add(info.data(), info.size() * sizeof(long long));
+    cache[key] = off;
+  }
+  (void)P;
+  d.info = reinterpret_cast<const long long*>(enc(off));
+  return d;
+}
+
+// exp(-2 pi i q/m) (negative exponent) in extended precision, rounded once.
+static size_t roots_table(pb_plan& P, int m) {
+  const std::string key = "W" + std::to_string(m) + "r" + std::to_string(P.real_bytes);
+  auto it = P.cache.find(key);
+  if (it != P.cache.end()) return it->second;
+  const long double pi = 3.14159265358979323846264338327950288L;
+  std::vector<double> d(2 * (size_t)m);
+  for (int q = 0; q < m; ++q) {
+    const long double th = -2.0L * pi * (long double)q / (long double)m;
+    d[2 * q] = (double)cosl(th);
+    d[2 * q + 1] = (double)sinl(th);
+  }
+  size_t off;
+  if (P.real_bytes == 4) {
+    std::vector<float> f(d.begin(), d.end());
+    off = P.host.add(f.data(), f.size() * sizeof(float));
+  } else {
+    off = P.host.add(d.data(), d.size() * sizeof(double));
+  }
+  P.cache[key] = off;
+  return off;
+}
+
+// exp(i * pi * (num_scale*k + num_off) / den) for k < count, rounded once.
+static size_t phase_table(pb_plan& P, int count, long double ks, long double k0, long double den) {
+  const std::string key = "A" + std::to_string(count) + "_" + std::to_string((double)ks) + "_" +
+                          std::to_string((double)k0) + "_" + std::to_string((double)den) + "r" +
+                          std::to_string(P.real_bytes);
+  auto it = P.cache.find(key);
+  if (it != P.cache.end()) return it->second;
+  const long double pi = 3.14159265358979323846264338327950288L;
+  std::vector<double> d(2 * (size_t)count);
+  for (int k = 0; k < count; ++k) {
+    const long double th = pi * (ks * (long double)k + k0) / den;
+    d[2 * k] = (double)cosl(th);
+    d[2 * k + 1] = (double)sinl(th);
+  }
+  size_t off;
+  if (P.real_bytes == 4) {
+    std::vector<float> f(d.begin(), d.end());
+    off = P.host.add(f.data(), f.size() * sizeof(float));
+  } else {
+    off = P.host.add(d.data(), d.size() * sizeof(double));
+  }
+  P.cache[key] = off;
+  return off;
+}
+
+static std::vector<int> radices(int m) {
+  std::vector<int> r;
+  while (m % 8 == 0) {
+    r.push_back(8);
+    m /= 8;
+  }
+  if (m % 4 == 0) {
+    r.push_back(4);
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    r.push_back(2);
+    m /= 2;
+  }
+  for (int p : {3, 5, 7}) {
+    while (m % p == 0) {
+      r.push_back(p);
+      m /= p;
+    }
+  }
+  for (int p = 11; (long long)p * p <= m; p += 2) {
+    while (m % p == 0) {
+      r.push_back(p);
+      m /= p;
+    }
+  }
+  if (m > 1) r.push_back(m);
+  if ((int)r.size() > MAXSTAGES) fail(PB_EUNSUPPORTED);
+  return r;
+}
+
+static int fft_len(int kind, int sub, int n) {
+  switch (kind) {
+    case P_COPY: return 1;
+    case P_C2C:
+    case P_R2C:
+    case P_C2R: return n;
+    default: break;
+  }
+  switch (sub) {
+    case S_DCT4:
+    case S_DST4: return (n % 2 == 0) ? n / 2 : 2 * n;
+    case S_DCT1: return 2 * (n - 1);
+    case S_DST1: return 2 * (n + 1);
+    default: return n;
+  }
+}
+
+struct LocalOp {
+  int kind = P_COPY;
+  int sub = 0;
+  int inv = 0;
+  double scale = 1.0;
+  int pre_mode = W_NONE, post_mode = W_NONE;
+  double pre_f = 1.0, post_f = 1.0;
+  bool gated = false;
+};
+
+static int backward_sub(int s) {
+  switch (s) {
+    case S_DCT2: return S_DCT3;
+    case S_DCT3: return S_DCT2;
+    case S_DST2: return S_DST3;
+    case S_DST3: return S_DST2;
+    default: return s;  // types I, IV and the DHT are self-paired (r2r.rs:67-78)
+  }
+}
+
+// (model length E_a, normalisation factor) of an R2R kind (r2r.rs:798-848; DHT n, n).
+static std::pair<long long, long long> r2r_lengths(int sub, long long n) {
+  switch (sub) {
+    case S_DCT1: return {2 * (n - 1), 2 * (n - 1)};
+    case S_DST1: return {2 * (n + 1), 2 * (n + 1)};
+    case S_DCT4:
+    case S_DST4: return {8 * n, 2 * n};
+    case S_DHT: return {n, n};
+    default: return {4 * n, 2 * n};
+  }
+}
+
+static void r2r_local(LocalOp& op, int sub, bool adjoint) {
+  op.kind = P_R2R;
+  op.sub = sub;
+  if (adjoint) {
+    switch (sub) {
+      case S_DCT1:
+        op.pre_mode = W_INTERIOR;
+        op.pre_f = 0.5;
+        op.post_mode = W_INTERIOR;
+        op.post_f = 2.0;
+        break;
+      case S_DCT2:
+        op.sub = S_DCT3;
+        op.pre_mode = W_FIRST;
+        op.pre_f = 2.0;
+        break;
+      case S_DCT3:
+        op.sub = S_DCT2;
+        op.post_mode = W_FIRST;
+        op.post_f = 0.5;
+        break;
+      case S_DST2:
+        op.sub = S_DST3;
+        op.pre_mode = W_LAST;
+        op.pre_f = 2.0;
+        break;
+      case S_DST3:
+        op.sub = S_DST2;
+        op.post_mode = W_LAST;
+        op.post_f = 0.5;
+        break;
+      default: break;
+    }
+  }
+  op.inv = (op.sub == S_DCT3 || op.sub == S_DST3) ? 1 : 0;
+}
+
+static LocalOp local_op(const Stage& st, int mode, long long n_axis) {
+  LocalOp op;
+  const bool scaled = (mode == M_FS || mode == M_I || mode == M_AFS || mode == M_AI);
+  switch (st.kind) {
+    case SK_ID: op.kind = P_COPY; return op;
+    case SK_C2C: {
+      op.kind = P_C2C;
+      const bool fwd_sign_positive = st.positive;
+      bool positive;
+      switch (mode) {
+        case M_F:
+        case M_FS:
+        case M_AB:
+        case M_AI: positive = fwd_sign_positive; break;
+        default: positive = !fwd_sign_positive; break;
+      }
+      op.inv = positive ? 1 : 0;
+      if (scaled) op.scale = 1.0 / (double)n_axis;
+      return op;
+    }
+    case SK_R2C: {
+      const long long n = n_axis;  // real length
+      switch (mode) {
+        case M_F:
+        case M_FS: op.kind = P_R2C; break;
+        case M_B:
+        case M_I:
+          op.kind = P_C2R;
+          op.inv = 1;
+          op.gated = true;
+          break;
+        case M_AF:
+        case M_AFS:
+          op.kind = P_C2R;
+          op.inv = 1;
+          op.pre_mode = W_HALF_INTERIOR;
+          op.pre_f = 0.5;
+          break;
+        default:  // M_AB, M_AI: adjoint of C2R
+          op.kind = P_R2C;
+          op.post_mode = W_HALF_INTERIOR;
+          op.post_f = 2.0;
+          break;
+      }
+      if (scaled) op.scale = 1.0 / (double)n;
+      return op;
+    }
+    default: {  // SK_R2R (DHT included)
+      int sub = st.sub;
+      bool adjoint = false;
+      switch (mode) {
+        case M_F:
+        case M_FS: break;
+        case M_B:
+        case M_I: sub = backward_sub(sub); break;
+        case M_AF:
+        case M_AFS: adjoint = true; break;
+        default:
+          sub = backward_sub(sub);
+          adjoint = true;
+          break;
+      }
+      r2r_local(op, sub, adjoint);
+      if (scaled) op.scale = 1.0 / (double)r2r_lengths(st.sub, n_axis).second;
+      if (st.sub == S_DHT && n_axis == 1) {
+        op.kind = P_COPY;  // the length-one DHT is a bit copy (dht.rs:213-217)
+      }
+      return op;
+    }
+  }
+}
+
+static int choose_lines(pb_plan& P, PassArgs& A, int pair_kind) {
+  const int cb = 2 * P.real_bytes;
+  const int big = std::max(std::max(A.n_in, A.n_out), A.m);
+  int L = std::max(1, std::min(64, 8192 / std::max(1, big)));
+  if (pair_kind && L > 1 && (L & 1)) --L;
+  const size_t budget = (size_t)std::min(P.max_smem, 112 * 1024);
+  for (;;) {
+    const int pairs = (A.kind == P_R2R && A.in_complex) ? L : (L + 1) / 2;
+    int nseq = L;
+    if (A.kind == P_R2C || A.kind == P_C2R) nseq = pairs;
+    if (A.kind == P_R2R) nseq = (A.sub == S_DCT4 || A.sub == S_DST4) ? 2 * pairs : pairs;
+    long long st_units = A.in_complex ? (long long)L * A.n_in : ((long long)L * A.n_in + 1) / 2;
+    long long out_units = A.out_complex ? (long long)L * A.n_out : ((long long)L * A.n_out + 1) / 2;
+    long long fft_units = (A.kind == P_COPY) ? 0 : (long long)nseq * A.ld;
+    if (A.kind == P_C2C) fft_units = (long long)L * A.ld;
+    A.buf_elems = (int)std::max(std::max(st_units, out_units), fft_units);
+    A.buf_elems = (A.buf_elems + 1) & ~1;
+    A.lines = L;
+    const size_t bytes = pass_smem_bytes(A, P.real_bytes);
+    if (bytes <= budget || (L == 1 && bytes <= (size_t)P.max_smem)) return L;
+    if (L == 1) fail(PB_EUNSUPPORTED);
+    L = (L > 2 && pair_kind) ? ((L / 2) & ~1) : L / 2;
+    if (L < 1) L = 1;
+    (void)cb;
+  }
+}
+
+// One fused pass for `st` under `op` from layout `src` to layout `dst`.
+static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Pencil& src, const Pencil& dst,
+                      bool in_complex, bool out_complex) {
+  Step s;
+  PassArgs& A = s.pa;
+  A = PassArgs{};
+  const int N = src.N;
+  const int a = st.axis;
+  A.kind = op.kind;
+  A.sub = op.sub;
+  A.inv = op.inv;
+  A.scale = op.scale;
+  A.pre_mode = op.pre_mode;
+  A.pre_factor = op.pre_f;
+  A.post_mode = op.post_mode;
+  A.post_factor = op.post_f;
+  A.a = a;
+  A.n_in = (int)src.shape[a];
+  A.n_out = (int)dst.shape[a];
+  A.n = (op.kind == P_R2C) ? A.n_in : (op.kind == P_C2R) ? A.n_out : A.n_in;
+  A.in_complex = in_complex ? 1 : 0;
+  A.out_complex = out_complex ? 1 : 0;
+  A.m = fft_len(op.kind, op.sub, A.n);
+  if (A.m > (1 << 20)) fail(PB_EUNSUPPORTED);
+  if (op.kind != P_COPY) {
+    auto r = radices(A.m);
+    A.nstages = (int)r.size();
+    for (int i = 0; i < A.nstages; ++i) A.radix[i] = r[i];
+    A.twiddle = enc(roots_table(P, A.m));
+  } else {
+    A.nstages = 0;
+    A.twiddle = nullptr;
+  }
+  A.ld = A.m + ((A.m % 8 == 0) ? 1 : 0);
+  if (op.kind == P_COPY) A.ld = 1;
+  // kind-specific twiddles (exp(i*pi*(ks*k+k0)/den))
+  if (op.kind == P_R2R) {
+    const int n = A.n;
+    switch (op.sub) {
+      case S_DCT2:
+      case S_DST2: A.aux0 = enc(phase_table(P, n, -1, 0, 2.0L * n)); break;
+      case S_DCT3:
+      case S_DST3: A.aux0 = enc(phase_table(P, n, 1, 0, 2.0L * n)); break;
+      case S_DCT4:
+      case S_DST4:
+        if (n % 2 == 0) {
+          A.aux0 = enc(phase_table(P, n / 2, -4, -1, 4.0L * n));
+          A.aux1 = enc(phase_table(P, n / 2, -1, 0, (long double)n));
+        } else {
+          A.aux0 = enc(phase_table(P, n, -2, -1, 4.0L * n));
+          A.aux1 = enc(phase_table(P, n, -1, 0, 2.0L * n));
+        }
+        break;
+      default: break;
+    }
+  }
+  // tile axis: contiguous in the destination if possible, else in the source
+  int b = dst.perm[N - 1];
+  if (b == a) b = src.perm[N - 1];
+  if (b == a) b = dst.perm[N - 2];
+  A.b = b;
+  A.src_k_contig = (src.perm[N - 1] == a) ? 1 : 0;
+  A.dst_k_contig = (dst.perm[N - 1] == a) ? 1 : 0;
+  const bool pair_kind = (op.kind == P_R2C || op.kind == P_C2R || (op.kind == P_R2R && !in_complex));
+  const int L = choose_lines(P, A, pair_kind ? 1 : 0);
+  // chunks of the tile axis, split at both partitions of axis b
+  std::vector<long long> cuts{0, src.shape[b]};
+  for (const Pencil* p : {&src, &dst}) {
+    const int t = p->split_of(b);
+    if (t >= 0)
+      for (int c = 1; c < p->grid[t]; ++c) cuts.push_back(Pencil::part(p->shape[b], p->grid[t], c));
+  }
+  std::sort(cuts.begin(), cuts.end());
+  cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+  std::vector<int2> chunks;
+  for (size_t i = 0; i + 1 < cuts.size(); ++i)
+    for (long long j = cuts[i]; j < cuts[i + 1]; j += L) {
+      int2 c;
+      c.x = (int)j;
+      c.y = (int)std::min<long long>(L, cuts[i + 1] - j);
+      chunks.push_back(c);
+    }
+  A.nchunks = (int)chunks.size();
+  A.chunks = reinterpret_cast<const int2*>(enc(P.host.add(chunks.data(), chunks.size() * sizeof(int2))));
+  A.nouter_axes = 0;
+  long long tiles = (long long)chunks.size() * P.extra;
+  for (int x = 0; x < N; ++x) {
+    if (x == a || x == b) continue;
+    A.outer_axis[A.nouter_axes] = x;
+    A.outer_ext[A.nouter_axes] = (int)src.shape[x];
+    ++A.nouter_axes;
+    tiles *= src.shape[x];
+  }
+  A.extra = P.extra;
+  A.ntiles = tiles;
+  A.src = dev_pencil(P, P.host, P.cache, src, P.extra);
+  A.dst = dev_pencil(P, P.host, P.cache, dst, P.extra);
+  return s;
+}
+
+static double ceil_log2(long long n) {
+  if (n <= 1) return 0.0;
+  int b = 0;
+  long long v = n - 1;
+  while (v > 0) {
+    ++b;
+    v >>= 1;
+  }
+  return (double)b;
+}
+
+static Step make_stats(pb_plan& P, const Pencil& pen, int red_axis, bool normalize) {
+  Step s;
+  s.type = 1;
+  StatsArgs& S = s.sa;
+  S = StatsArgs{};
+  S.pen = dev_pencil(P, P.host, P.cache, pen, P.extra);
+  S.red_axis = red_axis;
+  S.real_len = (int)P.real_len;
+  S.nplanes = (P.real_len % 2 == 0) ? 2 : 1;
+  S.extra = P.extra;
+  S.nother = 0;
+  long long pts = 1;
+  for (int x = 0; x < pen.N; ++x) {
+    if (x == red_axis) continue;
+    S.other_axes[S.nother] = x;
+    S.other_ext[S.nother] = (int)pen.shape[x];
+    ++S.nother;
+    pts *= pen.shape[x];
+  }
+  S.plane_points = pts;
+  // thresholds: distributed/r2c.rs:4841-4878, distributed/mixed.rs (MixedR2cPlan contract)
+  double depth = 1.0, factor = 1.0;
+  for (auto& t : P.terms) {
+    depth += ceil_log2((long long)t[0]) + t[1];
+    factor *= t[2];
+  }
+  const double eps = P.real_bytes == 4 ? (double)FLT_EPSILON : DBL_EPSILON;
+  const double tiny = P.real_bytes == 4 ? (double)std::ldexp(1.0f, -149) : std::ldexp(1.0, -1074);
+  S.relative = 128.0 * eps * depth;
+  const double inv_abs = 128.0 * tiny * depth;
+  S.absolute = normalize ? inv_abs : inv_abs * factor;
+  return s;
+}
+
+static void build_program(pb_plan& P, int mode) {
+  Program& prog = P.prog[mode];
+  prog.steps.clear();
+  const int N = (int)P.stages.size();
+  const bool fwd = (mode == M_F || mode == M_FS || mode == M_AB || mode == M_AI);
+  std::vector<int> order;
+  for (int i = 0; i < N; ++i) order.push_back(fwd ? i : N - 1 - i);
+  std::vector<int> active;
+  for (int i : order) {
+    const Stage& st = P.stages[i];
+    LocalOp op = local_op(st, mode, fwd ? st.in.shape[st.axis] : st.in.shape[st.axis]);
+    if (st.kind != SK_ID) active.push_back(i);
+  }
+  const Pencil& start = fwd ? P.fin : P.fout;
+  const Pencil& end = fwd ? P.fout : P.fin;
+  bool cur_complex = fwd ? P.fin_complex : P.fout_complex;
+  const bool end_complex = fwd ? P.fout_complex : P.fin_complex;
+  if (active.empty()) {
+    Stage id;
+    id.axis = end.perm[N - 1];
+    LocalOp op;
+    Step s = make_pass(P, id, op, start, end, cur_complex, end_complex);
+    s.src_slot = -1;
+    s.dst_slot = -2;
+    prog.steps.push_back(s);
+    return;
+  }
+  Pencil cur = start;
+  const int npass = (int)active.size();
+  for (int k = 0; k < npass; ++k) {
+    const Stage& st = P.stages[active[k]];
+    Pencil dst;
+    bool dst_complex;
+    if (k + 1 == npass) {
+      dst = end;
+      dst_complex = end_complex;
+    } else {
+      const Stage& nx = P.stages[active[k + 1]];
+      dst = fwd ? nx.in : nx.out;
+      dst_complex = fwd ? !nx.real_in : !nx.real_out;
+    }
+    // logical line length of the stage (real length for the R2C boundary)
+    const long long n_axis = (st.kind == SK_R2C) ? P.real_len : st.in.shape[st.axis];
+    LocalOp op = local_op(st, mode, n_axis);
+    if (op.gated) {
+      prog.steps.push_back(make_stats(P, cur, st.axis, mode == M_I));
+      prog.steps.back().src_slot = (k == 0) ? -1 : (k - 1) % 2;
+      prog.has_stats = true;
+    }
+    Step s = make_pass(P, st, op, cur, dst, cur_complex, dst_complex);
+    if (op.gated) s.pa.gate = reinterpret_cast<const int*>(1);  // resolved at execute time
+    s.src_slot = (k == 0) ? -1 : (k - 1) % 2;
+    s.dst_slot = (k + 1 == npass) ? -2 : k % 2;
+    if (s.dst_slot >= 0) {
+      const size_t bytes = (size_t)dst.total(P.extra) * (size_t)P.real_bytes * (dst_complex ? 2 : 1);
+      P.buf_bytes = std::max(P.buf_bytes, bytes);
+    }
+    prog.steps.push_back(s);
+    cur = dst;
+    cur_complex = dst_complex;
+  }
+  // every pass after a spectrum check must honour its verdict
+  bool gated = false;
+  for (auto& s : prog.steps) {
+    if (s.type == 1) gated = true;
+    if (s.type == 0 && gated) s.pa.gate = reinterpret_cast<const int*>(1);
+  }
+}
+
+static void finalize(pb_plan& P) {
+  int dev = 0;
+  cuda_ok(cudaGetDevice(&dev));
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+    P.max_smem = optin;
+  for (int m = 0; m < M_COUNT; ++m) build_program(P, m);
+  // upload tables
+  if (!P.host.bytes.empty()) {
+    cuda_ok(cudaMalloc(&P.arena, P.host.bytes.size()));
+    cuda_ok(cudaMemcpy(P.arena, P.host.bytes.data(), P.host.bytes.size(), cudaMemcpyHostToDevice));
+  }
+  const uintptr_t base = reinterpret_cast<uintptr_t>(P.arena);
+  auto fix = [&](const void*& p) {
+    if (p != nullptr) p = reinterpret_cast<const void*>(base + reinterpret_cast<uintptr_t>(p) - 1);
+  };
+  auto fixpen = [&](DevPencil& d) {
+    const void* v = d.info;
+    fix(v);
+    d.info = reinterpret_cast<const long long*>(v);
+  };
+  for (int m = 0; m < M_COUNT; ++m)
+    for (auto& s : P.prog[m].steps) {
+      if (s.type == 0) {
+        const void* c = s.pa.chunks;
+        fix(c);
+        s.pa.chunks = reinterpret_cast<const int2*>(c);
+        fix(s.pa.twiddle);
+        fix(s.pa.aux0);
+        fix(s.pa.aux1);
+        fixpen(s.pa.src);
+        fixpen(s.pa.dst);
+      } else {
+        fixpen(s.sa.pen);
+      }
+    }
+  // workspace: two intermediate buffers, then status words and statistics
+  const size_t buf = (P.buf_bytes + 255) & ~size_t(255);
+  P.buf_bytes = buf;
+  P.status_off = 2 * buf;
+  P.acc_off = P.status_off + 256;
+  const size_t acc = (size_t)std::max<long long>(P.extra, 1) * 2 * 4 * sizeof(double);
+  P.ws_bytes = P.acc_off + ((acc + 255) & ~size_t(255));
+}
+
+static void stage_fill(Stage& s, int axis, const Pencil& in, const Pencil& out, int kind, int sub, bool positive,
+                       bool real_in, bool real_out) {
+  s.axis = axis;
+  s.in = in;
+  s.out = out;
+  s.kind = kind;
+  s.sub = sub;
+  s.positive = positive;
+  s.real_in = real_in;
+  s.real_out = real_out;
+}
+
+static int sub_of_axis_kind(int k) {
+  switch (k) {
+    case PB_AXIS_DCT1: return S_DCT1;
+    case PB_AXIS_DCT2: return S_DCT2;
+    case PB_AXIS_DCT3: return S_DCT3;
+    case PB_AXIS_DCT4: return S_DCT4;
+    case PB_AXIS_DST1: return S_DST1;
+    case PB_AXIS_DST2: return S_DST2;
+    case PB_AXIS_DST3: return S_DST3;
+    case PB_AXIS_DST4: return S_DST4;
+    case PB_AXIS_DHT: return S_DHT;
+    default: return -1;
+  }
+}
+
+static void check_r2r_length(int sub, long long n) {
+  if (n == 0 || (sub == S_DCT1 && n == 1)) fail(PB_EINVALID_LENGTH);  // r2r.rs:801-803
+}
+
+static int precision_bytes(int precision) {
+  if (precision == PB_F32) return 4;
+  if (precision == PB_F64) return 8;
+  fail(PB_EINVALID_ARGUMENT);
+}
+
+// Generic complex-domain route: C2cPlan, R2rPlan, DhtPlan, MixedC2cPlan.
+static pb_plan* make_complex_plan(const pb_geom* g, int precision, const int* kinds, const uint8_t* positive,
+                                  bool complex_values) {
+  validate_geom(g);
+  std::unique_ptr<pb_plan> P(new pb_plan());
+  P->real_bytes = precision_bytes(precision);
+  P->extra = extra_count(g);
+  const int N = g->ndim;
+  Pencil input = canonical(g, g->shape);
+  validate_pencil(input);
+  auto route = build_route(input, g->permute_dims != 0, nullptr);
+  for (int i = 0; i < N; ++i) {
+    const int axis = N - 1 - i;
+    Stage st;
+    const int k = kinds[axis];
+    const bool real = !complex_values;
+    if (k == PB_AXIS_NONE) {
+      stage_fill(st, axis, route[i], route[i], SK_ID, 0, false, real, real);
+    } else if (k == PB_AXIS_FFT) {
+      stage_fill(st, axis, route[i], route[i], SK_C2C, 0, positive && positive[axis], real, real);
+    } else {
+      const int sub = sub_of_axis_kind(k);
+      if (sub < 0) fail(PB_EINVALID_GRAPH);
+      check_r2r_length(sub, g->shape[axis]);
+      stage_fill(st, axis, route[i], route[i], SK_R2R, sub, false, real, real);
+    }
+    P->stages.push_back(st);
+  }
+  P->fin = route.front();
+  P->fout = route.back();
+  P->fin_complex = P->fout_complex = complex_values;
+  finalize(*P);
+  return P.release();
+}
+
+// R2cPlan (R2c orientation) and MixedR2cPlan: real prefix, boundary, complex suffix.
+static pb_plan* make_r2c_plan(const pb_geom* g, int precision, int red, const int* prefix_kinds,
+                              const int* suffix_kinds) {
+  validate_geom(g);
+  std::unique_ptr<pb_plan> P(new pb_plan());
+  P->real_bytes = precision_bytes(precision);
+  P->extra = extra_count(g);
+  const int N = g->ndim;
+  const int boundary = N - 1 - red;
+  int64_t reduced[MAXN];
+  for (int x = 0; x < N; ++x) reduced[x] = g->shape[x];
+  P->real_len = g->shape[red];
+  reduced[red] = P->real_len / 2 + 1;
+  Pencil orig_in = canonical(g, g->shape), red_in = canonical(g, reduced);
+  validate_pencil(orig_in);
+  auto orig = build_route(orig_in, g->permute_dims != 0, nullptr);
+  auto redr = build_route(red_in, g->permute_dims != 0, nullptr);
+  for (int i = 0; i < N; ++i) {
+    const int axis = N - 1 - i;
+    Stage st;
+    if (i < boundary) {
+      const int k = prefix_kinds ? prefix_kinds[axis] : PB_AXIS_NONE;
+      if (k == PB_AXIS_NONE) {
+        stage_fill(st, axis, orig[i], orig[i], SK_ID, 0, false, true, true);
+      } else {
+        const int sub = sub_of_axis_kind(k);
+        if (sub < 0) fail(PB_EINVALID_GRAPH);
+        check_r2r_length(sub, g->shape[axis]);
+        stage_fill(st, axis, orig[i], orig[i], SK_R2R, sub, false, true, true);
+      }
+    } else if (i == boundary) {
+      stage_fill(st, axis, orig[i], redr[i], SK_R2C, 0, false, true, false);
+    } else {
+      const int k = suffix_kinds[axis];
+      if (k == PB_AXIS_NONE) {
+        stage_fill(st, axis, redr[i], redr[i], SK_ID, 0, false, false, false);
+      } else if (k == PB_AXIS_FFT) {
+        stage_fill(st, axis, redr[i], redr[i], SK_C2C, 0, false, false, false);
+        P->terms.push_back({(double)reduced[axis], 0.0, (double)reduced[axis]});
+      } else {
+        const int sub = sub_of_axis_kind(k);
+        if (sub < 0) fail(PB_EINVALID_GRAPH);
+        check_r2r_length(sub, reduced[axis]);
+        stage_fill(st, axis, redr[i], redr[i], SK_R2R, sub, false, false, false);
+        auto lf = r2r_lengths(sub, reduced[axis]);
+        P->terms.push_back({(double)lf.first, 2.0, (double)lf.second});
+      }
+    }
+    P->stages.push_back(st);
+  }
+  P->boundary = boundary;
+  P->fin = orig.front();
+  P->fout = redr.back();
+  P->fin_complex = false;
+  P->fout_complex = true;
+  finalize(*P);
+  return P.release();
+}
+
+// C2rPlan: R2C core in C2r orientation (reduction on the lowest selected axis,
+// routes from the canonical pencils reversed so stage index == axis).
+static pb_plan* make_c2r_plan(const pb_geom* g, long long real_len, int precision, const uint8_t* sel) {
+  validate_geom(g);
+  const int N = g->ndim;
+  int red = -1;
+  for (int x = 0; x < N; ++x)
+    if (!sel || sel[x]) {
+      red = x;
+      break;
+    }
+  if (red < 0) fail(PB_EINVALID_DIMENSIONS);
+  if (real_len <= 0) fail(PB_EINVALID_LENGTH);
+  if (g->shape[red] != real_len / 2 + 1) fail(PB_EINPUT_LAYOUT_MISMATCH);
+  std::unique_ptr<pb_plan> P(new pb_plan());
+  P->real_bytes = precision_bytes(precision);
+  P->extra = extra_count(g);
+  P->c2r_family = true;
+  int64_t orig_shape[MAXN];
+  for (int x = 0; x < N; ++x) orig_shape[x] = g->shape[x];
+  orig_shape[red] = real_len;
+  if (real_len > INT_MAX / 2) fail(PB_EUNSUPPORTED);
+  P->real_len = real_len;
+  Pencil orig_in = canonical(g, orig_shape), red_in = canonical(g, g->shape);
+  validate_pencil(red_in);
+  auto orig = build_route(orig_in, g->permute_dims != 0, nullptr);
+  auto redr = build_route(red_in, g->permute_dims != 0, nullptr);
+  std::reverse(orig.begin(), orig.end());
+  std::reverse(redr.begin(), redr.end());
+  for (int i = 0; i < N; ++i) {
+    const int axis = i;
+    Stage st;
+    if (i < red) {
+      stage_fill(st, axis, orig[i], orig[i], SK_ID, 0, false, true, true);
+    } else if (i == red) {
+      stage_fill(st, axis, orig[i], redr[i], SK_R2C, 0, false, true, false);
+    } else if (!sel || sel[axis]) {
+      stage_fill(st, axis, redr[i], redr[i], SK_C2C, 0, false, false, false);
+      P->terms.push_back({(double)g->shape[axis], 0.0, (double)g->shape[axis]});
+    } else {
+      stage_fill(st, axis, redr[i], redr[i], SK_ID, 0, false, false, false);
+    }
+    P->stages.push_back(st);
+  }
+  P->boundary = red;
+  P->fin = orig.front();
+  P->fout = redr.back();
+  P->fin_complex = false;
+  P->fout_complex = true;
+  finalize(*P);
+  return P.release();
+}
+
+static int user_mode(const pb_plan& P, int op) {
+  if (!P.c2r_family) {
+    switch (op) {
+      case PB_FORWARD: return M_F;
+      case PB_INVERSE: return M_I;
+      case PB_BACKWARD: return M_B;
+      case PB_VJP_FORWARD: return M_AF;
+      case PB_VJP_INVERSE: return M_AI;
+      case PB_VJP_BACKWARD: return M_AB;
+      default: fail(PB_EINVALID_ARGUMENT);
+    }
+  }
+  // C2rPlan: forward = raw C2R, backward = raw R2C, inverse = R2C / prod(n)
+  switch (op) {
+    case PB_FORWARD: return M_B;
+    case PB_INVERSE: return M_FS;
+    case PB_BACKWARD: return M_F;
+    case PB_VJP_FORWARD: return M_AB;
+    case PB_VJP_INVERSE: return M_AFS;
+    case PB_VJP_BACKWARD: return M_AF;
+    default: fail(PB_EINVALID_ARGUMENT);
+  }
+}
+
+static void* slot_ptr(const pb_plan& P, int slot, const void* in, void* out, void* ws) {
+  if (slot == -1) return const_cast<void*>(in);
+  if (slot == -2) return out;
+  return static_cast<unsigned char*>(ws) + (size_t)slot * P.buf_bytes;
+}
+
+static int run(pb_plan* P, int op, const void* in, void* out, void* ws, cudaStream_t s, float* ms, int cap,
+               int* count) {
+  const int mode = user_mode(*P, op);
+  Program& prog = P->prog[mode];
+  if ((!in || !out) && P->extra > 0) fail(PB_ENULL);
+  const bool needs_ws = prog.steps.size() > 1 || prog.has_stats;
+  if (needs_ws && !ws) fail(PB_ENULL);
+  int* status = ws ? reinterpret_cast<int*>(static_cast<unsigned char*>(ws) + P->status_off) : nullptr;
+  if (prog.has_stats) cuda_ok(cudaMemsetAsync(status, 0, P->ws_bytes - P->status_off, s));
+  std::vector<cudaEvent_t> ev;
+  if (ms) {
+    ev.resize(prog.steps.size() + 1);
+    for (auto& e : ev) cuda_ok(cudaEventCreate(&e));
+    cuda_ok(cudaEventRecord(ev[0], s));
+  }
+  int i = 0;
+  for (Step& st : prog.steps) {
+    if (st.type == 0) {
+      PassArgs A = st.pa;
+      A.in = slot_ptr(*P, st.src_slot, in, out, ws);
+      A.out = slot_ptr(*P, st.dst_slot, in, out, ws);
+      A.gate = (A.gate != nullptr) ? status : nullptr;
+      cuda_ok(launch_pass(A, P->real_bytes, s));
+    } else {
+      StatsArgs S = st.sa;
+      S.data = slot_ptr(*P, st.src_slot, in, out, ws);
+      S.acc = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + P->acc_off);
+      S.status = status;
+      cuda_ok(launch_stats(S, P->real_bytes, s));
+    }
+    if (ms) cuda_ok(cudaEventRecord(ev[i + 1], s));
+    ++i;
+  }
+  if (ms) {
+    cuda_ok(cudaEventSynchronize(ev.back()));
+    int n = 0;
+    for (size_t k = 0; k + 1 < ev.size() && (int)k < cap; ++k) {
+      cuda_ok(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+      ++n;
+    }
+    if (count) *count = n;
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  return PB_OK;
+}
+
+template <typename F>
+static int guard(F&& f) {
+  try {
+    return f();
+  } catch (const PbError& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return PB_EUNSUPPORTED;
+  } catch (...) {
+    return PB_EINVALID_ARGUMENT;
+  }
+}
+
+}  // namespace pb
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+using namespace pb;
+
+extern "C" {
+
+const char* pb_version(void) { return "pencil-b200 0.1 (sm_100a)"; }
+
+const char* pb_status_string(int status) {
+  switch (status) {
+    case PB_OK: return "ok";
+    case PB_EINVALID_DIMENSIONS: return "invalid dimensions";
+    case PB_EZERO_EXTENT: return "zero global extent";
+    case PB_EINVALID_DECOMPOSITION: return "invalid decomposition";
+    case PB_EINVALID_PERMUTATION: return "invalid permutation";
+    case PB_EINVALID_LENGTH: return "invalid transform length";
+    case PB_EINVALID_GRAPH: return "invalid mixed transform axis graph";
+    case PB_EINPUT_LAYOUT_MISMATCH: return "input layout mismatch";
+    case PB_EUNSUPPORTED_DECOMPOSITION_CHANGE: return "unsupported decomposition change";
+    case PB_ECOUNT_OVERFLOW: return "count overflow";
+    case PB_ESHAPE_MISMATCH: return "shape or layout mismatch";
+    case PB_EINVALID_SIGN: return "invalid affine sign";
+    case PB_EINVALID_SPECTRUM: return "invalid spectrum: constrained endpoint plane is not real";
+    case PB_ETIMEOUT: return "device wait timed out";
+    case PB_ENULL: return "null pointer";
+    case PB_EUNSUPPORTED: return "unsupported by this library";
+    case PB_ECUDA: return "CUDA error";
+    case PB_EINVALID_ARGUMENT: return "invalid argument";
+    case PB_EWRONG_PLAN: return "workspace or batch belongs to another plan";
+    default: return "unknown status";
+  }
+}
+
+int pb_pencil_local(const pb_pencil_desc* pencil, int32_t rank, int64_t extra_count, int64_t* start,
+                    int64_t* shape_logical, int64_t* shape_memory, int64_t* local_len, int64_t* offset) {
+  return guard([&] {
+    Pencil p = pencil_from_desc(pencil);
+    if (rank < 0 || rank >= p.nranks()) return (int)PB_EINVALID_ARGUMENT;
+    long long lo[MAXN], ext[MAXN];
+    p.local(rank, lo, ext);
+    for (int x = 0; x < p.N; ++x) {
+      if (start) start[x] = lo[x];
+      if (shape_logical) shape_logical[x] = ext[x];
+      if (shape_memory) shape_memory[x] = ext[p.perm[x]];
+    }
+    if (local_len) *local_len = p.local_len(rank);
+    if (offset) {
+      long long o = 0;
+      for (int r = 0; r < rank; ++r) o += p.local_len(r) * extra_count;
+      *offset = o;
+    }
+    return (int)PB_OK;
+  });
+}
+
+int pb_route_stage(const pb_geom* geom, int32_t stage, pb_pencil_desc* out, int32_t* distributed_edge) {
+  return guard([&] {
+    validate_geom(geom);
+    if (!out) return (int)PB_ENULL;
+    Pencil input = canonical(geom, geom->shape);
+    std::vector<int> dist;
+    auto route = build_route(input, geom->permute_dims != 0, &dist);
+    if (stage < 0 || stage >= (int)route.size()) return (int)PB_EINVALID_ARGUMENT;
+    pencil_to_desc(route[stage], out);
+    if (distributed_edge) *distributed_edge = (stage < (int)dist.size()) ? dist[stage] : 0;
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_c2c(const pb_geom* geom, int32_t precision, const uint8_t* selection, const uint8_t* positive,
+                       pb_plan** plan) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    validate_geom(geom);
+    int kinds[MAXN];
+    for (int x = 0; x < geom->ndim; ++x) kinds[x] = (!selection || selection[x]) ? PB_AXIS_FFT : PB_AXIS_NONE;
+    *plan = make_complex_plan(geom, precision, kinds, positive, true);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_r2c(const pb_geom* geom, int32_t precision, const uint8_t* selection, pb_plan** plan) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    validate_geom(geom);
+    int red = -1;
+    int suffix[MAXN];
+    for (int x = 0; x < geom->ndim; ++x) {
+      const bool s = !selection || selection[x];
+      suffix[x] = s ? PB_AXIS_FFT : PB_AXIS_NONE;
+      if (s) red = x;  // the largest selected axis (r2c.rs:1274-1280)
+    }
+    if (red < 0) return (int)PB_EINVALID_DIMENSIONS;
+    *plan = make_r2c_plan(geom, precision, red, nullptr, suffix);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_c2r(const pb_geom* geom, int64_t real_len, int32_t precision, const uint8_t* selection,
+                       pb_plan** plan) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    *plan = make_c2r_plan(geom, real_len, precision, selection);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_r2r(const pb_geom* geom, int32_t precision, int32_t complex_values, const int32_t* kinds,
+                       pb_plan** plan) {
+  return guard([&] {
+    if (!plan || !kinds) return (int)PB_ENULL;
+    validate_geom(geom);
+    int k[MAXN];
+    for (int x = 0; x < geom->ndim; ++x) {
+      if (kinds[x] != PB_AXIS_NONE && sub_of_axis_kind(kinds[x]) < 0) return (int)PB_EINVALID_GRAPH;
+      k[x] = kinds[x];
+    }
+    *plan = make_complex_plan(geom, precision, k, nullptr, complex_values != 0);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_mixed_c2c(const pb_geom* geom, int32_t precision, const int32_t* transforms,
+                             const uint8_t* positive, pb_plan** plan) {
+  return guard([&] {
+    if (!plan || !transforms) return (int)PB_ENULL;
+    validate_geom(geom);
+    int k[MAXN];
+    for (int x = 0; x < geom->ndim; ++x) {
+      // validate_c2c_graph (distributed/mixed.rs:1592-1600): no Rfft axis
+      if (transforms[x] == PB_AXIS_RFFT) return (int)PB_EINVALID_GRAPH;
+      if (transforms[x] != PB_AXIS_NONE && transforms[x] != PB_AXIS_FFT && sub_of_axis_kind(transforms[x]) < 0)
+        return (int)PB_EINVALID_GRAPH;
+      k[x] = transforms[x];
+    }
+    *plan = make_complex_plan(geom, precision, k, positive, true);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_create_mixed_r2c(const pb_geom* geom, int32_t precision, const int32_t* transforms, pb_plan** plan) {
+  return guard([&] {
+    if (!plan || !transforms) return (int)PB_ENULL;
+    validate_geom(geom);
+    // validate_r2c_graph (distributed/mixed.rs:1602-1626)
+    int boundary = -1;
+    for (int x = 0; x < geom->ndim; ++x)
+      if (transforms[x] == PB_AXIS_RFFT) {
+        if (boundary >= 0) return (int)PB_EINVALID_GRAPH;
+        boundary = x;
+      }
+    if (boundary < 0) return (int)PB_EINVALID_GRAPH;
+    int prefix[MAXN], suffix[MAXN];
+    for (int x = 0; x < geom->ndim; ++x) {
+      const int t = transforms[x];
+      prefix[x] = suffix[x] = PB_AXIS_NONE;
+      if (x == boundary) continue;
+      const bool r2r = sub_of_axis_kind(t) >= 0;
+      if (x > boundary) {
+        if (!(t == PB_AXIS_NONE || r2r)) return (int)PB_EINVALID_GRAPH;
+        prefix[x] = t;
+      } else {
+        if (!(t == PB_AXIS_NONE || t == PB_AXIS_FFT || r2r)) return (int)PB_EINVALID_GRAPH;
+        suffix[x] = t;
+      }
+    }
+    *plan = make_r2c_plan(geom, precision, boundary, prefix, suffix);
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_destroy(pb_plan* plan) {
+  delete plan;
+  return PB_OK;
+}
+
+int pb_plan_get_info(const pb_plan* plan, pb_plan_info* info) {
+  return guard([&] {
+    if (!plan || !info) return (int)PB_ENULL;
+    std::memset(info, 0, sizeof(*info));
+    const pb_plan& P = *plan;
+    // user-facing FORWARD input/output (C2rPlan swaps the inner orientation)
+    const Pencil& in = P.c2r_family ? P.fout : P.fin;
+    const Pencil& out = P.c2r_family ? P.fin : P.fout;
+    info->input_elems = in.total(P.extra);
+    info->output_elems = out.total(P.extra);
+    info->input_complex = P.c2r_family ? P.fout_complex : P.fin_complex;
+    info->output_complex = P.c2r_family ? P.fin_complex : P.fout_complex;
+    info->real_bytes = P.real_bytes;
+    info->nranks = in.nranks();
+    info->workspace_bytes = (int64_t)P.ws_bytes;
+    info->passes_forward = (int)P.prog[user_mode(P, PB_FORWARD)].steps.size();
+    info->passes_inverse = (int)P.prog[user_mode(P, PB_INVERSE)].steps.size();
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_pencil(const pb_plan* plan, int32_t which, pb_pencil_desc* out) {
+  return guard([&] {
+    if (!plan || !out) return (int)PB_ENULL;
+    const pb_plan& P = *plan;
+    const Pencil& in = P.c2r_family ? P.fout : P.fin;
+    const Pencil& o = P.c2r_family ? P.fin : P.fout;
+    if (which == 0)
+      pencil_to_desc(in, out);
+    else if (which == 1)
+      pencil_to_desc(o, out);
+    else
+      return (int)PB_EINVALID_ARGUMENT;
+    return (int)PB_OK;
+  });
+}
+
+int pb_execute(pb_plan* plan, int32_t op, const void* in, void* out, void* workspace, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    return run(plan, op, in, out, workspace, static_cast<cudaStream_t>(stream), nullptr, 0, nullptr);
+  });
+}
+
+int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void* workspace, void* stream,
+                     float* stage_ms, int32_t capacity, int32_t* count) {
+  return guard([&] {
+    if (!plan || !stage_ms) return (int)PB_ENULL;
+    return run(plan, op, in, out, workspace, static_cast<cudaStream_t>(stream), stage_ms, capacity, count);
+  });
+}
+
+int pb_execute_status(pb_plan* plan, void* workspace, void* stream) {
+  return guard([&] {
+    if (!plan || !workspace) return (int)PB_ENULL;
+    int st[2] = {0, 0};
+    cuda_ok(cudaMemcpyAsync(st, static_cast<unsigned char*>(workspace) + plan->status_off, sizeof(st),
+                            cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    cuda_ok(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return (st[0] != 0 || st[1] != 0) ? (int)PB_EINVALID_SPECTRUM : (int)PB_OK;
+  });
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// transposes and remap
+// ===========================================================================
+namespace pb {
+
+// Uploads a plan-owned table arena and resolves the encoded pointers of one
+// step list (used by the single-pass helpers below).
+static void upload_steps(pb_plan& P, std::vector<Step>& steps) {
+  if (!P.host.bytes.empty()) {
+    cuda_ok(cudaMalloc(&P.arena, P.host.bytes.size()));
+    cuda_ok(cudaMemcpy(P.arena, P.host.bytes.data(), P.host.bytes.size(), cudaMemcpyHostToDevice));
+  }
+  const uintptr_t base = reinterpret_cast<uintptr_t>(P.arena);
+  auto fix = [&](const void*& p) {
+    if (p != nullptr) p = reinterpret_cast<const void*>(base + reinterpret_cast<uintptr_t>(p) - 1);
+  };
+  auto fixpen = [&](DevPencil& d) {
+    const void* v = d.info;
+    fix(v);
+    d.info = reinterpret_cast<const long long*>(v);
+  };
+  for (auto& s : steps) {
+    const void* c = s.pa.chunks;
+    fix(c);
+    s.pa.chunks = reinterpret_cast<const int2*>(c);
+    fix(s.pa.twiddle);
+    fix(s.pa.aux0);
+    fix(s.pa.aux1);
+    fixpen(s.pa.src);
+    fixpen(s.pa.dst);
+  }
+}
+
+static const void* fix_ptr(const pb_plan& P, const void* p) {
+  if (p == nullptr) return nullptr;
+  return reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(P.arena) + reinterpret_cast<uintptr_t>(p) - 1);
+}
+
+}  // namespace pb
+
+struct pb_transpose {
+  pb::Pencil src, dst;
+  long long extra = 1;
+  int elem_bytes = 0;
+  bool alltoallv = false;
+  std::unique_ptr<pb_plan> tables;  // owns the device arena
+  bool use_pass = false;
+  pb::Step pass;
+  pb::RemapArgs gather{};
+  std::vector<pb::SegDesc> send_segs, recv_segs;
+  std::vector<long long> recv_off, send_off;
+  long long send_total = 0, recv_total = 0;
+  const pb::SegDesc* d_send = nullptr;
+  const pb::SegDesc* d_recv = nullptr;
+  const long long* d_recv_off = nullptr;
+  const long long* d_send_off = nullptr;
+};
+
+struct pb_remap {
+  std::unique_ptr<pb_plan> tables;
+  pb::RemapArgs args{};
+};
+
+namespace pb {
+
+static void same_topology_and_shape(const Pencil& a, const Pencil& b) {
+  if (a.N != b.N || a.M != b.M) fail(PB_ESHAPE_MISMATCH);
+  for (int x = 0; x < a.N; ++x)
+    if (a.shape[x] != b.shape[x]) fail(PB_ESHAPE_MISMATCH);
+  for (int t = 0; t < a.M; ++t)
+    if (a.grid[t] != b.grid[t]) fail(PB_ESHAPE_MISMATCH);
+}
+
+// A fused layout-change pass for 4/8/16-byte elements, else an element gather.
+static void build_copy(pb_transpose& T) {
+  T.tables.reset(new pb_plan());
+  pb_plan& P = *T.tables;
+  P.extra = T.extra;
+  int dev = 0;
+  cuda_ok(cudaGetDevice(&dev));
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+    P.max_smem = optin;
+  const int N = T.src.N;
+  std::vector<Step> steps;
+  if (T.elem_bytes == 4 || T.elem_bytes == 8 || T.elem_bytes == 16) {
+    P.real_bytes = (T.elem_bytes == 16) ? 8 : 4;
+    const bool cplx = T.elem_bytes != 4;
+    Stage id;
+    id.axis = T.src.perm[N - 1];
+    LocalOp op;
+    steps.push_back(make_pass(P, id, op, T.src, T.dst, cplx, cplx));
+    T.use_pass = true;
+  }
+  RemapArgs& G = T.gather;
+  G.src = dev_pencil(P, P.host, P.cache, T.src, T.extra);
+  G.dst = dev_pencil(P, P.host, P.cache, T.dst, T.extra);
+  G.total = T.dst.total(T.extra);
+  G.elem_bytes = T.elem_bytes;
+  for (int x = 0; x < N; ++x) {
+    G.sign[x] = 1;
+    G.offset[x] = 0;
+  }
+  // segment tables (alltoallv only)
+  size_t send_tab = 0, recv_tab = 0, roff_tab = 0, soff_tab = 0;
+  if (T.alltoallv) {
+    send_tab = P.host.add(T.send_segs.data(), T.send_segs.size() * sizeof(SegDesc));
+    recv_tab = P.host.add(T.recv_segs.data(), T.recv_segs.size() * sizeof(SegDesc));
+    roff_tab = P.host.add(T.recv_off.data(), T.recv_off.size() * sizeof(long long));
+    soff_tab = P.host.add(T.send_off.data(), T.send_off.size() * sizeof(long long));
+  }
+  upload_steps(P, steps);
+  if (T.use_pass) T.pass = steps[0];
+  auto fixpen = [&](DevPencil& d) { d.info = reinterpret_cast<const long long*>(fix_ptr(P, d.info)); };
+  fixpen(G.src);
+  fixpen(G.dst);
+  if (T.alltoallv) {
+    T.d_send = reinterpret_cast<const SegDesc*>(fix_ptr(P, enc(send_tab)));
+    T.d_recv = reinterpret_cast<const SegDesc*>(fix_ptr(P, enc(recv_tab)));
+    T.d_recv_off = reinterpret_cast<const long long*>(fix_ptr(P, enc(roff_tab)));
+    T.d_send_off = reinterpret_cast<const long long*>(fix_ptr(P, enc(soff_tab)));
+  }
+}
+
+// Per-(rank, peer) regions of the changed sub-communicator
+// (build_peer_metadata, transpose.rs:601-656) in the segment layout of
+// pack_source / unpack_destination (transpose.rs:1126-1281).
+static void build_segments(pb_transpose& T, int changed) {
+  const Pencil& S = T.src;
+  const Pencil& D = T.dst;
+  const int N = S.N;
+  const int R = S.nranks();
+  const int P = S.grid[changed];
+  std::vector<long long> send_base(R + 1, 0), recv_base(R + 1, 0);
+  // [rank][peer] spatial lengths and displacements
+  std::vector<long long> slen((size_t)R * P), rlen((size_t)R * P), sdisp((size_t)R * P), rdisp((size_t)R * P);
+  auto region = [&](const Pencil& A, const int* ca, const Pencil& B, const int* cb, long long* lo, long long* ext) {
+    long long alo[MAXN], aext[MAXN], blo[MAXN], bext[MAXN];
+    // ranges at explicit coordinates
+    auto ranges = [&](const Pencil& p, const int* c, long long* l, long long* e) {
+      for (int x = 0; x < N; ++x) {
+        l[x] = 0;
+        e[x] = p.shape[x];
+      }
+      for (int t = 0; t < p.M; ++t) {
+        const int ax = p.dec[t];
+        l[ax] = Pencil::part(p.shape[ax], p.grid[t], c[t]);
+        e[ax] = Pencil::part(p.shape[ax], p.grid[t], c[t] + 1) - l[ax];
+      }
+    };
+    ranges(A, ca, alo, aext);
+    ranges(B, cb, blo, bext);
+    long long len = 1;
+    for (int x = 0; x < N; ++x) {
+      const long long s = std::max(alo[x], blo[x]);
+      const long long e = std::min(alo[x] + aext[x], blo[x] + bext[x]);
+      lo[x] = s;
+      ext[x] = e > s ? e - s : 0;
+      len *= ext[x];
+    }
+    return len;
+  };
+  std::vector<std::array<long long, 2 * MAXN>> sreg((size_t)R * P), rreg((size_t)R * P);
+  for (int r = 0; r < R; ++r) {
+    int me[MAXM];
+    S.coords(r, me);
+    long long sd = 0, rd = 0;
+    for (int p = 0; p < P; ++p) {
+      int pc[MAXM];
+      std::memcpy(pc, me, sizeof(pc));
+      pc[changed] = p;
+      long long lo[MAXN], ext[MAXN];
+      const size_t k = (size_t)r * P + p;
+      slen[k] = region(S, me, D, pc, lo, ext);
+      for (int x = 0; x < N; ++x) {
+        sreg[k][x] = lo[x];
+        sreg[k][MAXN + x] = ext[x];
+      }
+      rlen[k] = region(S, pc, D, me, lo, ext);
+      for (int x = 0; x < N; ++x) {
+        rreg[k][x] = lo[x];
+        rreg[k][MAXN + x] = ext[x];
+      }
+      sdisp[k] = sd;
+      rdisp[k] = rd;
+      // checked_count (transpose.rs:684-721): counts and displacements fit i32
+      const long long e = T.extra;
+      if (slen[k] * e > INT_MAX || rlen[k] * e > INT_MAX || sd * e > INT_MAX || rd * e > INT_MAX)
+        fail(PB_ECOUNT_OVERFLOW);
+      sd += slen[k];
+      rd += rlen[k];
+    }
+    send_base[r + 1] = send_base[r] + sd * T.extra;
+    recv_base[r + 1] = recv_base[r] + rd * T.extra;
+  }
+  T.send_total = send_base[R];
+  T.recv_total = recv_base[R];
+  for (int r = 0; r < R; ++r) {
+    int me[MAXM];
+    S.coords(r, me);
+    for (int p = 0; p < P; ++p) {
+      const size_t k = (size_t)r * P + p;
+      if (slen[k] > 0 && T.extra > 0) {
+        SegDesc s{};
+        s.buf_off = send_base[r] + sdisp[k] * T.extra;
+        s.len = slen[k];
+        for (int x = 0; x < N; ++x) {
+          s.start[x] = (int)sreg[k][x];
+          s.ext[x] = (int)sreg[k][MAXN + x];
+        }
+        T.send_segs.push_back(s);
+      }
+      if (rlen[k] > 0 && T.extra > 0) {
+        SegDesc s{};
+        s.buf_off = recv_base[r] + rdisp[k] * T.extra;
+        s.len = rlen[k];
+        for (int x = 0; x < N; ++x) {
+          s.start[x] = (int)rreg[k][x];
+          s.ext[x] = (int)rreg[k][MAXN + x];
+        }
+        T.recv_segs.push_back(s);
+        // the matching send segment: peer q = (my coords with changed = p), addressed to my coordinate
+        int qc[MAXM];
+        std::memcpy(qc, me, sizeof(qc));
+        qc[changed] = p;
+        int q = 0;
+        for (int t = 0; t < S.M; ++t) q = q * S.grid[t] + qc[t];
+        const size_t kq = (size_t)q * P + me[changed];
+        T.recv_off.push_back(s.buf_off);
+        T.send_off.push_back(send_base[q] + sdisp[kq] * T.extra);
+      }
+    }
+  }
+}
+
+static int transpose_create(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra, int32_t elem,
+                            bool alltoallv, pb_transpose** out) {
+  if (!out) return PB_ENULL;
+  if (extra < 0 || elem <= 0) return PB_EINVALID_ARGUMENT;
+  std::unique_ptr<pb_transpose> T(new pb_transpose());
+  T->src = pencil_from_desc(src);
+  T->dst = pencil_from_desc(dst);
+  T->extra = extra;
+  T->elem_bytes = elem;
+  T->alltoallv = alltoallv;
+  same_topology_and_shape(T->src, T->dst);
+  if (alltoallv) {
+    // validate_plan_layout (transpose.rs:590-599): exactly one decomposition slot changes
+    int changed = -1, count = 0;
+    for (int t = 0; t < T->src.M; ++t)
+      if (T->src.dec[t] != T->dst.dec[t]) {
+        changed = t;
+        ++count;
+      }
+    if (count != 1) return PB_EUNSUPPORTED_DECOMPOSITION_CHANGE;
+    build_segments(*T, changed);
+  } else if (!T->src.same_distribution(T->dst)) {
+    return PB_EUNSUPPORTED_DECOMPOSITION_CHANGE;  // LocalTransposeError::IncompatibleDistribution
+  }
+  build_copy(*T);
+  *out = T.release();
+  return PB_OK;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_transpose_create_alltoallv(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,
+                                  int32_t elem_bytes, pb_transpose** plan) {
+  return guard([&] { return transpose_create(src, dst, extra_count, elem_bytes, true, plan); });
+}
+
+int pb_transpose_create_local(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,
+                              int32_t elem_bytes, pb_transpose** plan) {
+  return guard([&] { return transpose_create(src, dst, extra_count, elem_bytes, false, plan); });
+}
+
+int pb_transpose_workspace(const pb_transpose* plan, int64_t* send_elems, int64_t* receive_elems) {
+  if (!plan) return PB_ENULL;
+  if (send_elems) *send_elems = plan->alltoallv ? plan->send_total : 0;
+  if (receive_elems) *receive_elems = plan->alltoallv ? plan->recv_total : 0;
+  return PB_OK;
+}
+
+int pb_transpose_execute(pb_transpose* plan, const void* src, void* dst, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (plan->extra == 0) return (int)PB_OK;
+    if (!src || !dst) return (int)PB_ENULL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (plan->use_pass) {
+      PassArgs A = plan->pass.pa;
+      A.in = src;
+      A.out = dst;
+      A.gate = nullptr;
+      cuda_ok(launch_pass(A, plan->tables->real_bytes, s));
+    } else {
+      RemapArgs G = plan->gather;
+      G.in = src;
+      G.out = dst;
+      cuda_ok(launch_remap(G, s));
+    }
+    return (int)PB_OK;
+  });
+}
+
+int pb_transpose_pack(pb_transpose* plan, const void* src, void* send, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
+    if (plan->send_segs.empty()) return (int)PB_OK;
+    if (!src || !send) return (int)PB_ENULL;
+    SegArgs A{};
+    A.pen = plan->gather.src;
+    A.segs = plan->d_send;
+    A.nseg = (int)plan->send_segs.size();
+    A.total = plan->send_total;
+    A.elem_bytes = plan->elem_bytes;
+    A.to_buffer = 1;
+    A.pencil_data = src;
+    A.buffer = send;
+    cuda_ok(launch_segments(A, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
+  });
+}
+
+int pb_transpose_exchange(pb_transpose* plan, const void* send, void* receive, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
+    if (plan->recv_off.empty()) return (int)PB_OK;
+    if (!send || !receive) return (int)PB_ENULL;
+    ExchArgs A{};
+    A.recv_off = plan->d_recv_off;
+    A.send_off = plan->d_send_off;
+    A.nseg = (int)plan->recv_off.size();
+    A.total = plan->recv_total;
+    A.elem_bytes = plan->elem_bytes;
+    A.send = send;
+    A.recv = receive;
+    cuda_ok(launch_exchange(A, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
+  });
+}
+
+int pb_transpose_unpack(pb_transpose* plan, const void* receive, void* dst, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
+    if (plan->recv_segs.empty()) return (int)PB_OK;
+    if (!receive || !dst) return (int)PB_ENULL;
+    SegArgs A{};
+    A.pen = plan->gather.dst;
+    A.segs = plan->d_recv;
+    A.nseg = (int)plan->recv_segs.size();
+    A.total = plan->recv_total;
+    A.elem_bytes = plan->elem_bytes;
+    A.to_buffer = 0;
+    A.buffer_in = receive;
+    A.pencil_out = dst;
+    cuda_ok(launch_segments(A, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
+  });
+}
+
+int pb_transpose_destroy(pb_transpose* plan) {
+  delete plan;
+  return PB_OK;
+}
+
+int pb_remap_create(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count, int32_t elem_bytes,
+                    const int8_t* signs, const int64_t* offsets, pb_remap** plan) {
+  return guard([&] {
+    if (!plan || !signs || !offsets) return (int)PB_ENULL;
+    if (extra_count < 0 || elem_bytes <= 0) return (int)PB_EINVALID_ARGUMENT;
+    Pencil S = pencil_from_desc(src), D = pencil_from_desc(dst);
+    same_topology_and_shape(S, D);
+    for (int x = 0; x < S.N; ++x)
+      if (signs[x] != 1 && signs[x] != -1) return (int)PB_EINVALID_SIGN;
+    std::unique_ptr<pb_remap> R(new pb_remap());
+    R->tables.reset(new pb_plan());
+    pb_plan& P = *R->tables;
+    P.extra = extra_count;
+    RemapArgs& G = R->args;
+    G.src = dev_pencil(P, P.host, P.cache, S, extra_count);
+    G.dst = dev_pencil(P, P.host, P.cache, D, extra_count);
+    G.total = D.total(extra_count);
+    G.elem_bytes = elem_bytes;
+    for (int x = 0; x < S.N; ++x) {
+      G.sign[x] = signs[x];
+      long long o = offsets[x] % S.shape[x];  // rem_euclid (spatial_remap.rs:786)
+      if (o < 0) o += S.shape[x];
+      G.offset[x] = o;
+    }
+    std::vector<Step> none;
+    upload_steps(P, none);
+    G.src.info = reinterpret_cast<const long long*>(fix_ptr(P, G.src.info));
+    G.dst.info = reinterpret_cast<const long long*>(fix_ptr(P, G.dst.info));
+    *plan = R.release();
+    return (int)PB_OK;
+  });
+}
+
+int pb_remap_apply(pb_remap* plan, const void* src, void* dst, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (plan->args.total == 0) return (int)PB_OK;
+    if (!src || !dst) return (int)PB_ENULL;
+    RemapArgs G = plan->args;
+    G.in = src;
+    G.out = dst;
+    cuda_ok(launch_remap(G, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
+  });
+}
+
+int pb_remap_destroy(pb_remap* plan) {
+  delete plan;
+  return PB_OK;
+}
+
+}  // extern "C"
