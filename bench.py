@@ -245,7 +245,7 @@ def b200_arm(args):
     L.check(lib.pb_execute_status(plan._h, hw, sp), "spectrum")
     lg = math.log2(shape[0] * shape[1] * shape[2])
     rt = float(torch.linalg.vector_norm((back - x).double()) / torch.linalg.vector_norm(x.double()))
-    kvec = torch.from_numpy(rng.integers(0, shape[0] // 2, size=(16, 3))).to(dev)
+    kvec = torch.from_numpy(rng.integers(0, shape[0] // 2, size=(16, 3))).to(dev, torch.float64)
     phase = torch.from_numpy(rng.uniform(0.0, 2 * math.pi, 16)).to(dev)
     axes = [torch.arange(n, device=dev, dtype=torch.float64) for n in shape]
     fb = torch.zeros(shape, dtype=torch.float64, device=dev)
@@ -263,10 +263,11 @@ def b200_arm(args):
     for m in range(16):
         k = [int(v) for v in kvec[m]]
         ph = float(phase[m])
-        exp[k[0], k[1], k[2]] += (ntot / 2) * complex(math.cos(ph), math.sin(ph))
+        pk = (k[0] % shape[0], k[1] % shape[1], k[2] % shape[2])
         mk = ((-k[0]) % shape[0], (-k[1]) % shape[1], (-k[2]) % shape[2])
-        if mk[2] <= shape[2] // 2:
-            exp[mk] += (ntot / 2) * complex(math.cos(ph), -math.sin(ph))
+        for idx, sgn in ((pk, 1.0), (mk, -1.0)):
+            if idx[2] <= shape[2] // 2:  # the stored half spectrum
+                exp[idx] += (ntot / 2) * complex(math.cos(ph), sgn * math.sin(ph))
     kb = float(torch.linalg.vector_norm((got - exp).to(torch.complex128)) /
                torch.linalg.vector_norm(exp.to(torch.complex128)))
     del got, exp, xb

@@ -701,7 +701,24 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   A.src_k_contig = (src.perm[N - 1] == a) ? 1 : 0;
   A.dst_k_contig = (dst.perm[N - 1] == a) ? 1 : 0;
   const bool pair_kind = (op.kind == P_R2C || op.kind == P_C2R || (op.kind == P_R2R && !in_complex));
-  const int L = choose_lines(P, A, pair_kind ? 1 : 0);
+  int L = 0;
+  // register-resident power-of-two kernel: lines contiguous in one source rank,
+  // destination either with the same property (direct) or with the tile axis
+  // innermost and unsplit (transposed store)
+  const bool pow2 = A.m >= 32 && A.m <= 2048 && (A.m & (A.m - 1)) == 0;
+  if ((op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && pow2 && src.perm[N - 1] == a &&
+      src.split_of(a) < 0) {
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    if (direct || transposed) {
+      A.fast = 1;
+      A.dst_k_contig = direct ? 1 : 0;
+      L = pow2_lines(A.m, op.kind, P.real_bytes);
+      A.lines = L;
+    }
+  }
+  if (!A.fast) L = choose_lines(P, A, pair_kind ? 1 : 0);
   // chunks of the tile axis, split at both partitions of axis b
   std::vector<long long> cuts{0, src.shape[b]};
   for (const Pencil* p : {&src, &dst}) {

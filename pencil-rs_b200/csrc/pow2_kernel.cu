@@ -1,0 +1,454 @@
+// Register-resident fused pass for power-of-two line lengths (32..2048): the
+// hot path of the canonical route (every stage axis is contiguous in its own
+// layout, so each line is one contiguous run in one virtual rank).
+//
+// Per tile of L lines: each line (or pair of real lines) is one complex
+// sequence handled by T = n/8 threads holding 8 elements each.  Loads go from
+// global straight into registers (coalesced: thread t of a line reads
+// elements t + T*m).  Stockham stages run in registers with a radix 2/4 lead
+// stage and radix-8 stages; between stages the 8 values per thread are
+// exchanged through padded shared memory.  Twiddles come from the table of
+// n-th roots (generated on the host in extended precision, rounded once) and
+// stay in registers for the whole tile.  The results are stored either
+// directly (transform axis contiguous in the destination) or through shared
+// memory transposed so that the L lines of a tile form contiguous runs of the
+// destination's innermost axis (the fused pencil transpose).
+#include <cuda_runtime.h>
+
+#include "pb_aux.hpp"
+#include "pb_device.cuh"
+#include "pb_fft.cuh"
+
+namespace pb {
+
+constexpr int P2_THREADS = 256;
+constexpr int P2_MAXPIECES = 64;
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+__host__ __device__ constexpr int ipow8(int s) { return s == 0 ? 1 : 8 * ipow8(s - 1); }
+
+template <int N>
+struct Sched {
+  static constexpr int LOG = ilog2c(N);
+  static constexpr int LEAD = (LOG % 3 == 0) ? 8 : ((LOG % 3 == 1) ? 2 : 4);
+  static constexpr int NST = (LOG % 3 == 0) ? LOG / 3 : LOG / 3 + 1;
+  static constexpr int T = N / 8;
+  __host__ __device__ static constexpr int radix(int s) { return s == 0 ? LEAD : 8; }
+  __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : LEAD * ipow8(s - 1); }
+};
+
+template <typename R, int N>
+struct P2Geom {
+  static constexpr int T = N / 8;
+  static constexpr int SLOTS = P2_THREADS / T;
+  static constexpr int LPT = (sizeof(R) == 4 && N >= 64) ? 2 : 1;
+  static constexpr int NSEQ = SLOTS * LPT;
+  static constexpr int SEQ = N + N / 8 + 1;  // padded sequence stride (complex units)
+};
+
+__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+
+// One Stockham stage on the 8 register values of each of the thread's sequences.
+template <typename C, int N, int ST, bool INV, int LPT>
+__device__ __forceinline__ void p2_stage(C (&v)[LPT][8], const C (&tw)[Sched<N>::NST][7], int t) {
+  using S = Sched<N>;
+  constexpr int RAD = S::radix(ST);
+  constexpr int NS = S::ns(ST);
+  constexpr int U = 8 / RAD;
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    C out[8];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      C b[RAD];
+#pragma unroll
+      for (int r = 0; r < RAD; ++r) b[r] = v[i][u + r * U];
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < RAD; ++r) b[r] = twmul<INV>(b[r], tw[ST][r - 1]);
+      }
+      Bfly<C, RAD, INV>::run(b);
+#pragma unroll
+      for (int r = 0; r < RAD; ++r) out[u * RAD + r] = b[r];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[i][q] = out[q];
+  }
+  (void)t;
+}
+
+// Output position of value q (= u*RAD + r) of a stage for thread t.
+template <int N, int ST>
+__device__ __forceinline__ int p2_out_index(int t, int q) {
+  using S = Sched<N>;
+  constexpr int RAD = S::radix(ST);
+  constexpr int NS = S::ns(ST);
+  constexpr int U = 8 / RAD;
+  const int u = q / RAD, r = q - u * RAD;
+  const int jb = t + u * S::T;
+  const int k = jb & (NS - 1);
+  return (jb - k) * RAD + k + r * NS;
+  (void)U;
+}
+
+template <typename R, int N, int KIND, bool INV, bool DIRECT>
+__global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
+  using C = typename Cx<R>::T;
+  using S = Sched<N>;
+  using G = P2Geom<R, N>;
+  constexpr int T = G::T;
+  constexpr int SLOTS = G::SLOTS;
+  constexpr int LPT = G::LPT;
+  constexpr int NSEQ = G::NSEQ;
+  constexpr int SEQ = G::SEQ;
+  constexpr int LMAX = (KIND == P_C2C) ? NSEQ : 2 * NSEQ;
+  constexpr int H = N / 2 + 1;
+  constexpr int NOUT = (KIND == P_R2C) ? H : N;
+  extern __shared__ __align__(16) unsigned char smem[];
+  C* sm = reinterpret_cast<C*>(smem);
+  long long* Atab = reinterpret_cast<long long*>(sm + NSEQ * SEQ);
+  __shared__ long long s_src0, s_dst0, s_rowbase[P2_MAXPIECES];
+  __shared__ int s_srcb, s_dstb, s_stride_a[P2_MAXPIECES], s_pstart[P2_MAXPIECES];
+
+  if (A.gate != nullptr && *A.gate != 0) return;
+  const int tid = threadIdx.x;
+  const int slot = tid / T;
+  const int t = tid - slot * T;
+
+  // ---- tile decode
+  const long long tile = blockIdx.x;
+  const int ci = (int)(tile % A.nchunks);
+  long long outer = tile / A.nchunks;
+  const int2 ch = A.chunks[ci];
+  int g[MAXN];
+#pragma unroll
+  for (int x = 0; x < MAXN; ++x) g[x] = 0;
+  for (int i = A.nouter_axes - 1; i >= 0; --i) {
+    g[A.outer_axis[i]] = (int)(outer % A.outer_ext[i]);
+    outer /= A.outer_ext[i];
+  }
+  const long long e = outer;
+  g[A.b] = ch.x;
+  const int L = ch.y;
+  g[A.a] = 0;
+
+  // ---- per-tile addressing
+  if (tid == 0) {
+    int sb;
+    s_src0 = locate(A.src, e, g, A.b, &sb);
+    s_srcb = sb;
+    if (DIRECT) {
+      int db;
+      s_dst0 = locate(A.dst, e, g, A.b, &db);
+      s_dstb = db;
+    }
+  }
+  int npieces = 1;
+  int ta = -1;
+  if (!DIRECT) {
+    ta = A.dst.split[A.a];
+    npieces = ta >= 0 ? A.dst.gdim[ta] : 1;
+    for (int p = tid; p < npieces; p += P2_THREADS) {
+      const int start = (int)(((long long)NOUT * p) / npieces);
+      int gg[MAXN];
+#pragma unroll
+      for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
+      gg[A.a] = start;
+      const int end = (int)(((long long)NOUT * (p + 1)) / npieces);
+      int sa = 0;
+      s_rowbase[p] = (end > start) ? locate(A.dst, e, gg, A.a, &sa) : 0;
+      s_stride_a[p] = sa;
+      s_pstart[p] = start;
+    }
+  }
+  __syncthreads();
+  if (!DIRECT) {
+    for (int k = tid; k < NOUT; k += P2_THREADS) {
+      const int p = (ta >= 0) ? owner_of(k, NOUT, npieces) : 0;
+      Atab[k] = s_rowbase[p] + (long long)(k - s_pstart[p]) * s_stride_a[p];
+    }
+  }
+
+  // ---- twiddles of this thread (constant over the tile): stage ST > 0 uses
+  // W_N^{k*r*N/(NS*8)} with k = t mod NS (NS divides T for every radix-8 stage)
+  const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
+  C tw[S::NST][7];
+#pragma unroll
+  for (int st = 1; st < S::NST; ++st) {
+    const int NS = S::ns(st);
+    const int k = t & (NS - 1);
+    const int step = N / (NS * 8);
+#pragma unroll
+    for (int r = 1; r < 8; ++r) tw[st][r - 1] = Wg[(k * r * step) & (N - 1)];
+  }
+#pragma unroll
+  for (int r = 0; r < 7; ++r) tw[0][r] = mk<C, R>(R(1), R(0));
+
+  // ---- load: global -> registers
+  const long long src0 = s_src0;
+  const long long srcb = s_srcb;
+  C v[LPT][8];
+  const R zero = R(0);
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int s = slot + SLOTS * i;
+    if (KIND == P_C2C) {
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok = s < L;
+      const long long base = src0 + (long long)s * srcb + t;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[i][m] = ok ? in[base + T * m] : mk<C, R>(zero, zero);
+    } else if (KIND == P_R2C) {
+      const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+      const long long b0 = src0 + (long long)(2 * s) * srcb + t;
+      const long long b1 = b0 + srcb;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[i][m] = mk<C, R>(ok0 ? in[b0 + T * m] : zero, ok1 ? in[b1 + T * m] : zero);
+    } else {  // P_C2R: Hermitian extension of two half spectra
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+      const long long b0 = src0 + (long long)(2 * s) * srcb;
+      const long long b1 = b0 + srcb;
+      const R w_in = R(A.pre_factor);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int q = t + T * m;
+        const bool mirror = q > N / 2;
+        const int hq = mirror ? N - q : q;
+        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
+        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
+        const bool edge = (hq == 0) || (hq == N / 2);
+        if (mirror) {
+          X.y = -X.y;
+          Y.y = -Y.y;
+        }
+        if (edge) {
+          X.y = zero;
+          Y.y = zero;
+        }
+        const R w = (A.pre_mode == W_HALF_INTERIOR && !edge) ? w_in : R(1);
+        v[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
+      }
+    }
+  }
+
+  // ---- Stockham stages
+#pragma unroll
+  for (int st = 0; st < S::NST; ++st) {
+    // (st is a compile-time constant after unrolling)
+    if (st > 0) {
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < LPT; ++i) {
+        const C* seq = sm + (slot + SLOTS * i) * SEQ;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[i][m] = seq[pad8(t + T * m)];
+      }
+    }
+    switch (st) {
+      case 0: p2_stage<C, N, 0, INV, LPT>(v, tw, t); break;
+      case 1: p2_stage<C, N, (S::NST > 1 ? 1 : 0), INV, LPT>(v, tw, t); break;
+      case 2: p2_stage<C, N, (S::NST > 2 ? 2 : 0), INV, LPT>(v, tw, t); break;
+      default: p2_stage<C, N, (S::NST > 3 ? 3 : 0), INV, LPT>(v, tw, t); break;
+    }
+    if (st + 1 < S::NST) {
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < LPT; ++i) {
+        C* seq = sm + (slot + SLOTS * i) * SEQ;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          int o;
+          switch (st) {
+            case 0: o = p2_out_index<N, 0>(t, q); break;
+            case 1: o = p2_out_index<N, (S::NST > 1 ? 1 : 0)>(t, q); break;
+            default: o = p2_out_index<N, (S::NST > 2 ? 2 : 0)>(t, q); break;
+          }
+          seq[pad8(o)] = v[i][q];
+        }
+      }
+    }
+  }
+  // after the last (radix-8) stage thread t holds natural-order outputs t + T*r
+
+  const R sc = R(A.scale);
+  if (DIRECT && KIND != P_R2C) {
+    const long long dst0 = s_dst0;
+    const long long dstb = s_dstb;
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int s = slot + SLOTS * i;
+      if (KIND == P_C2C) {
+        if (s < L) {
+          C* __restrict__ out = reinterpret_cast<C*>(A.out);
+          const long long base = dst0 + (long long)s * dstb + t;
+#pragma unroll
+          for (int r = 0; r < 8; ++r) out[base + T * r] = scl(v[i][r], sc);
+        }
+      } else {  // C2R
+        R* __restrict__ out = reinterpret_cast<R*>(A.out);
+        const long long b0 = dst0 + (long long)(2 * s) * dstb + t;
+        if (2 * s < L) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) out[b0 + T * r] = v[i][r].x * sc;
+        }
+        if (2 * s + 1 < L) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) out[b0 + dstb + T * r] = v[i][r].y * sc;
+        }
+      }
+    }
+    return;
+  }
+
+  // ---- natural-order results to shared memory
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    C* seq = sm + (slot + SLOTS * i) * SEQ;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) seq[pad8(t + T * r)] = v[i][r];
+  }
+  __syncthreads();
+
+  const R pf = R(A.post_factor);
+  if (KIND == P_R2C && DIRECT) {
+    const long long dst0 = s_dst0;
+    const long long dstb = s_dstb;
+    C* __restrict__ out = reinterpret_cast<C*>(A.out);
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int s = slot + SLOTS * i;
+      const C* seq = sm + s * SEQ;
+      for (int k = t; k < H; k += T) {
+        const C a = seq[pad8(k)];
+        const C b = seq[pad8((N - k) & (N - 1))];
+        R f = sc;
+        if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
+        if (2 * s < L)
+          out[dst0 + (long long)(2 * s) * dstb + k] = mk<C, R>((a.x + b.x) * R(0.5) * f, (a.y - b.y) * R(0.5) * f);
+        if (2 * s + 1 < L)
+          out[dst0 + (long long)(2 * s + 1) * dstb + k] =
+              mk<C, R>((a.y + b.y) * R(0.5) * f, (b.x - a.x) * R(0.5) * f);
+      }
+    }
+    return;
+  }
+
+  // ---- transposed store: the L lines of a tile are contiguous along the
+  // destination's innermost axis; element (k, j) goes to Atab[k] + j.
+  constexpr int TOTAL = LMAX * NOUT;
+  if (KIND == P_C2C) {
+    C* __restrict__ out = reinterpret_cast<C*>(A.out);
+    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+      const int j = idx & (LMAX - 1);
+      const int k = idx / LMAX;
+      if (j < L) out[Atab[k] + j] = scl(sm[j * SEQ + pad8(k)], sc);
+    }
+  } else if (KIND == P_R2C) {
+    C* __restrict__ out = reinterpret_cast<C*>(A.out);
+    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+      const int j = idx & (LMAX - 1);
+      const int k = idx / LMAX;
+      if (j < L) {
+        const C* seq = sm + (j >> 1) * SEQ;
+        const C a = seq[pad8(k)];
+        const C b = seq[pad8((N - k) & (N - 1))];
+        R f = sc * R(0.5);
+        if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
+        out[Atab[k] + j] = (j & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f) : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+      }
+    }
+  } else {  // C2R, transposed real store
+    R* __restrict__ out = reinterpret_cast<R*>(A.out);
+    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+      const int j = idx & (LMAX - 1);
+      const int k = idx / LMAX;
+      if (j < L) {
+        const C z = sm[(j >> 1) * SEQ + pad8(k)];
+        out[Atab[k] + j] = ((j & 1) ? z.y : z.x) * sc;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side dispatch
+// ---------------------------------------------------------------------------
+template <typename R, int N>
+static int p2_lines(int kind) {
+  return kind == P_C2C ? P2Geom<R, N>::NSEQ : 2 * P2Geom<R, N>::NSEQ;
+}
+
+template <typename R, int N>
+static size_t p2_smem(int kind) {
+  const int nout = (kind == P_R2C) ? N / 2 + 1 : N;
+  return (size_t)P2Geom<R, N>::NSEQ * P2Geom<R, N>::SEQ * sizeof(typename Cx<R>::T) + (size_t)nout * 8;
+}
+
+template <typename R, int N, int KIND, bool INV, bool DIRECT>
+static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
+  const size_t smem = p2_smem<R, N>(KIND);
+  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT>;
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  fn<<<dim3((unsigned)A.ntiles), P2_THREADS, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+template <typename R, int N>
+static cudaError_t p2_dispatch_n(const PassArgs& A, cudaStream_t stream) {
+  const bool direct = A.dst_k_contig != 0;
+  switch (A.kind) {
+    case P_C2C:
+      if (A.inv)
+        return direct ? p2_launch<R, N, P_C2C, true, true>(A, stream) : p2_launch<R, N, P_C2C, true, false>(A, stream);
+      return direct ? p2_launch<R, N, P_C2C, false, true>(A, stream) : p2_launch<R, N, P_C2C, false, false>(A, stream);
+    case P_R2C:
+      return direct ? p2_launch<R, N, P_R2C, false, true>(A, stream) : p2_launch<R, N, P_R2C, false, false>(A, stream);
+    case P_C2R:
+      return direct ? p2_launch<R, N, P_C2R, true, true>(A, stream) : p2_launch<R, N, P_C2R, true, false>(A, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename R>
+static cudaError_t p2_dispatch(const PassArgs& A, cudaStream_t stream) {
+  switch (A.m) {
+    case 32: return p2_dispatch_n<R, 32>(A, stream);
+    case 64: return p2_dispatch_n<R, 64>(A, stream);
+    case 128: return p2_dispatch_n<R, 128>(A, stream);
+    case 256: return p2_dispatch_n<R, 256>(A, stream);
+    case 512: return p2_dispatch_n<R, 512>(A, stream);
+    case 1024: return p2_dispatch_n<R, 1024>(A, stream);
+    case 2048: return p2_dispatch_n<R, 2048>(A, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename R>
+static int p2_lines_r(int m, int kind) {
+  switch (m) {
+    case 32: return p2_lines<R, 32>(kind);
+    case 64: return p2_lines<R, 64>(kind);
+    case 128: return p2_lines<R, 128>(kind);
+    case 256: return p2_lines<R, 256>(kind);
+    case 512: return p2_lines<R, 512>(kind);
+    case 1024: return p2_lines<R, 1024>(kind);
+    case 2048: return p2_lines<R, 2048>(kind);
+    default: return 0;
+  }
+}
+
+int pow2_lines(int m, int kind, int real_bytes) {
+  return real_bytes == 4 ? p2_lines_r<float>(m, kind) : p2_lines_r<double>(m, kind);
+}
+
+cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.ntiles <= 0) return cudaSuccess;
+  if (A.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+  return real_bytes == 4 ? p2_dispatch<float>(A, stream) : p2_dispatch<double>(A, stream);
+}
+
+}  // namespace pb

@@ -384,3 +384,69 @@ def test_vjp_adjoint_identity_f64(family):
         lhs = _dot(to_host(ax), to_host(y))
         rhs = _dot(to_host(x), to_host(aty))
         assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (op, lhs, rhs)
+
+
+POW2_CASES = [((2, 3), (64, 128, 256), (2,)), ((4, 2), (256, 32, 512), ()), ((2, 2), (2048, 8, 32), ()),
+              ((3,), (32, 1024, 64), ()), ((4, 8), (64, 64, 128), ())]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape,extra", POW2_CASES)
+def test_pow2_register_kernel_c2c_and_r2c(rb, dims, shape, extra):
+    """Power-of-two lengths take the register-resident pass kernel."""
+    rng = np.random.default_rng(10)
+    topo = pb.MpiTopology(dims)
+    e = int(np.prod(extra)) if extra else 1
+    plan = pb.C2cPlan.from_shape(topo, shape, extra, dtype=CDT[rb])
+    route = po.c2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, extra, True, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, e, rb, True, d)
+    plan = pb.R2cPlan.from_shape(topo, shape, extra, dtype=RDT[rb])
+    route = po.r2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, extra, False, rb)
+    check_transform(plan, route, x, e, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), (e,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, e, rb, True, d)
+
+
+@pytest.mark.parametrize("family", ["r2c", "c2r", "c2c"])
+def test_pow2_vjp_adjoint_identity_f64(family):
+    rng = np.random.default_rng(11)
+    topo = pb.MpiTopology((2, 2))
+    if family == "r2c":
+        plan = pb.R2cPlan.from_shape(topo, (32, 64, 64), (), dtype=torch.float64)
+    elif family == "c2r":
+        plan = pb.C2rPlan.from_shape(topo, (33, 64, 32), 64, (), dtype=torch.float64)
+    else:
+        plan = pb.C2cPlan.from_shape(topo, (32, 64, 128), (), dtype=torch.complex128)
+
+    def rnd(n, dtype):
+        if dtype.is_complex:
+            return torch.from_numpy(rng.standard_normal(n) + 1j * rng.standard_normal(n)).to("cuda", dtype)
+        return torch.from_numpy(rng.standard_normal(n)).to("cuda", dtype)
+
+    ni, no = plan.info.input_elems, plan.info.output_elems
+    for op, vjp in (("forward", "vjp_forward"), ("inverse", "vjp_inverse"), ("backward", "vjp_backward")):
+        fwd_like = op == "forward"
+        a_in, a_out = (plan.input_dtype, plan.output_dtype) if fwd_like else (plan.output_dtype, plan.input_dtype)
+        n_in, n_out = (ni, no) if fwd_like else (no, ni)
+        if family == "r2c" and not fwd_like:
+            x = torch.zeros(n_in, dtype=a_in, device="cuda")
+            plan.forward(rnd(ni, plan.input_dtype), x)
+        elif family == "c2r" and fwd_like:
+            x = torch.zeros(n_in, dtype=a_in, device="cuda")
+            plan.backward(rnd(no, plan.output_dtype), x)
+        else:
+            x = rnd(n_in, a_in)
+        y = rnd(n_out, a_out)
+        ax = torch.zeros(n_out, dtype=a_out, device="cuda")
+        getattr(plan, op)(x, ax)
+        aty = torch.zeros(n_in, dtype=a_in, device="cuda")
+        getattr(plan, vjp)(y, aty)
+        torch.cuda.synchronize()
+        lhs = _dot(to_host(ax), to_host(y))
+        rhs = _dot(to_host(x), to_host(aty))
+        assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (op, lhs, rhs)
