@@ -123,26 +123,45 @@ __global__ void exchange_kernel(const ExchArgs A) {
 // ---------------------------------------------------------------------------
 // C2R endpoint statistics (validate_boundary, distributed/r2c.rs:4709-4807;
 // EndpointStatistics, distributed.rs:4205-4370): per extra batch and plane
-// (DC; Nyquist for even n) max(|re|,|im|), max|im|, then sums of squares scaled
-// by the first maximum; accept a plane if max|im| <= absolute or
-// ||im|| <= relative * ||re||; any non-finite value rejects.
+// (DC; Nyquist for even n) max(|re|,|im|), max|im| and the sums of squares;
+// accept a plane if max|im| <= absolute or ||im|| <= relative * ||re||; any
+// non-finite value rejects.  One block per (batch, plane, rank) walks that
+// rank's plane points with plain stride arithmetic; the last block to finish
+// takes the decision.  f32 data: one pass with unscaled f64 sums (squares of
+// f32 values cannot overflow f64, and the comparison is scale-invariant).
+// f64 data: the reference's two passes (maxima, then sums scaled by the
+// maximum).
 // ---------------------------------------------------------------------------
 template <typename R>
-__device__ __forceinline__ void plane_value(const StatsArgs& A, long long group, long long i, double* re,
+__device__ __forceinline__ bool plane_point(const StatsArgs& A, long long group, long long i, double* re,
                                             double* im) {
-  const long long e = group / A.nplanes;
-  const int plane = (int)(group - e * A.nplanes);
-  int g[MAXN];
-  long long rem = i;
-  for (int q = A.nother - 1; q >= 0; --q) {
-    g[A.other_axes[q]] = (int)(rem % A.other_ext[q]);
-    rem /= A.other_ext[q];
+  const DevPencil& p = A.pen;
+  const long long per_e = (long long)A.nplanes * p.nranks;
+  const long long e = group / per_e;
+  const long long rem = group - e * per_e;
+  const int plane = (int)(rem / p.nranks);
+  const int r = (int)(rem - (long long)plane * p.nranks);
+  const long long* inf = p.info + (long long)r * info_words(p.N);
+  const int red = A.red_axis;
+  const int kp = plane == 0 ? 0 : A.real_len / 2;
+  const long long s_red = inf[2 + red], ext_red = inf[2 + 2 * p.N + red];
+  if (kp < s_red || kp >= s_red + ext_red) return false;
+  long long off = inf[0] + e * inf[1] + (kp - s_red) * inf[2 + p.N + red];
+  long long rest = i;
+  for (int q = p.N - 1; q >= 0; --q) {
+    const int ax = p.perm[q];
+    if (ax == red) continue;
+    const long long ext = inf[2 + 2 * p.N + ax];
+    if (ext == 0) return false;
+    const long long c = rest % ext;
+    rest /= ext;
+    off += c * inf[2 + p.N + ax];
   }
-  g[A.red_axis] = plane == 0 ? 0 : A.real_len / 2;
-  const long long off = locate0(A.pen, e, g);
+  if (rest != 0) return false;  // beyond this rank's plane
   const R* d = reinterpret_cast<const R*>(A.data);
   *re = (double)d[2 * off];
   *im = (double)d[2 * off + 1];
+  return true;
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
@@ -150,74 +169,105 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
-template <typename R>
-__global__ void stats_max_kernel(const StatsArgs A) {
+__device__ void stats_decide(const StatsArgs& A) {
+  const long long groups = A.extra * A.nplanes;
+  for (long long gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+    const volatile double* acc = A.acc + gi * 4;
+    const double m0 = acc[0], m1 = acc[1], s0 = acc[2], s1 = acc[3];
+    bool ok = isfinite(m0) && isfinite(m1) && isfinite(s0) && isfinite(s1) && isfinite(A.relative) &&
+              isfinite(A.absolute);
+    const bool absolute_ok = m1 <= A.absolute;
+    const bool relative_ok = sqrt(s1) <= A.relative * sqrt(s0);
+    if (!(absolute_ok || relative_ok)) ok = false;
+    if (!ok) atomicOr(A.status, 1);
+  }
+  if (threadIdx.x == 0 && *(volatile int*)(A.status + 1) != 0) atomicOr(A.status, 1);
+}
+
+// block-wide reduction of up to 4 doubles (max, max, sum, sum) + flag
+__device__ __forceinline__ void block_reduce4(double* v, int* bad, double (*sh)[4], int* shbad) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] = fmax(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+    v[1] = fmax(v[1], __shfl_xor_sync(0xffffffffu, v[1], o));
+    v[2] += __shfl_xor_sync(0xffffffffu, v[2], o);
+    v[3] += __shfl_xor_sync(0xffffffffu, v[3], o);
+    *bad |= __shfl_xor_sync(0xffffffffu, *bad, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    for (int k = 0; k < 4; ++k) sh[w][k] = v[k];
+    shbad[w] = *bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) {
+      v[0] = fmax(v[0], sh[ww][0]);
+      v[1] = fmax(v[1], sh[ww][1]);
+      v[2] += sh[ww][2];
+      v[3] += sh[ww][3];
+      *bad |= shbad[ww];
+    }
+  }
+}
+
+// MODE 0: f32 single pass; MODE 1: f64 maxima; MODE 2: f64 scaled sums.
+template <typename R, int MODE>
+__global__ void __launch_bounds__(256) stats_kernel(const StatsArgs A) {
+  __shared__ double sh[8][4];
+  __shared__ int shbad[8];
+  __shared__ int s_last;
   const long long group = blockIdx.y;
-  double mx = 0.0, mi = 0.0;
+  const long long acc_group = group / A.pen.nranks;  // (batch, plane)
+  double* acc = A.acc + acc_group * 4;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
   int bad = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.plane_points;
+  double scale = 1.0;
+  bool scaled = false;
+  if (MODE == 2) {
+    scale = acc[0];
+    scaled = scale != 0.0 && isfinite(scale);
+  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.max_points;
        i += (long long)gridDim.x * blockDim.x) {
     double re, im;
-    plane_value<R>(A, group, i, &re, &im);
+    if (!plane_point<R>(A, group, i, &re, &im)) break;
     if (!isfinite(re) || !isfinite(im)) {
       bad = 1;
       continue;
     }
-    mx = fmax(mx, fmax(fabs(re), fabs(im)));
-    mi = fmax(mi, fabs(im));
+    if (MODE != 2) {
+      v[0] = fmax(v[0], fmax(fabs(re), fabs(im)));
+      v[1] = fmax(v[1], fabs(im));
+    }
+    if (MODE == 0) {
+      v[2] += re * re;
+      v[3] += im * im;
+    } else if (MODE == 2 && scaled) {
+      const double nr = re / scale, ni = im / scale;
+      v[2] += nr * nr;
+      v[3] += ni * ni;
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
-    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    double* acc = A.acc + group * 4;
-    atomic_max_nonneg(acc + 0, mx);
-    atomic_max_nonneg(acc + 1, mi);
+  block_reduce4(v, &bad, sh, shbad);
+  if (threadIdx.x == 0) {
+    if (MODE != 2) {
+      atomic_max_nonneg(acc + 0, v[0]);
+      atomic_max_nonneg(acc + 1, v[1]);
+    }
+    if (MODE != 1 && (v[2] != 0.0 || v[3] != 0.0)) {
+      atomicAdd(acc + 2, v[2]);
+      atomicAdd(acc + 3, v[3]);
+    }
     if (bad) atomicOr(A.status + 1, 1);
+    __threadfence();
+    const unsigned total = gridDim.x * gridDim.y;
+    s_last = (MODE != 1) && (atomicAdd(A.counter, 1u) == total - 1);
   }
-}
-
-template <typename R>
-__global__ void stats_sum_kernel(const StatsArgs A) {
-  const long long group = blockIdx.y;
-  double* acc = A.acc + group * 4;
-  const double scale = acc[0];
-  if (!(scale != 0.0 && isfinite(scale))) return;
-  double sr = 0.0, si = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.plane_points;
-       i += (long long)gridDim.x * blockDim.x) {
-    double re, im;
-    plane_value<R>(A, group, i, &re, &im);
-    if (!isfinite(re) || !isfinite(im)) continue;
-    const double nr = re / scale, ni = im / scale;
-    sr += nr * nr;
-    si += ni * ni;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    stats_decide(A);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    sr += __shfl_xor_sync(0xffffffffu, sr, o);
-    si += __shfl_xor_sync(0xffffffffu, si, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(acc + 2, sr);
-    atomicAdd(acc + 3, si);
-  }
-}
-
-__global__ void stats_decide_kernel(const StatsArgs A) {
-  const long long groups = A.extra * A.nplanes;
-  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < groups;
-       gi += (long long)gridDim.x * blockDim.x) {
-    const double* acc = A.acc + gi * 4;
-    bool ok = isfinite(acc[0]) && isfinite(acc[1]) && isfinite(acc[2]) && isfinite(acc[3]) &&
-              isfinite(A.relative) && isfinite(A.absolute);
-    const bool absolute_ok = acc[1] <= A.absolute;
-    const bool relative_ok = sqrt(acc[3]) <= A.relative * sqrt(acc[2]);
-    if (!(absolute_ok || relative_ok)) ok = false;
-    if (!ok) atomicOr(A.status, 1);
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && A.status[1] != 0) atomicOr(A.status, 1);
 }
 
 static unsigned grid_for(long long total, int threads, long long cap = 148LL * 16) {
@@ -228,20 +278,18 @@ static unsigned grid_for(long long total, int threads, long long cap = 148LL * 1
 }
 
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream) {
-  const long long groups = A.extra * A.nplanes;
-  if (groups <= 0) return cudaSuccess;
+  const long long groups = A.extra * A.nplanes * A.pen.nranks;
+  if (groups <= 0 || A.max_points <= 0) return cudaSuccess;
   if (groups > 65535) return cudaErrorInvalidValue;
   const int threads = 256;
-  unsigned bx = grid_for(A.plane_points, threads, 256);
-  dim3 grid(bx, (unsigned)groups);
+  const unsigned bx = grid_for(A.max_points, threads, 64);
+  const dim3 grid(bx, (unsigned)groups);
   if (real_bytes == 4) {
-    stats_max_kernel<float><<<grid, threads, 0, stream>>>(A);
-    stats_sum_kernel<float><<<grid, threads, 0, stream>>>(A);
+    stats_kernel<float, 0><<<grid, threads, 0, stream>>>(A);
   } else {
-    stats_max_kernel<double><<<grid, threads, 0, stream>>>(A);
-    stats_sum_kernel<double><<<grid, threads, 0, stream>>>(A);
+    stats_kernel<double, 1><<<grid, threads, 0, stream>>>(A);
+    stats_kernel<double, 2><<<grid, threads, 0, stream>>>(A);
   }
-  stats_decide_kernel<<<grid_for(groups, 128), 128, 0, stream>>>(A);
   return cudaGetLastError();
 }
 

@@ -117,12 +117,10 @@ struct StatsArgs {
   int real_len;
   int nplanes;       // 1 (odd n) or 2
   long long extra;
-  long long plane_points;  // product of the other axes' extents
-  int other_axes[MAXN];
-  int other_ext[MAXN];
-  int nother;
+  long long max_points;  // largest per-rank plane size (points of the other axes)
   double* acc;       // per (batch, plane): [max_all, max_im, sum_re, sum_im]
   int* status;       // [0]: 1 if any plane rejected; [1]: 1 if a value was not finite
+  unsigned int* counter;  // blocks finished (last-block decision)
   double relative;
   double absolute;
 };

@@ -775,16 +775,16 @@ static Step make_stats(pb_plan& P, const Pencil& pen, int red_axis, bool normali
   S.real_len = (int)P.real_len;
   S.nplanes = (P.real_len % 2 == 0) ? 2 : 1;
   S.extra = P.extra;
-  S.nother = 0;
-  long long pts = 1;
-  for (int x = 0; x < pen.N; ++x) {
-    if (x == red_axis) continue;
-    S.other_axes[S.nother] = x;
-    S.other_ext[S.nother] = (int)pen.shape[x];
-    ++S.nother;
-    pts *= pen.shape[x];
+  long long mx = 0;
+  for (int r = 0; r < pen.nranks(); ++r) {
+    long long lo[MAXN], ext[MAXN];
+    pen.local(r, lo, ext);
+    long long pts = 1;
+    for (int x = 0; x < pen.N; ++x)
+      if (x != red_axis) pts *= ext[x];
+    mx = std::max(mx, pts);
   }
-  S.plane_points = pts;
+  S.max_points = mx;
   // thresholds: distributed/r2c.rs:4841-4878, distributed/mixed.rs (MixedR2cPlan contract)
   double depth = 1.0, factor = 1.0;
   for (auto& t : P.terms) {
@@ -1155,6 +1155,7 @@ static int run(pb_plan* P, int op, const void* in, void* out, void* ws, cudaStre
       S.data = slot_ptr(*P, st.src_slot, in, out, ws);
       S.acc = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + P->acc_off);
       S.status = status;
+      S.counter = reinterpret_cast<unsigned int*>(status + 4);
       cuda_ok(launch_stats(S, P->real_bytes, s));
     }
     if (ms) cuda_ok(cudaEventRecord(ev[i + 1], s));
