@@ -228,18 +228,22 @@ def b200_arm(args):
     value = bytes_step * world / (ms * 1e-3) / 1e9
 
     # per-launch device times of the same steps (roofline of the pass kernel)
+    kinds_f = plan.step_kinds(L.FORWARD)
+    kinds_i = plan.step_kinds(L.INVERSE)
     fwd_t, inv_t = [], []
     for _ in range(max(3, min(args.steps, 10))):
         fwd_t.append(plan.execute_timed(L.FORWARD, x, spec, ws, stream))
         inv_t.append(plan.execute_timed(L.INVERSE, spec, back, ws, stream))
-    n_fwd = len(fwd_t[0])
-    n_inv = len(inv_t[0])  # passes plus one spectrum check
-    pass_ms = sum(sum(t) for t in fwd_t) + sum(sum(t[1:]) for t in inv_t)
-    pass_bytes = len(fwd_t) * sum(per_pass) * 2
-    launches = len(fwd_t) * (n_fwd + n_inv - 1)
+    reps = len(fwd_t)
+    pass_ms = sum(t[i] for t in fwd_t for i, k in enumerate(kinds_f) if k == "pass") + \
+        sum(t[i] for t in inv_t for i, k in enumerate(kinds_i) if k == "pass")
+    check_ms = sum(t[i] for t in inv_t for i, k in enumerate(kinds_i) if k == "check") / reps
+    launches = reps * (kinds_f.count("pass") + kinds_i.count("pass"))
+    pass_bytes = reps * sum(per_pass) * 2
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    check_ms = sum(t[0] for t in inv_t) / len(inv_t)
+    per_pass_ms = [sum(t[i] for t in fwd_t) / reps for i in range(len(kinds_f))] + \
+        [sum(t[i] for t in inv_t) / reps for i in range(len(kinds_i))]
 
     # accuracy: round trip of field A and the known spectrum of field B
     L.check(lib.pb_execute_status(plan._h, hw, sp), "spectrum")
@@ -330,7 +334,11 @@ def b200_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "pb::pass_kernel<float>", "bytes_per_launch": per_pass,
-                         "launch_ms_avg": pass_ms / launches, "spectrum_check_ms": check_ms},
+                         "launch_ms_avg": pass_ms / launches, "spectrum_check_ms": check_ms,
+                         "launch_ms": {"forward": dict(zip([f"{i}:{k}" for i, k in enumerate(kinds_f)],
+                                                           per_pass_ms[:len(kinds_f)])),
+                                       "inverse": dict(zip([f"{i}:{k}" for i, k in enumerate(kinds_i)],
+                                                           per_pass_ms[len(kinds_f):]))}},
             "e2e": {"value": bytes_step / (e2e_ms * 1e-3) / 1e9 * world, "unit": "GB/s", "ms_per_step": e2e_ms,
                     "wall_ms_per_step": e2e_wall_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * (plan.info.passes_forward + plan.info.passes_inverse + 2),

@@ -190,6 +190,11 @@ int pb_execute_status(pb_plan* plan, void* workspace, void* stream);
 int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void* workspace, void* stream,
                      float* stage_ms, int32_t capacity, int32_t* count);
 
+/* Launch kinds of one operation, in order (the stage layout of
+ * TransformTiming): 0 = fused pass (local transform + transition), 1 = C2R
+ * spectrum check.  *count = number of launches. */
+int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capacity, int32_t* count);
+
 /* ---- transposes ------------------------------------------------------- */
 /* AllToAllvTransposePlan::new (crates/pencil-array/src/alltoallv_transpose.rs:65-72). */
 int pb_transpose_create_alltoallv(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,

@@ -54,6 +54,7 @@ struct ExchArgs {
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int pow2_lines(int m, int kind, int real_bytes);
+int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes);
 size_t pass_smem_bytes(const PassArgs& A, int real_bytes);
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_remap(const RemapArgs& A, cudaStream_t stream);

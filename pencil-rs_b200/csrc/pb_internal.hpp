@@ -107,6 +107,28 @@ struct PassArgs {
   const void* aux0;     // kind-specific pre/post twiddles
   const void* aux1;
   const int* gate;      // if non-null and nonzero: spectrum rejected, write nothing
+  // register kernel (pow2_kernel.cu): host-precomputed addressing
+  const void* tile_tab;   // TileAddr per tile
+  const void* piece_tab;  // PieceAddr per (tile, piece of the transform axis in the destination)
+  const int2* ktab;       // per output index k: (piece, local index along the transform axis)
+  int npieces;
+  int grid_ctas;          // persistent grid size
+};
+
+// Per-tile addresses (element offsets into the concatenated rank buffers).
+struct TileAddr {
+  long long src0;  // first element of line 0 in the source
+  long long dst0;  // first element of line 0 in the destination (direct store)
+  int srcb;        // line-to-line stride in the source
+  int dstb;        // line-to-line stride in the destination (direct store)
+  int lines;       // lines in this tile
+  int pad;
+};
+
+// Destination row of one piece (virtual rank) of the transform axis.
+struct PieceAddr {
+  long long rowbase;  // offset of (first index of the piece, line 0)
+  long long stride;   // memory stride of the transform axis in that rank
 };
 
 // Endpoint statistics of the C2R boundary (distributed/r2c.rs:4709-4807).

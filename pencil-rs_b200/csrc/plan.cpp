@@ -373,6 +373,58 @@ static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size
   return d;
 }
 
+// Host restatement of the device addressing (pb_device.cuh: locate).
+struct HostLayout {
+  const Pencil& p;
+  long long extra;
+  std::vector<long long> base, len;
+  std::vector<std::array<long long, MAXN>> lo, ext, stride;
+  int rstride[MAXM];
+  HostLayout(const Pencil& pen, long long e) : p(pen), extra(e) {
+    const int R = p.nranks();
+    base.resize(R);
+    len.resize(R);
+    lo.resize(R);
+    ext.resize(R);
+    stride.resize(R);
+    long long b = 0;
+    for (int r = 0; r < R; ++r) {
+      p.local(r, lo[r].data(), ext[r].data());
+      long long l = 1;
+      for (int x = 0; x < p.N; ++x) l *= ext[r][x];
+      long long s = 1;
+      for (int q = p.N - 1; q >= 0; --q) {
+        stride[r][p.perm[q]] = s;
+        s *= ext[r][p.perm[q]];
+      }
+      base[r] = b;
+      len[r] = l;
+      b += l * extra;
+    }
+    int rs = 1;
+    for (int t = p.M - 1; t >= 0; --t) {
+      rstride[t] = rs;
+      rs *= p.grid[t];
+    }
+  }
+  int rank(const long long* g) const {
+    int r = 0;
+    for (int t = 0; t < p.M; ++t) {
+      const int ax = p.dec[t];
+      const long long c = ((g[ax] + 1) * p.grid[t] - 1) / p.shape[ax];
+      r += (int)c * rstride[t];
+    }
+    return r;
+  }
+  long long offset(long long e, const long long* g, int* r_out) const {
+    const int r = rank(g);
+    long long o = base[r] + e * len[r];
+    for (int x = 0; x < p.N; ++x) o += (g[x] - lo[r][x]) * stride[r][x];
+    if (r_out) *r_out = r;
+    return o;
+  }
+};
+
 // exp(-2 pi i q/m) (negative exponent) in extended precision, rounded once.
 static size_t roots_table(pb_plan& P, int m) {
   const std::string key = "W" + std::to_string(m) + "r" + std::to_string(P.real_bytes);
@@ -637,6 +689,81 @@ static int choose_lines(pb_plan& P, PassArgs& A, int pair_kind) {
   }
 }
 
+// Tile, piece and k tables of the register kernel, in the tile order of the
+// generic kernel: tile = ((e * outer) + outer_index) * nchunks + chunk.
+static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const Pencil& dst,
+                              const std::vector<int2>& chunks) {
+  HostLayout hs(src, P.extra), hd(dst, P.extra);
+  const int N = src.N;
+  const bool direct = A.dst_k_contig != 0;
+  const int ta = dst.split_of(A.a);
+  const int npieces = direct ? 1 : (ta >= 0 ? dst.grid[ta] : 1);
+  const long long nout = dst.shape[A.a];
+  std::vector<TileAddr> tiles((size_t)A.ntiles);
+  std::vector<PieceAddr> pieces(direct ? 0 : (size_t)A.ntiles * npieces);
+  long long outer_total = 1;
+  for (int i = 0; i < A.nouter_axes; ++i) outer_total *= A.outer_ext[i];
+  long long t = 0;
+  for (long long e = 0; e < P.extra; ++e) {
+    for (long long o = 0; o < outer_total; ++o) {
+      long long g[MAXN] = {};
+      long long rem = o;
+      for (int i = A.nouter_axes - 1; i >= 0; --i) {
+        g[A.outer_axis[i]] = rem % A.outer_ext[i];
+        rem /= A.outer_ext[i];
+      }
+      for (const int2& c : chunks) {
+        g[A.b] = c.x;
+        g[A.a] = 0;
+        TileAddr& ta_ = tiles[(size_t)t];
+        int r;
+        ta_.src0 = hs.offset(e, g, &r);
+        ta_.srcb = (int)hs.stride[r][A.b];
+        ta_.lines = c.y;
+        ta_.pad = 0;
+        if (direct) {
+          ta_.dst0 = hd.offset(e, g, &r);
+          ta_.dstb = (int)hd.stride[r][A.b];
+        } else {
+          ta_.dst0 = 0;
+          ta_.dstb = 0;
+          for (int p = 0; p < npieces; ++p) {
+            const long long st = Pencil::part(nout, npieces, p), en = Pencil::part(nout, npieces, p + 1);
+            PieceAddr& pa = pieces[(size_t)t * npieces + p];
+            if (en <= st) {
+              pa.rowbase = 0;
+              pa.stride = 0;
+              continue;
+            }
+            g[A.a] = st;
+            pa.rowbase = hd.offset(e, g, &r);
+            pa.stride = hd.stride[r][A.a];
+          }
+          g[A.a] = 0;
+        }
+        ++t;
+      }
+    }
+  }
+  (void)N;
+  A.tile_tab = enc(P.host.add(tiles.data(), tiles.size() * sizeof(TileAddr)));
+  if (!direct) {
+    A.piece_tab = enc(P.host.add(pieces.data(), pieces.size() * sizeof(PieceAddr)));
+    std::vector<int2> kt((size_t)nout);
+    for (long long k = 0; k < nout; ++k) {
+      const int p = (npieces > 1) ? (int)(((k + 1) * npieces - 1) / nout) : 0;
+      kt[(size_t)k].x = p;
+      kt[(size_t)k].y = (int)(k - Pencil::part(nout, npieces, p));
+    }
+    A.ktab = reinterpret_cast<const int2*>(enc(P.host.add(kt.data(), kt.size() * sizeof(int2))));
+  }
+  A.npieces = npieces;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int occ = pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
+  A.grid_ctas = sms * std::max(1, occ);
+}
+
 // One fused pass for `st` under `op` from layout `src` to layout `dst`.
 static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Pencil& src, const Pencil& dst,
                       bool in_complex, bool out_complex) {
@@ -751,6 +878,7 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   A.ntiles = tiles;
   A.src = dev_pencil(P, P.host, P.cache, src, P.extra);
   A.dst = dev_pencil(P, P.host, P.cache, dst, P.extra);
+  if (A.fast) build_fast_tables(P, A, src, dst, chunks);
   return s;
 }
 
@@ -898,6 +1026,11 @@ static void finalize(pb_plan& P) {
         fix(s.pa.twiddle);
         fix(s.pa.aux0);
         fix(s.pa.aux1);
+        fix(s.pa.tile_tab);
+        fix(s.pa.piece_tab);
+        const void* kt = s.pa.ktab;
+        fix(kt);
+        s.pa.ktab = reinterpret_cast<const int2*>(kt);
         fixpen(s.pa.src);
         fixpen(s.pa.dst);
       } else {
@@ -1418,6 +1551,20 @@ int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void*
   });
 }
 
+int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capacity, int32_t* count) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    const Program& prog = plan->prog[user_mode(*plan, op)];
+    int n = 0;
+    for (const Step& s : prog.steps) {
+      if (kinds && n < capacity) kinds[n] = s.type;
+      ++n;
+    }
+    if (count) *count = n;
+    return (int)PB_OK;
+  });
+}
+
 int pb_execute_status(pb_plan* plan, void* workspace, void* stream) {
   return guard([&] {
     if (!plan || !workspace) return (int)PB_ENULL;
@@ -1459,6 +1606,11 @@ static void upload_steps(pb_plan& P, std::vector<Step>& steps) {
     fix(s.pa.twiddle);
     fix(s.pa.aux0);
     fix(s.pa.aux1);
+    fix(s.pa.tile_tab);
+    fix(s.pa.piece_tab);
+    const void* kt = s.pa.ktab;
+    fix(kt);
+    s.pa.ktab = reinterpret_cast<const int2*>(kt);
     fixpen(s.pa.src);
     fixpen(s.pa.dst);
   }

@@ -2,17 +2,20 @@
 // hot path of the canonical route (every stage axis is contiguous in its own
 // layout, so each line is one contiguous run in one virtual rank).
 //
+// Persistent CTAs walk the tiles of the pass (tile = blockIdx.x + i*gridDim.x).
 // Per tile of L lines: each line (or pair of real lines) is one complex
 // sequence handled by T = n/8 threads holding 8 elements each.  Loads go from
 // global straight into registers (coalesced: thread t of a line reads
-// elements t + T*m).  Stockham stages run in registers with a radix 2/4 lead
-// stage and radix-8 stages; between stages the 8 values per thread are
-// exchanged through padded shared memory.  Twiddles come from the table of
-// n-th roots (generated on the host in extended precision, rounded once) and
-// stay in registers for the whole tile.  The results are stored either
-// directly (transform axis contiguous in the destination) or through shared
-// memory transposed so that the L lines of a tile form contiguous runs of the
-// destination's innermost axis (the fused pencil transpose).
+// elements t + T*m), and the next tile's loads are issued before the current
+// tile is transformed, so HBM latency overlaps the arithmetic.  Stockham
+// stages run in registers with a radix 2/4 lead stage and radix-8 stages;
+// between stages the 8 values per thread are exchanged through padded shared
+// memory.  Twiddles come from the table of n-th roots (generated on the host
+// in extended precision, rounded once) and stay in registers for the whole
+// kernel.  Results are stored either directly (transform axis contiguous in
+// the destination) or through shared memory transposed so that the L lines of
+// a tile form contiguous runs of the destination's innermost axis (the fused
+// pencil transpose).  Tile and row addresses are precomputed on the host.
 #include <cuda_runtime.h>
 
 #include "pb_aux.hpp"
@@ -22,7 +25,6 @@
 namespace pb {
 
 constexpr int P2_THREADS = 256;
-constexpr int P2_MAXPIECES = 64;
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 __host__ __device__ constexpr int ipow8(int s) { return s == 0 ? 1 : 8 * ipow8(s - 1); }
@@ -41,7 +43,7 @@ template <typename R, int N>
 struct P2Geom {
   static constexpr int T = N / 8;
   static constexpr int SLOTS = P2_THREADS / T;
-  static constexpr int LPT = (sizeof(R) == 4 && N >= 64) ? 2 : 1;
+  static constexpr int LPT = (sizeof(R) == 4 && N >= 64 && N <= 512) ? 2 : 1;
   static constexpr int NSEQ = SLOTS * LPT;
   static constexpr int SEQ = N + N / 8 + 1;  // padded sequence stride (complex units)
 };
@@ -50,7 +52,7 @@ __device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
 
 // One Stockham stage on the 8 register values of each of the thread's sequences.
 template <typename C, int N, int ST, bool INV, int LPT>
-__device__ __forceinline__ void p2_stage(C (&v)[LPT][8], const C (&tw)[Sched<N>::NST][7], int t) {
+__device__ __forceinline__ void p2_stage(C (&v)[LPT][8], const C (&tw)[Sched<N>::NST][7]) {
   using S = Sched<N>;
   constexpr int RAD = S::radix(ST);
   constexpr int NS = S::ns(ST);
@@ -74,21 +76,86 @@ __device__ __forceinline__ void p2_stage(C (&v)[LPT][8], const C (&tw)[Sched<N>:
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[i][q] = out[q];
   }
-  (void)t;
 }
 
-// Output position of value q (= u*RAD + r) of a stage for thread t.
+// Output position of value q (= u*RAD + r) of stage ST for thread t.
 template <int N, int ST>
 __device__ __forceinline__ int p2_out_index(int t, int q) {
   using S = Sched<N>;
   constexpr int RAD = S::radix(ST);
   constexpr int NS = S::ns(ST);
-  constexpr int U = 8 / RAD;
   const int u = q / RAD, r = q - u * RAD;
   const int jb = t + u * S::T;
   const int k = jb & (NS - 1);
   return (jb - k) * RAD + k + r * NS;
-  (void)U;
+}
+
+// Loads the thread's sequences of one tile into registers.
+template <typename R, int N, int KIND, int LPT>
+__device__ __forceinline__ void p2_load(typename Cx<R>::T (&v)[LPT][8], const PassArgs& A, const TileAddr& ta,
+                                        int slot, int t) {
+  using C = typename Cx<R>::T;
+  constexpr int T = N / 8;
+  constexpr int SLOTS = P2_THREADS / T;
+  const R zero = R(0);
+  const int L = ta.lines;
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int s = slot + SLOTS * i;
+    if (KIND == P_C2C) {
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok = s < L;
+      const long long base = ta.src0 + (long long)s * ta.srcb + t;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[i][m] = ok ? in[base + T * m] : mk<C, R>(zero, zero);
+    } else if (KIND == P_R2C) {
+      const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb + t;
+      const long long b1 = b0 + ta.srcb;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[i][m] = mk<C, R>(ok0 ? in[b0 + T * m] : zero, ok1 ? in[b1 + T * m] : zero);
+    } else {  // P_C2R: Hermitian extension of two half spectra
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
+      const long long b1 = b0 + ta.srcb;
+      const R w_in = R(A.pre_factor);
+      const bool weighted = A.pre_mode == W_HALF_INTERIOR;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int q = t + T * m;
+        const bool mirror = q > N / 2;
+        const int hq = mirror ? N - q : q;
+        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
+        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
+        const bool edge = (hq == 0) || (hq == N / 2);
+        if (mirror) {
+          X.y = -X.y;
+          Y.y = -Y.y;
+        }
+        if (edge) {
+          X.y = zero;
+          Y.y = zero;
+        }
+        const R w = (weighted && !edge) ? w_in : R(1);
+        v[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) {
+  const longlong2* p = reinterpret_cast<const longlong2*>(tab + t);
+  const longlong2 r0 = p[0], r1 = p[1];
+  TileAddr a;
+  a.src0 = r0.x;
+  a.dst0 = r0.y;
+  a.srcb = (int)(r1.x & 0xffffffffLL);
+  a.dstb = (int)(r1.x >> 32);
+  a.lines = (int)(r1.y & 0xffffffffLL);
+  a.pad = 0;
+  return a;
 }
 
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
@@ -107,70 +174,18 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   C* sm = reinterpret_cast<C*>(smem);
   long long* Atab = reinterpret_cast<long long*>(sm + NSEQ * SEQ);
-  __shared__ long long s_src0, s_dst0, s_rowbase[P2_MAXPIECES];
-  __shared__ int s_srcb, s_dstb, s_stride_a[P2_MAXPIECES], s_pstart[P2_MAXPIECES];
 
   if (A.gate != nullptr && *A.gate != 0) return;
+  long long tile = blockIdx.x;
+  if (tile >= A.ntiles) return;
   const int tid = threadIdx.x;
   const int slot = tid / T;
   const int t = tid - slot * T;
+  const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
+  const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
 
-  // ---- tile decode
-  const long long tile = blockIdx.x;
-  const int ci = (int)(tile % A.nchunks);
-  long long outer = tile / A.nchunks;
-  const int2 ch = A.chunks[ci];
-  int g[MAXN];
-#pragma unroll
-  for (int x = 0; x < MAXN; ++x) g[x] = 0;
-  for (int i = A.nouter_axes - 1; i >= 0; --i) {
-    g[A.outer_axis[i]] = (int)(outer % A.outer_ext[i]);
-    outer /= A.outer_ext[i];
-  }
-  const long long e = outer;
-  g[A.b] = ch.x;
-  const int L = ch.y;
-  g[A.a] = 0;
-
-  // ---- per-tile addressing
-  if (tid == 0) {
-    int sb;
-    s_src0 = locate(A.src, e, g, A.b, &sb);
-    s_srcb = sb;
-    if (DIRECT) {
-      int db;
-      s_dst0 = locate(A.dst, e, g, A.b, &db);
-      s_dstb = db;
-    }
-  }
-  int npieces = 1;
-  int ta = -1;
-  if (!DIRECT) {
-    ta = A.dst.split[A.a];
-    npieces = ta >= 0 ? A.dst.gdim[ta] : 1;
-    for (int p = tid; p < npieces; p += P2_THREADS) {
-      const int start = (int)(((long long)NOUT * p) / npieces);
-      int gg[MAXN];
-#pragma unroll
-      for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
-      gg[A.a] = start;
-      const int end = (int)(((long long)NOUT * (p + 1)) / npieces);
-      int sa = 0;
-      s_rowbase[p] = (end > start) ? locate(A.dst, e, gg, A.a, &sa) : 0;
-      s_stride_a[p] = sa;
-      s_pstart[p] = start;
-    }
-  }
-  __syncthreads();
-  if (!DIRECT) {
-    for (int k = tid; k < NOUT; k += P2_THREADS) {
-      const int p = (ta >= 0) ? owner_of(k, NOUT, npieces) : 0;
-      Atab[k] = s_rowbase[p] + (long long)(k - s_pstart[p]) * s_stride_a[p];
-    }
-  }
-
-  // ---- twiddles of this thread (constant over the tile): stage ST > 0 uses
-  // W_N^{k*r*N/(NS*8)} with k = t mod NS (NS divides T for every radix-8 stage)
+  // twiddles of this thread, fixed for the whole kernel: stage ST > 0 (radix 8)
+  // multiplies input r by W_N^{k*r*N/(NS*8)} with k = t mod NS
   const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
   C tw[S::NST][7];
 #pragma unroll
@@ -184,192 +199,167 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 #pragma unroll
   for (int r = 0; r < 7; ++r) tw[0][r] = mk<C, R>(R(1), R(0));
 
-  // ---- load: global -> registers
-  const long long src0 = s_src0;
-  const long long srcb = s_srcb;
+  const R sc = R(A.scale);
+  const R pf = R(A.post_factor);
+  TileAddr ta = load_tile(tiles, tile);
   C v[LPT][8];
-  const R zero = R(0);
+  p2_load<R, N, KIND, LPT>(v, A, ta, slot, t);
+
+  for (;;) {
+    const long long next = tile + gridDim.x;
+    const bool has_next = next < A.ntiles;
+    TileAddr tn;
+    C nv[LPT][8];
+    if (has_next) {
+      tn = load_tile(tiles, next);
+      p2_load<R, N, KIND, LPT>(nv, A, tn, slot, t);
+    }
+    const int L = ta.lines;
+
+    // ---- Stockham stages
 #pragma unroll
-  for (int i = 0; i < LPT; ++i) {
-    const int s = slot + SLOTS * i;
-    if (KIND == P_C2C) {
-      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
-      const bool ok = s < L;
-      const long long base = src0 + (long long)s * srcb + t;
+    for (int st = 0; st < S::NST; ++st) {
+      if (st > 0) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[i][m] = ok ? in[base + T * m] : mk<C, R>(zero, zero);
-    } else if (KIND == P_R2C) {
-      const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
-      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
-      const long long b0 = src0 + (long long)(2 * s) * srcb + t;
-      const long long b1 = b0 + srcb;
+        for (int i = 0; i < LPT; ++i) {
+          const C* seq = sm + (slot + SLOTS * i) * SEQ;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[i][m] = mk<C, R>(ok0 ? in[b0 + T * m] : zero, ok1 ? in[b1 + T * m] : zero);
-    } else {  // P_C2R: Hermitian extension of two half spectra
-      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
-      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
-      const long long b0 = src0 + (long long)(2 * s) * srcb;
-      const long long b1 = b0 + srcb;
-      const R w_in = R(A.pre_factor);
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int q = t + T * m;
-        const bool mirror = q > N / 2;
-        const int hq = mirror ? N - q : q;
-        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
-        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
-        const bool edge = (hq == 0) || (hq == N / 2);
-        if (mirror) {
-          X.y = -X.y;
-          Y.y = -Y.y;
+          for (int m = 0; m < 8; ++m) v[i][m] = seq[pad8(t + T * m)];
         }
-        if (edge) {
-          X.y = zero;
-          Y.y = zero;
+      }
+      switch (st) {
+        case 0: p2_stage<C, N, 0, INV, LPT>(v, tw); break;
+        case 1: p2_stage<C, N, (S::NST > 1 ? 1 : 0), INV, LPT>(v, tw); break;
+        case 2: p2_stage<C, N, (S::NST > 2 ? 2 : 0), INV, LPT>(v, tw); break;
+        default: p2_stage<C, N, (S::NST > 3 ? 3 : 0), INV, LPT>(v, tw); break;
+      }
+      if (st + 1 < S::NST) {
+        __syncthreads();  // every thread has read the buffer (previous stage or tile)
+#pragma unroll
+        for (int i = 0; i < LPT; ++i) {
+          C* seq = sm + (slot + SLOTS * i) * SEQ;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            int o;
+            switch (st) {
+              case 0: o = p2_out_index<N, 0>(t, q); break;
+              case 1: o = p2_out_index<N, (S::NST > 1 ? 1 : 0)>(t, q); break;
+              default: o = p2_out_index<N, (S::NST > 2 ? 2 : 0)>(t, q); break;
+            }
+            seq[pad8(o)] = v[i][q];
+          }
         }
-        const R w = (A.pre_mode == W_HALF_INTERIOR && !edge) ? w_in : R(1);
-        v[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
+        __syncthreads();
       }
     }
-  }
+    // thread t now holds natural-order outputs t + T*r
 
-  // ---- Stockham stages
-#pragma unroll
-  for (int st = 0; st < S::NST; ++st) {
-    // (st is a compile-time constant after unrolling)
-    if (st > 0) {
-      __syncthreads();
+    if (DIRECT && KIND != P_R2C) {
 #pragma unroll
       for (int i = 0; i < LPT; ++i) {
-        const C* seq = sm + (slot + SLOTS * i) * SEQ;
+        const int s = slot + SLOTS * i;
+        if (KIND == P_C2C) {
+          if (s < L) {
+            C* __restrict__ out = reinterpret_cast<C*>(A.out);
+            const long long base = ta.dst0 + (long long)s * ta.dstb + t;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) v[i][m] = seq[pad8(t + T * m)];
+            for (int r = 0; r < 8; ++r) out[base + T * r] = scl(v[i][r], sc);
+          }
+        } else {  // C2R
+          R* __restrict__ out = reinterpret_cast<R*>(A.out);
+          const long long b0 = ta.dst0 + (long long)(2 * s) * ta.dstb + t;
+          if (2 * s < L) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) out[b0 + T * r] = v[i][r].x * sc;
+          }
+          if (2 * s + 1 < L) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) out[b0 + ta.dstb + T * r] = v[i][r].y * sc;
+          }
+        }
       }
-    }
-    switch (st) {
-      case 0: p2_stage<C, N, 0, INV, LPT>(v, tw, t); break;
-      case 1: p2_stage<C, N, (S::NST > 1 ? 1 : 0), INV, LPT>(v, tw, t); break;
-      case 2: p2_stage<C, N, (S::NST > 2 ? 2 : 0), INV, LPT>(v, tw, t); break;
-      default: p2_stage<C, N, (S::NST > 3 ? 3 : 0), INV, LPT>(v, tw, t); break;
-    }
-    if (st + 1 < S::NST) {
+    } else {
+      // ---- natural-order results to shared memory, then the store
       __syncthreads();
 #pragma unroll
       for (int i = 0; i < LPT; ++i) {
         C* seq = sm + (slot + SLOTS * i) * SEQ;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          int o;
-          switch (st) {
-            case 0: o = p2_out_index<N, 0>(t, q); break;
-            case 1: o = p2_out_index<N, (S::NST > 1 ? 1 : 0)>(t, q); break;
-            default: o = p2_out_index<N, (S::NST > 2 ? 2 : 0)>(t, q); break;
+        for (int r = 0; r < 8; ++r) seq[pad8(t + T * r)] = v[i][r];
+      }
+      if (!DIRECT) {
+        const PieceAddr* pt = pieces + tile * A.npieces;
+        for (int k = tid; k < NOUT; k += P2_THREADS) {
+          const int2 kp = A.ktab[k];
+          const PieceAddr pa = pt[kp.x];
+          Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+        }
+      }
+      __syncthreads();
+      if (KIND == P_R2C && DIRECT) {
+        C* __restrict__ out = reinterpret_cast<C*>(A.out);
+#pragma unroll
+        for (int i = 0; i < LPT; ++i) {
+          const int s = slot + SLOTS * i;
+          const C* seq = sm + s * SEQ;
+          for (int k = t; k < H; k += T) {
+            const C a = seq[pad8(k)];
+            const C b = seq[pad8((N - k) & (N - 1))];
+            R f = sc * R(0.5);
+            if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
+            if (2 * s < L) out[ta.dst0 + (long long)(2 * s) * ta.dstb + k] = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+            if (2 * s + 1 < L)
+              out[ta.dst0 + (long long)(2 * s + 1) * ta.dstb + k] = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
           }
-          seq[pad8(o)] = v[i][q];
         }
-      }
-    }
-  }
-  // after the last (radix-8) stage thread t holds natural-order outputs t + T*r
-
-  const R sc = R(A.scale);
-  if (DIRECT && KIND != P_R2C) {
-    const long long dst0 = s_dst0;
-    const long long dstb = s_dstb;
-#pragma unroll
-    for (int i = 0; i < LPT; ++i) {
-      const int s = slot + SLOTS * i;
-      if (KIND == P_C2C) {
-        if (s < L) {
+      } else {
+        // transposed store: element (k, j) of the tile goes to Atab[k] + j
+        constexpr int TOTAL = LMAX * NOUT;
+        if (KIND == P_C2C) {
           C* __restrict__ out = reinterpret_cast<C*>(A.out);
-          const long long base = dst0 + (long long)s * dstb + t;
-#pragma unroll
-          for (int r = 0; r < 8; ++r) out[base + T * r] = scl(v[i][r], sc);
+          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+            const int j = idx & (LMAX - 1);
+            const int k = idx / LMAX;
+            if (j < L) out[Atab[k] + j] = scl(sm[j * SEQ + pad8(k)], sc);
+          }
+        } else if (KIND == P_R2C) {
+          C* __restrict__ out = reinterpret_cast<C*>(A.out);
+          const bool weighted = A.post_mode == W_HALF_INTERIOR;
+          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+            const int j = idx & (LMAX - 1);
+            const int k = idx / LMAX;
+            if (j < L) {
+              const C* seq = sm + (j >> 1) * SEQ;
+              const C a = seq[pad8(k)];
+              const C b = seq[pad8((N - k) & (N - 1))];
+              R f = sc * R(0.5);
+              if (weighted && k != 0 && k != N / 2) f *= pf;
+              out[Atab[k] + j] = (j & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f)
+                                         : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+            }
+          }
+        } else {  // C2R, transposed real store
+          R* __restrict__ out = reinterpret_cast<R*>(A.out);
+          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+            const int j = idx & (LMAX - 1);
+            const int k = idx / LMAX;
+            if (j < L) {
+              const C z = sm[(j >> 1) * SEQ + pad8(k)];
+              out[Atab[k] + j] = ((j & 1) ? z.y : z.x) * sc;
+            }
+          }
         }
-      } else {  // C2R
-        R* __restrict__ out = reinterpret_cast<R*>(A.out);
-        const long long b0 = dst0 + (long long)(2 * s) * dstb + t;
-        if (2 * s < L) {
-#pragma unroll
-          for (int r = 0; r < 8; ++r) out[b0 + T * r] = v[i][r].x * sc;
-        }
-        if (2 * s + 1 < L) {
-#pragma unroll
-          for (int r = 0; r < 8; ++r) out[b0 + dstb + T * r] = v[i][r].y * sc;
-        }
       }
     }
-    return;
-  }
 
-  // ---- natural-order results to shared memory
-  __syncthreads();
+    if (!has_next) break;
+    tile = next;
+    ta = tn;
 #pragma unroll
-  for (int i = 0; i < LPT; ++i) {
-    C* seq = sm + (slot + SLOTS * i) * SEQ;
+    for (int i = 0; i < LPT; ++i)
 #pragma unroll
-    for (int r = 0; r < 8; ++r) seq[pad8(t + T * r)] = v[i][r];
-  }
-  __syncthreads();
-
-  const R pf = R(A.post_factor);
-  if (KIND == P_R2C && DIRECT) {
-    const long long dst0 = s_dst0;
-    const long long dstb = s_dstb;
-    C* __restrict__ out = reinterpret_cast<C*>(A.out);
-#pragma unroll
-    for (int i = 0; i < LPT; ++i) {
-      const int s = slot + SLOTS * i;
-      const C* seq = sm + s * SEQ;
-      for (int k = t; k < H; k += T) {
-        const C a = seq[pad8(k)];
-        const C b = seq[pad8((N - k) & (N - 1))];
-        R f = sc;
-        if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
-        if (2 * s < L)
-          out[dst0 + (long long)(2 * s) * dstb + k] = mk<C, R>((a.x + b.x) * R(0.5) * f, (a.y - b.y) * R(0.5) * f);
-        if (2 * s + 1 < L)
-          out[dst0 + (long long)(2 * s + 1) * dstb + k] =
-              mk<C, R>((a.y + b.y) * R(0.5) * f, (b.x - a.x) * R(0.5) * f);
-      }
-    }
-    return;
-  }
-
-  // ---- transposed store: the L lines of a tile are contiguous along the
-  // destination's innermost axis; element (k, j) goes to Atab[k] + j.
-  constexpr int TOTAL = LMAX * NOUT;
-  if (KIND == P_C2C) {
-    C* __restrict__ out = reinterpret_cast<C*>(A.out);
-    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-      const int j = idx & (LMAX - 1);
-      const int k = idx / LMAX;
-      if (j < L) out[Atab[k] + j] = scl(sm[j * SEQ + pad8(k)], sc);
-    }
-  } else if (KIND == P_R2C) {
-    C* __restrict__ out = reinterpret_cast<C*>(A.out);
-    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-      const int j = idx & (LMAX - 1);
-      const int k = idx / LMAX;
-      if (j < L) {
-        const C* seq = sm + (j >> 1) * SEQ;
-        const C a = seq[pad8(k)];
-        const C b = seq[pad8((N - k) & (N - 1))];
-        R f = sc * R(0.5);
-        if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
-        out[Atab[k] + j] = (j & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f) : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
-      }
-    }
-  } else {  // C2R, transposed real store
-    R* __restrict__ out = reinterpret_cast<R*>(A.out);
-    for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-      const int j = idx & (LMAX - 1);
-      const int k = idx / LMAX;
-      if (j < L) {
-        const C z = sm[(j >> 1) * SEQ + pad8(k)];
-        out[Atab[k] + j] = ((j & 1) ? z.y : z.x) * sc;
-      }
-    }
+      for (int m = 0; m < 8; ++m) v[i][m] = nv[i][m];
+    __syncthreads();  // the smem of this tile has been read by every thread
   }
 }
 
@@ -393,7 +383,9 @@ static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
   auto fn = pow2_kernel<R, N, KIND, INV, DIRECT>;
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  fn<<<dim3((unsigned)A.ntiles), P2_THREADS, smem, stream>>>(A);
+  long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
+  if (grid > A.ntiles) grid = A.ntiles;
+  fn<<<dim3((unsigned)grid), P2_THREADS, smem, stream>>>(A);
   return cudaGetLastError();
 }
 
@@ -439,6 +431,44 @@ static int p2_lines_r(int m, int kind) {
     case 2048: return p2_lines<R, 2048>(kind);
     default: return 0;
   }
+}
+
+template <typename R, int N, int KIND, bool INV, bool DIRECT>
+static int p2_occ() {
+  int blocks = 0;
+  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2_smem<R, N>(KIND)) != cudaSuccess)
+    return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, P2_THREADS, p2_smem<R, N>(KIND)) != cudaSuccess)
+    return 1;
+  return blocks > 0 ? blocks : 1;
+}
+
+template <typename R, int N>
+static int p2_occ_n(int kind, int inv, int direct) {
+  if (kind == P_C2C)
+    return inv ? (direct ? p2_occ<R, N, P_C2C, true, true>() : p2_occ<R, N, P_C2C, true, false>())
+               : (direct ? p2_occ<R, N, P_C2C, false, true>() : p2_occ<R, N, P_C2C, false, false>());
+  if (kind == P_R2C) return direct ? p2_occ<R, N, P_R2C, false, true>() : p2_occ<R, N, P_R2C, false, false>();
+  return direct ? p2_occ<R, N, P_C2R, true, true>() : p2_occ<R, N, P_C2R, true, false>();
+}
+
+template <typename R>
+static int p2_occ_r(int m, int kind, int inv, int direct) {
+  switch (m) {
+    case 32: return p2_occ_n<R, 32>(kind, inv, direct);
+    case 64: return p2_occ_n<R, 64>(kind, inv, direct);
+    case 128: return p2_occ_n<R, 128>(kind, inv, direct);
+    case 256: return p2_occ_n<R, 256>(kind, inv, direct);
+    case 512: return p2_occ_n<R, 512>(kind, inv, direct);
+    case 1024: return p2_occ_n<R, 1024>(kind, inv, direct);
+    default: return p2_occ_n<R, 2048>(kind, inv, direct);
+  }
+}
+
+// Resident CTAs per SM of the register kernel for (length, kind, sign, store mode).
+int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes) {
+  return real_bytes == 4 ? p2_occ_r<float>(m, kind, inv, direct) : p2_occ_r<double>(m, kind, inv, direct);
 }
 
 int pow2_lines(int m, int kind, int real_bytes) {

@@ -73,6 +73,7 @@ SIGNATURES = {
     "pb_plan_pencil": ([_P, C.c_int32, C.POINTER(PbPencilDesc)], C.c_int),
     "pb_execute": ([_P, C.c_int32, _P, _P, _P, _P], C.c_int),
     "pb_execute_status": ([_P, _P, _P], C.c_int),
+    "pb_plan_steps": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),
     "pb_transpose_create_alltoallv": ([C.POINTER(PbPencilDesc), C.POINTER(PbPencilDesc), C.c_int64, C.c_int32,

@@ -263,6 +263,15 @@ class _Plan:
                                           ms, cap, C.byref(cnt)), "execute_timed")
         return [ms[i] for i in range(cnt.value)]
 
+    def step_kinds(self, op) -> list:
+        """Launch kinds of one operation: "pass" (fused transform + transition)
+        or "check" (C2R spectrum check)."""
+        cap = 64
+        kinds = (C.c_int32 * cap)()
+        cnt = C.c_int32()
+        L.check(L.load().pb_plan_steps(self._h, op, kinds, cap, C.byref(cnt)), "steps")
+        return ["check" if kinds[i] == 1 else "pass" for i in range(cnt.value)]
+
     _forward_checks = False
     _reverse_checks = False
 
