@@ -43,7 +43,7 @@ template <typename R, int N>
 struct P2Geom {
   static constexpr int T = N / 8;
   static constexpr int SLOTS = P2_THREADS / T;
-  static constexpr int LPT = (sizeof(R) == 4 && N >= 64 && N <= 512) ? 2 : 1;
+  static constexpr int LPT = 1;
   static constexpr int NSEQ = SLOTS * LPT;
   static constexpr int SEQ = N + N / 8 + 1;  // padded sequence stride (complex units)
 };
@@ -159,7 +159,7 @@ __device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) 
 }
 
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
-__global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(P2_THREADS, sizeof(R) == 4 ? 3 : 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
   using S = Sched<N>;
   using G = P2Geom<R, N>;
@@ -313,40 +313,58 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
           }
         }
       } else {
-        // transposed store: element (k, j) of the tile goes to Atab[k] + j
-        constexpr int TOTAL = LMAX * NOUT;
-        if (KIND == P_C2C) {
+        // transposed store: element (k, j) of the tile goes to Atab[k] + j;
+        // lanes take pairs (j, j+1) of one row k and store 16-byte vectors
+        // where the destination address allows it
+        constexpr int PAIRS = LMAX >= 2 ? LMAX / 2 : 1;
+        constexpr int TOTAL = PAIRS * NOUT;
+        if (KIND == P_C2C || KIND == P_R2C) {
           C* __restrict__ out = reinterpret_cast<C*>(A.out);
+          const bool weighted = KIND == P_R2C && A.post_mode == W_HALF_INTERIOR;
           for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-            const int j = idx & (LMAX - 1);
-            const int k = idx / LMAX;
-            if (j < L) out[Atab[k] + j] = scl(sm[j * SEQ + pad8(k)], sc);
-          }
-        } else if (KIND == P_R2C) {
-          C* __restrict__ out = reinterpret_cast<C*>(A.out);
-          const bool weighted = A.post_mode == W_HALF_INTERIOR;
-          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-            const int j = idx & (LMAX - 1);
-            const int k = idx / LMAX;
-            if (j < L) {
+            const int j = 2 * (idx & (PAIRS - 1));
+            const int k = idx / PAIRS;
+            if (j >= L) continue;
+            C v0, v1;
+            if (KIND == P_C2C) {
+              v0 = scl(sm[j * SEQ + pad8(k)], sc);
+              v1 = scl(sm[(j + 1) * SEQ + pad8(k)], sc);
+            } else {
               const C* seq = sm + (j >> 1) * SEQ;
               const C a = seq[pad8(k)];
               const C b = seq[pad8((N - k) & (N - 1))];
               R f = sc * R(0.5);
               if (weighted && k != 0 && k != N / 2) f *= pf;
-              out[Atab[k] + j] = (j & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f)
-                                         : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+              v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+              v1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
+            }
+            const long long o = Atab[k] + j;
+            if (j + 1 < L) {
+              if (sizeof(R) == 4 && (o & 1) == 0) {
+                float4 w;
+                w.x = (float)v0.x;
+                w.y = (float)v0.y;
+                w.z = (float)v1.x;
+                w.w = (float)v1.y;
+                *reinterpret_cast<float4*>(out + o) = w;
+              } else {
+                out[o] = v0;
+                out[o + 1] = v1;
+              }
+            } else {
+              out[o] = v0;
             }
           }
         } else {  // C2R, transposed real store
           R* __restrict__ out = reinterpret_cast<R*>(A.out);
           for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-            const int j = idx & (LMAX - 1);
-            const int k = idx / LMAX;
-            if (j < L) {
-              const C z = sm[(j >> 1) * SEQ + pad8(k)];
-              out[Atab[k] + j] = ((j & 1) ? z.y : z.x) * sc;
-            }
+            const int j = 2 * (idx & (PAIRS - 1));
+            const int k = idx / PAIRS;
+            if (j >= L) continue;
+            const C z = sm[(j >> 1) * SEQ + pad8(k)];
+            const long long o = Atab[k] + j;
+            out[o] = z.x * sc;
+            if (j + 1 < L) out[o + 1] = z.y * sc;
           }
         }
       }
@@ -359,7 +377,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     for (int i = 0; i < LPT; ++i)
 #pragma unroll
       for (int m = 0; m < 8; ++m) v[i][m] = nv[i][m];
-    __syncthreads();  // the smem of this tile has been read by every thread
+    // the next tile's first shared-memory write is preceded by a barrier
   }
 }
 

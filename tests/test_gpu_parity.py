@@ -387,7 +387,8 @@ def test_vjp_adjoint_identity_f64(family):
 
 
 POW2_CASES = [((2, 3), (64, 128, 256), (2,)), ((4, 2), (256, 32, 512), ()), ((2, 2), (2048, 8, 32), ()),
-              ((3,), (32, 1024, 64), ()), ((4, 8), (64, 64, 128), ())]
+              ((3,), (32, 1024, 64), ()), ((4, 8), (64, 64, 128), ()), ((2, 2), (4, 1024, 2048), ()),
+              ((2, 3), (33, 64, 32), (3,))]
 
 
 @pytest.mark.parametrize("rb", [4, 8])
