@@ -327,8 +327,9 @@ __global__ void __launch_bounds__(P2_THREADS, sizeof(R) == 4 ? 3 : 2) pow2_kerne
             if (j >= L) continue;
             C v0, v1;
             if (KIND == P_C2C) {
+              // row j + 1 exists only when the tile holds that line (j + 1 < L <= NSEQ)
               v0 = scl(sm[j * SEQ + pad8(k)], sc);
-              v1 = scl(sm[(j + 1) * SEQ + pad8(k)], sc);
+              v1 = (j + 1 < L) ? scl(sm[(j + 1) * SEQ + pad8(k)], sc) : v0;
             } else {
               const C* seq = sm + (j >> 1) * SEQ;
               const C a = seq[pad8(k)];
