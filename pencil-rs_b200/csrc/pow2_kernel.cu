@@ -43,7 +43,7 @@ template <typename R, int N>
 struct P2Geom {
   static constexpr int T = N / 8;
   static constexpr int SLOTS = P2_THREADS / T;
-  static constexpr int LPT = 1;
+  static constexpr int LPT = (sizeof(R) == 4 && N >= 64 && N <= 512) ? 2 : 1;
   static constexpr int NSEQ = SLOTS * LPT;
   static constexpr int SEQ = N + N / 8 + 1;  // padded sequence stride (complex units)
 };
@@ -159,7 +159,7 @@ __device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) 
 }
 
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
-__global__ void __launch_bounds__(P2_THREADS, sizeof(R) == 4 ? 3 : 2) pow2_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
   using S = Sched<N>;
   using G = P2Geom<R, N>;
