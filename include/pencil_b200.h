@@ -59,7 +59,8 @@ typedef enum pb_status {
   PB_EUNSUPPORTED = 15,              /* valid for the reference, not (yet) for this library */
   PB_ECUDA = 16,                     /* CUDA runtime error */
   PB_EINVALID_ARGUMENT = 17,
-  PB_EWRONG_PLAN = 18                /* workspace/batch does not belong to this plan */
+  PB_EWRONG_PLAN = 18,               /* workspace/batch does not belong to this plan */
+  PB_ENO_ALLOC_LIMIT = 19            /* plan workspace exceeds PB_NO_ALLOC_SCRATCH_BYTES */
 } pb_status;
 
 typedef enum pb_precision { PB_F32 = 0, PB_F64 = 1 } pb_precision;
@@ -194,6 +195,23 @@ int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void*
  * TransformTiming): 0 = fused pass (local transform + transition), 1 = C2R
  * spectrum check.  *count = number of launches. */
 int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capacity, int32_t* count);
+
+/* Allocation-free execution.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc when they execute (host callbacks,
+ * real-time loops, embedders whose device memory is a fixed pre-set budget).
+ * Runs `op` of an existing plan like pb_execute, but the workspace is one
+ * file-scope device array of PB_NO_ALLOC_SCRATCH_BYTES that every GPU loading
+ * this library holds until exit; the call allocates nothing.  A plan whose
+ * pb_plan_info.workspace_bytes exceeds that size is rejected with
+ * PB_ENO_ALLOC_LIMIT before any device work.  The first call on a device looks
+ * up the array's device address (once per device, with that device current):
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  The spectrum-check words are cleared
+ * at the start of every call; operations that include the C2R spectrum check
+ * wait for `stream` and return PB_EINVALID_SPECTRUM when it rejects. */
+#define PB_NO_ALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int pb_execute_no_alloc(pb_plan* plan, int32_t op, const void* in, void* out, void* stream);
 
 /* ---- transposes ------------------------------------------------------- */
 /* AllToAllvTransposePlan::new (crates/pencil-array/src/alltoallv_transpose.rs:65-72). */

@@ -62,3 +62,11 @@ cudaError_t launch_segments(const SegArgs& A, cudaStream_t stream);
 cudaError_t launch_exchange(const ExchArgs& A, cudaStream_t stream);
 
 }  // namespace pb
+
+struct pb_plan;
+
+namespace pb {
+long long plan_workspace_bytes(const pb_plan* plan);
+int execute_with_workspace(pb_plan* plan, int op, const void* in, void* out, void* ws, void* stream,
+                           int report_spectrum);
+}  // namespace pb

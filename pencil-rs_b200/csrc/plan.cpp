@@ -1320,6 +1320,30 @@ static int guard(F&& f) {
   }
 }
 
+// Workspace size of a plan (bytes), for callers that supply their own scratch.
+long long plan_workspace_bytes(const pb_plan* plan) { return plan ? (long long)plan->ws_bytes : -1; }
+
+// Runs `op` with the caller-chosen workspace `ws`; with report_spectrum, an
+// operation that includes the C2R spectrum check waits for the stream and
+// returns PB_EINVALID_SPECTRUM when the check rejected.
+int execute_with_workspace(pb_plan* plan, int op, const void* in, void* out, void* ws, void* stream,
+                           int report_spectrum) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int rc = run(plan, op, in, out, ws, s, nullptr, 0, nullptr);
+    if (rc != PB_OK) return rc;
+    if (report_spectrum && plan->prog[user_mode(*plan, op)].has_stats) {
+      int st[2] = {0, 0};
+      cuda_ok(cudaMemcpyAsync(st, static_cast<unsigned char*>(ws) + plan->status_off, sizeof(st),
+                              cudaMemcpyDeviceToHost, s));
+      cuda_ok(cudaStreamSynchronize(s));
+      if (st[0] != 0 || st[1] != 0) return (int)PB_EINVALID_SPECTRUM;
+    }
+    return (int)PB_OK;
+  });
+}
+
 }  // namespace pb
 
 // ===========================================================================
@@ -1352,6 +1376,7 @@ const char* pb_status_string(int status) {
     case PB_ECUDA: return "CUDA error";
     case PB_EINVALID_ARGUMENT: return "invalid argument";
     case PB_EWRONG_PLAN: return "workspace or batch belongs to another plan";
+    case PB_ENO_ALLOC_LIMIT: return "plan workspace exceeds the fixed no-allocation scratch (PB_NO_ALLOC_SCRATCH_BYTES)";
     default: return "unknown status";
   }
 }

@@ -18,7 +18,7 @@ INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libpencil_b200.so")
 
-SOURCES = ["pass_kernel.cu", "pow2_kernel.cu", "aux_kernels.cu", "plan.cpp"]
+SOURCES = ["pass_kernel.cu", "pow2_kernel.cu", "aux_kernels.cu", "plan.cpp", "no_alloc.cu"]
 HEADERS = ["pb_internal.hpp", "pb_aux.hpp", "pb_device.cuh", "pb_fft.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

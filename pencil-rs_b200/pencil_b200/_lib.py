@@ -22,7 +22,7 @@ STATUS_NAMES = {
     4: "InvalidPermutation", 5: "InvalidLength", 6: "InvalidGraph", 7: "InputLayoutMismatch",
     8: "UnsupportedDecompositionChange", 9: "CountOverflow", 10: "ShapeMismatch", 11: "InvalidSign",
     12: "InvalidSpectrum", 13: "Timeout", 14: "Null", 15: "Unsupported", 16: "Cuda",
-    17: "InvalidArgument", 18: "WrongPlan",
+    17: "InvalidArgument", 18: "WrongPlan", 19: "NoAllocLimit",
 }
 
 # pb_op
@@ -73,6 +73,7 @@ SIGNATURES = {
     "pb_plan_pencil": ([_P, C.c_int32, C.POINTER(PbPencilDesc)], C.c_int),
     "pb_execute": ([_P, C.c_int32, _P, _P, _P, _P], C.c_int),
     "pb_execute_status": ([_P, _P, _P], C.c_int),
+    "pb_execute_no_alloc": ([_P, C.c_int32, _P, _P, _P], C.c_int),
     "pb_plan_steps": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),
