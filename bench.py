@@ -158,6 +158,80 @@ def reference_arm(args):
     return 0
 
 
+def batch_section(pb, L, torch, dev, steps=10, warmup=3):
+    """Ragged batch: 64 C2C f32 grids, each axis length drawn (seed 4) from the
+    55 numbers 2^a 3^b 5^c 7^d in [32, 256], 16 grids (25%) with an extra dim
+    of 2, forward + inverse.  One graph-replayed persistent launch for the whole
+    batch against per-grid launches of the plain kernels (pb_execute per grid
+    and direction), at the same accuracy bound."""
+    import numpy as np
+    smooth = sorted({2 ** a * 3 ** b * 5 ** c * 7 ** d for a in range(9) for b in range(6) for c in range(4)
+                     for d in range(3) if 32 <= 2 ** a * 3 ** b * 5 ** c * 7 ** d <= 256})
+    rng = np.random.default_rng(4)
+    shapes = [tuple(int(v) for v in rng.choice(smooth, 3)) for _ in range(64)]
+    with_extra = set(int(i) for i in rng.choice(64, 16, replace=False))
+    gen = torch.Generator(device=dev).manual_seed(4)
+    plans, xs, ws = [], [], []
+    for i, shp in enumerate(shapes):
+        extra = (2,) if i in with_extra else ()
+        plan = pb.C2cPlan.from_shape(pb.MpiTopology((1, 1)), shp, extra, dtype=torch.complex64)
+        n = plan.info.input_elems
+        xs.append(torch.complex(torch.randn(n, generator=gen, device=dev), torch.randn(n, generator=gen, device=dev)))
+        ws.append(plan.allocate_workspace(dev))
+        plans.append(plan)
+    batch = pb.PlanBatch(plans, ("forward", "inverse"), autotune=True)
+    bws = batch.allocate_workspace(dev)
+    mids = [p.allocate_output(dev) for p in plans]
+    ends = [p.allocate_input(dev) for p in plans]
+    pmids = [p.allocate_output(dev) for p in plans]
+    pends = [p.allocate_input(dev) for p in plans]
+    stream = torch.cuda.Stream(dev)
+    lib = L.load()
+    sp = pb.plans._stream_ptr(stream)
+    hp = [(p._h, pb.plans._ptr(x), pb.plans._ptr(m), pb.plans._ptr(e), pb.plans._ptr(w))
+          for p, x, m, e, w in zip(plans, xs, pmids, pends, ws)]
+
+    def per_grid():
+        for h, x, m, e, w in hp:
+            L.check(lib.pb_execute(h, L.FORWARD, x, m, w, sp), "forward")
+            L.check(lib.pb_execute(h, L.INVERSE, m, e, w, sp), "inverse")
+
+    def batched():
+        batch.execute([xs, mids, ends], bws, stream)
+
+    times = {}
+    with torch.cuda.stream(stream):
+        for name, fn in (("batch", batched), ("per_grid", per_grid)):
+            for _ in range(warmup):
+                fn()
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+            times[name] = e0.elapsed_time(e1) / steps
+        batch.status(bws, stream)
+    rt_b = rt_p = diff = 0.0
+    worst_bound = 1.0
+    for plan, x, m, e, pm, pe, shp in zip(plans, xs, mids, ends, pmids, pends, shapes):
+        nrm = float(torch.linalg.vector_norm(x))
+        rt_b = max(rt_b, float(torch.linalg.vector_norm(e - x)) / nrm)
+        rt_p = max(rt_p, float(torch.linalg.vector_norm(pe - x)) / nrm)
+        diff = max(diff, float(torch.linalg.vector_norm(m - pm) / torch.linalg.vector_norm(pm)))
+        worst_bound = min(worst_bound, 1e-6 * math.log2(shp[0] * shp[1] * shp[2]))
+    nbytes = 0
+    for plan in plans:
+        nbytes += 2 * 3 * 2 * plan.info.input_elems * 8  # 2 directions x 3 passes x (read + write)
+    return {"grids": 64, "with_extra": 16, "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
+            "speedup": times["per_grid"] / times["batch"], "gbs_batch": nbytes / (times["batch"] * 1e-3) / 1e9,
+            "launches_batch": 1, "launches_per_grid": 64 * (plans[0].info.passes_forward + plans[0].info.passes_inverse),
+            "roundtrip_rel_l2_batch": rt_b, "roundtrip_rel_l2_per_grid": rt_p, "batch_vs_per_grid_rel_l2": diff,
+            "bound": worst_bound, "shapes_seed": 4}
+
+
 def b200_arm(args):
     import torch
     import pencil_b200 as pb
@@ -308,6 +382,10 @@ def b200_arm(args):
     d2h = h_out.numel() * h_out.element_size()
     e2e_err = float(torch.linalg.vector_norm((h_out - h_in).double()) / torch.linalg.vector_norm(h_in.double()))
 
+    batch = None
+    if not args.no_batch:
+        batch = batch_section(pb, L, torch, dev)
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline()
@@ -344,6 +422,7 @@ def b200_arm(args):
             "gpu_launches": args.steps * (plan.info.passes_forward + plan.info.passes_inverse + 2),
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "cpu_baseline": base,
+            "ragged_batch": batch,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -360,6 +439,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-grid ragged-batch comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

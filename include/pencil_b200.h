@@ -213,6 +213,27 @@ int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capac
 #define PB_NO_ALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int pb_execute_no_alloc(pb_plan* plan, int32_t op, const void* in, void* out, void* stream);
 
+/* ---- ragged batches ---------------------------------------------------- */
+/* The collections API (crates/pencil-fft/src/distributed/collections.rs:1-17)
+ * runs forward_many as a sequential loop over arrays of ONE plan.  A batch here
+ * holds any number of plans of one precision (different shapes, extras and
+ * layouts) and an operation chain (e.g. FORWARD then INVERSE); one execution is
+ * ONE persistent kernel launch over a level-ordered (plan, pass, tile) work
+ * queue, replayed from a CUDA graph on a non-default stream.  Tile heights are
+ * chosen by an autotuner that caches its choice per pass shape (process-wide;
+ * persisted in the file named by PB_TUNE_CACHE when set).  Plans whose chain
+ * needs the C2R spectrum check are not accepted (PB_EUNSUPPORTED). */
+int pb_batch_create(pb_plan* const* plans, int32_t count, const int32_t* ops, int32_t nops, int32_t autotune,
+                    pb_batch** batch);
+int pb_batch_workspace_bytes(const pb_batch* batch, int64_t* bytes);
+/* buffers: (nops + 1) * count device pointers; buffers[k*count + i] is plan i's
+ * input of op k (k < nops) and its output of op k-1 (k > 0). */
+int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, void* stream);
+/* Waits for `stream`; PB_ETIMEOUT if a bounded dependency wait in the last
+ * execution gave up (its tiles were skipped), else PB_OK. */
+int pb_batch_status(pb_batch* batch, void* workspace, void* stream);
+int pb_batch_destroy(pb_batch* batch);
+
 /* ---- transposes ------------------------------------------------------- */
 /* AllToAllvTransposePlan::new (crates/pencil-array/src/alltoallv_transpose.rs:65-72). */
 int pb_transpose_create_alltoallv(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count,

@@ -119,14 +119,13 @@ __device__ __forceinline__ bool weight_hit(int mode, int idx, int n) {
   }
 }
 
+// One tile of a pass: gather, transform, scatter.  `smem` is the block's
+// dynamic shared memory (pass_smem_bytes(A) bytes).
 template <typename R>
-__global__ void __launch_bounds__(256) pass_kernel(const PassArgs A) {
+__device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsigned char* smem) {
   using C = typename Cx<R>::T;
-  extern __shared__ __align__(16) unsigned char smem[];
-  if (A.gate != nullptr && *A.gate != 0) return;
 
   // ---- tile decode: (extra, outer coordinates, chunk of the tile axis)
-  long long t = blockIdx.x;
   const int ci = (int)(t % A.nchunks);
   long long outer = t / A.nchunks;
   const int2 ch = A.chunks[ci];
@@ -493,6 +492,110 @@ __global__ void __launch_bounds__(256) pass_kernel(const PassArgs A) {
       }
     }
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) pass_kernel(const PassArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (A.gate != nullptr && *A.gate != 0) return;
+  pass_tile<R>(A, blockIdx.x, smem);
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batch: one persistent launch over the passes of many plans.  Work
+// items (pass descriptor, tile) are dequeued in level-major order (pass l of
+// every plan before pass l+1 of any), so an item only waits for items that
+// were dequeued before it by resident CTAs.  Waits are bounded; a wait that
+// gives up sets B.error and the item is skipped.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) batch_kernel(const BatchArgs B) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ PassArgs sA;
+  __shared__ long long s_item;
+  __shared__ int s_desc, s_ok;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long it = (long long)atomicAdd(B.head, 1ULL);
+      s_item = it;
+      s_ok = 0;
+      if (it < B.total_items) {
+        int lo = 0, hi = B.ndesc - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (B.item_start[mid] <= it)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        s_desc = lo;
+        int ok = 1;
+        const int dep = B.dep[lo];
+        if (dep >= 0) {
+          const unsigned need = (unsigned)(B.item_start[dep + 1] - B.item_start[dep]);
+          const volatile unsigned* cnt = B.done + dep;
+          long long spins = 0;
+          while (*cnt < need) {
+            if (++spins > B.spin_limit || *(volatile int*)B.error != 0) {
+              atomicExch(B.error, 1);
+              ok = 0;
+              break;
+            }
+            __nanosleep(100);
+          }
+          __threadfence();
+        }
+        s_ok = ok;
+      }
+    }
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= B.total_items) break;
+    const int d = s_desc;
+    {
+      const int* src = reinterpret_cast<const int*>(B.descs + d);
+      int* dst = reinterpret_cast<int*>(&sA);
+      for (int i = threadIdx.x; i < (int)(sizeof(PassArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (s_ok) pass_tile<R>(sA, it - B.item_start[d], smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(B.done + d, 1u);
+    }
+  }
+}
+
+cudaError_t launch_batch(const BatchArgs& B, int real_bytes, size_t smem, int grid, cudaStream_t stream) {
+  if (B.total_items <= 0) return cudaSuccess;
+  if (real_bytes == 4) {
+    cudaError_t err = cudaFuncSetAttribute(batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    batch_kernel<float><<<grid, 256, smem, stream>>>(B);
+  } else {
+    cudaError_t err =
+        cudaFuncSetAttribute(batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    batch_kernel<double><<<grid, 256, smem, stream>>>(B);
+  }
+  return cudaGetLastError();
+}
+
+int batch_occupancy(int real_bytes, size_t smem) {
+  int blocks = 0;
+  if (real_bytes == 4) {
+    if (cudaFuncSetAttribute(batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_kernel<float>, 256, smem) != cudaSuccess)
+      return 1;
+  } else {
+    if (cudaFuncSetAttribute(batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_kernel<double>, 256, smem) != cudaSuccess)
+      return 1;
+  }
+  return blocks > 0 ? blocks : 1;
 }
 
 size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {

@@ -51,7 +51,22 @@ struct ExchArgs {
   void* recv;
 };
 
+// One persistent launch over the passes of several plans (pass_kernel.cu).
+struct BatchArgs {
+  const PassArgs* descs;         // pass descriptors in queue (level-major) order
+  const long long* item_start;   // ndesc + 1 prefix sums of tiles
+  const int* dep;                // descriptor each one waits for, or -1
+  int ndesc;
+  long long total_items;
+  unsigned long long* head;      // queue head (zeroed before the launch)
+  unsigned int* done;            // tiles finished per descriptor (zeroed)
+  int* error;                    // set when a bounded wait gives up
+  long long spin_limit;
+};
+
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream);
+cudaError_t launch_batch(const BatchArgs& B, int real_bytes, size_t smem, int grid, cudaStream_t stream);
+int batch_occupancy(int real_bytes, size_t smem);
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int pow2_lines(int m, int kind, int real_bytes);
 int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes);

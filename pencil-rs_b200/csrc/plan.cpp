@@ -303,6 +303,8 @@ struct pb_plan {
   size_t buf_bytes = 0;
   size_t status_off = 0, acc_off = 0, ws_bytes = 0;
   int max_smem = 227 * 1024;
+  bool force_generic = false;                // batch building: generic pass kernel only
+  std::map<std::string, int> tuned_lines;    // batch building: autotuned lines per tile by pass shape
   ~pb_plan() {
     if (arena) cudaFree(arena);
   }
@@ -662,10 +664,22 @@ static LocalOp local_op(const Stage& st, int mode, long long n_axis) {
   }
 }
 
-static int choose_lines(pb_plan& P, PassArgs& A, int pair_kind) {
+static int choose_lines_capped(pb_plan& P, PassArgs& A, int pair_kind, int cap);
+
+// Shape key of a generic pass (the autotuner's cache key).
+static std::string pass_key(const PassArgs& A, int real_bytes) {
+  return "k" + std::to_string(A.kind) + "s" + std::to_string(A.sub) + "n" + std::to_string(A.n_in) + "o" +
+         std::to_string(A.n_out) + "m" + std::to_string(A.m) + "r" + std::to_string(real_bytes) + "c" +
+         std::to_string(A.in_complex) + std::to_string(A.out_complex) + "t" + std::to_string(A.src_k_contig) +
+         std::to_string(A.dst_k_contig) + "i" + std::to_string(A.inv);
+}
+
+static int choose_lines(pb_plan& P, PassArgs& A, int pair_kind) { return choose_lines_capped(P, A, pair_kind, 64); }
+
+static int choose_lines_capped(pb_plan& P, PassArgs& A, int pair_kind, int cap) {
   const int cb = 2 * P.real_bytes;
   const int big = std::max(std::max(A.n_in, A.n_out), A.m);
-  int L = std::max(1, std::min(64, 8192 / std::max(1, big)));
+  int L = std::max(1, std::min(cap, 8192 / std::max(1, big)));
   if (pair_kind && L > 1 && (L & 1)) --L;
   const size_t budget = (size_t)std::min(P.max_smem, 112 * 1024);
   for (;;) {
@@ -832,7 +846,7 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   // register-resident power-of-two kernel: lines contiguous in one source rank,
   // destination either with the same property (direct) or with the tile axis
   // innermost and unsplit (transposed store)
-  const bool pow2 = A.m >= 32 && A.m <= 2048 && (A.m & (A.m - 1)) == 0;
+  const bool pow2 = !P.force_generic && A.m >= 32 && A.m <= 2048 && (A.m & (A.m - 1)) == 0;
   if ((op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && pow2 && src.perm[N - 1] == a &&
       src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
@@ -846,6 +860,10 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
     }
   }
   if (!A.fast) L = choose_lines(P, A, pair_kind ? 1 : 0);
+  if (!A.fast && P.force_generic) {
+    auto it = P.tuned_lines.find(pass_key(A, P.real_bytes));
+    if (it != P.tuned_lines.end() && it->second < L) L = choose_lines_capped(P, A, pair_kind ? 1 : 0, it->second);
+  }
   // chunks of the tile axis, split at both partitions of axis b
   std::vector<long long> cuts{0, src.shape[b]};
   for (const Pencil* p : {&src, &dst}) {
@@ -2027,6 +2045,396 @@ int pb_remap_apply(pb_remap* plan, const void* src, void* dst, void* stream) {
 
 int pb_remap_destroy(pb_remap* plan) {
   delete plan;
+  return PB_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// ragged batch: many plans, one persistent launch (collections.rs analogue)
+// ===========================================================================
+struct pb_batch {
+  int real_bytes = 4;
+  int count = 0;
+  int nops = 0;
+  std::vector<pb_plan*> plans;
+  std::unique_ptr<pb_plan> tables;  // owns the device tables of every descriptor
+  struct Desc {
+    pb::PassArgs pa;
+    int plan;
+    int src_slot, dst_slot;  // >= 0: workspace slot of the plan; < 0: -(1 + buffer set index)
+  };
+  std::vector<Desc> descs;
+  std::vector<long long> item_start;
+  std::vector<int> dep;
+  std::vector<size_t> ws_off, buf_bytes;
+  size_t ctrl_off = 0, ws_bytes = 0;
+  size_t smem = 0;
+  int grid = 1;
+  pb::PassArgs* d_descs = nullptr;
+  long long* d_item_start = nullptr;
+  int* d_dep = nullptr;
+  pb::PassArgs* h_descs = nullptr;  // pinned staging of the resolved descriptors
+  std::vector<const void*> bound;   // buffers + workspace the device descriptors were resolved with
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  ~pb_batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (d_descs) cudaFree(d_descs);
+    if (d_item_start) cudaFree(d_item_start);
+    if (d_dep) cudaFree(d_dep);
+    if (h_descs) cudaFreeHost(h_descs);
+  }
+};
+
+namespace pb {
+
+static std::mutex g_tune_mutex;
+static std::map<std::string, int> g_tune_cache;  // pass shape -> lines per tile
+static bool g_tune_loaded = false;
+
+// Optional persistence of the autotuner cache: PB_TUNE_CACHE=<file> holds
+// "key lines" pairs, one per line.
+static void tune_cache_load() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = std::getenv("PB_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return;
+  char key[256];
+  int lines = 0;
+  while (std::fscanf(f, "%255s %d", key, &lines) == 2) g_tune_cache[key] = lines;
+  std::fclose(f);
+}
+
+static void tune_cache_store() {
+  const char* path = std::getenv("PB_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return;
+  for (auto& kv : g_tune_cache) std::fprintf(f, "%s %d\n", kv.first.c_str(), kv.second);
+  std::fclose(f);
+}
+
+// Copies the route of `src` into the batch's table builder.
+static void adopt_route(pb_plan& T, const pb_plan& src) {
+  T.c2r_family = src.c2r_family;
+  T.stages = src.stages;
+  T.boundary = src.boundary;
+  T.real_len = src.real_len;
+  T.terms = src.terms;
+  T.extra = src.extra;
+  T.fin = src.fin;
+  T.fout = src.fout;
+  T.fin_complex = src.fin_complex;
+  T.fout_complex = src.fout_complex;
+  T.buf_bytes = 0;
+}
+
+// Times the generic pass of `A` with each candidate tile height on scratch
+// buffers and records the fastest in the cache.
+static void autotune_pass(pb_plan& T, const pb_plan& plan, int mode, int step, void* scratch_a, void* scratch_b) {
+  adopt_route(T, plan);
+  build_program(T, mode);
+  const Step& base = T.prog[mode].steps[step];
+  if (base.type != 0 || base.pa.fast) return;
+  const std::string key = pass_key(base.pa, T.real_bytes);
+  if (g_tune_cache.count(key)) return;
+  const int pair_kind = (base.pa.kind == P_R2C || base.pa.kind == P_C2R ||
+                         (base.pa.kind == P_R2R && !base.pa.in_complex)) ? 1 : 0;
+  std::vector<int> cands;
+  for (int c = base.pa.lines; c >= 1 && (int)cands.size() < 4; c /= 2) {
+    if (pair_kind && c > 1 && (c & 1)) continue;
+    cands.push_back(c);
+  }
+  cudaEvent_t e0, e1;
+  cuda_ok(cudaEventCreate(&e0));
+  cuda_ok(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_l = base.pa.lines;
+  for (int c : cands) {
+    T.tuned_lines[key] = c;
+    adopt_route(T, plan);
+    const size_t mark = T.host.bytes.size();
+    build_program(T, mode);
+    Step st = T.prog[mode].steps[step];
+    // upload this candidate's tables into a temporary arena
+    void* arena = nullptr;
+    cuda_ok(cudaMalloc(&arena, T.host.bytes.size()));
+    cuda_ok(cudaMemcpy(arena, T.host.bytes.data(), T.host.bytes.size(), cudaMemcpyHostToDevice));
+    const uintptr_t b = reinterpret_cast<uintptr_t>(arena);
+    auto fix = [&](const void*& p) {
+      if (p != nullptr) p = reinterpret_cast<const void*>(b + reinterpret_cast<uintptr_t>(p) - 1);
+    };
+    const void* ch = st.pa.chunks;
+    fix(ch);
+    st.pa.chunks = reinterpret_cast<const int2*>(ch);
+    fix(st.pa.twiddle);
+    fix(st.pa.aux0);
+    fix(st.pa.aux1);
+    const void* si = st.pa.src.info;
+    fix(si);
+    st.pa.src.info = reinterpret_cast<const long long*>(si);
+    const void* di = st.pa.dst.info;
+    fix(di);
+    st.pa.dst.info = reinterpret_cast<const long long*>(di);
+    st.pa.in = scratch_a;
+    st.pa.out = scratch_b;
+    st.pa.gate = nullptr;
+    cuda_ok(launch_pass(st.pa, T.real_bytes, 0));
+    cuda_ok(cudaEventRecord(e0, 0));
+    for (int r = 0; r < 3; ++r) cuda_ok(launch_pass(st.pa, T.real_bytes, 0));
+    cuda_ok(cudaEventRecord(e1, 0));
+    cuda_ok(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cuda_ok(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_l = c;
+    }
+    cudaFree(arena);
+    T.host.bytes.resize(mark);  // candidate tables are not kept
+    T.cache.clear();
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g_tune_cache[key] = best_l;
+  T.tuned_lines.erase(key);
+}
+
+static int user_mode_batch(const pb_plan& P, int op) { return user_mode(P, op); }
+
+static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, int nops, int autotune) {
+  if (!plans || !ops || count <= 0 || nops <= 0) fail(PB_EINVALID_ARGUMENT);
+  std::unique_ptr<pb_batch> B(new pb_batch());
+  B->count = count;
+  B->nops = nops;
+  B->real_bytes = plans[0] ? plans[0]->real_bytes : 4;
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i]) fail(PB_ENULL);
+    if (plans[i]->real_bytes != B->real_bytes) fail(PB_EINVALID_ARGUMENT);
+    B->plans.push_back(plans[i]);
+    for (int k = 0; k < nops; ++k) {
+      const Program& pr = plans[i]->prog[user_mode_batch(*plans[i], ops[k])];
+      if (pr.has_stats) fail(PB_EUNSUPPORTED);  // the batch carries no C2R spectrum check
+    }
+  }
+  B->tables.reset(new pb_plan());
+  pb_plan& T = *B->tables;
+  T.real_bytes = B->real_bytes;
+  T.force_generic = true;
+  int dev = 0, sms = 148;
+  cuda_ok(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+    T.max_smem = optin;
+
+  // autotune the tile height of every distinct pass shape (process-wide cache)
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    tune_cache_load();
+    if (autotune) {
+      size_t big = 0;
+      for (pb_plan* p : B->plans) {
+        big = std::max(big, (size_t)p->fin.total(p->extra) * p->real_bytes * 2);
+        big = std::max(big, (size_t)p->fout.total(p->extra) * p->real_bytes * 2);
+        big = std::max(big, p->buf_bytes);
+      }
+      void* sa = nullptr;
+      void* sb = nullptr;
+      cuda_ok(cudaMalloc(&sa, big));
+      cuda_ok(cudaMalloc(&sb, big));
+      cuda_ok(cudaMemset(sa, 0, big));
+      for (pb_plan* p : B->plans)
+        for (int k = 0; k < nops; ++k) {
+          const int mode = user_mode_batch(*p, ops[k]);
+          adopt_route(T, *p);
+          build_program(T, mode);
+          const int nsteps = (int)T.prog[mode].steps.size();
+          for (int st = 0; st < nsteps; ++st) autotune_pass(T, *p, mode, st, sa, sb);
+        }
+      cudaFree(sa);
+      cudaFree(sb);
+      tune_cache_store();
+      T.host.bytes.clear();
+      T.cache.clear();
+    }
+    T.tuned_lines = g_tune_cache;
+  }
+
+  // per plan: its op chain as generic passes; queue in level-major order
+  std::vector<std::vector<pb_batch::Desc>> chain(count);
+  size_t ws = 0;
+  for (int i = 0; i < count; ++i) {
+    pb_plan& p = *B->plans[i];
+    size_t buf = 0;
+    for (int k = 0; k < nops; ++k) {
+      const int mode = user_mode_batch(p, ops[k]);
+      adopt_route(T, p);
+      build_program(T, mode);
+      buf = std::max(buf, T.buf_bytes);
+      for (const Step& s : T.prog[mode].steps) {
+        pb_batch::Desc d;
+        d.pa = s.pa;
+        d.plan = i;
+        d.src_slot = s.src_slot == -1 ? -(1 + k) : (s.src_slot == -2 ? -(2 + k) : s.src_slot);
+        d.dst_slot = s.dst_slot == -2 ? -(2 + k) : (s.dst_slot == -1 ? -(1 + k) : s.dst_slot);
+        chain[i].push_back(d);
+      }
+    }
+    buf = (buf + 255) & ~size_t(255);
+    B->buf_bytes.push_back(buf);
+    B->ws_off.push_back(ws);
+    ws += 2 * buf;
+  }
+  size_t maxlev = 0;
+  for (auto& c : chain) maxlev = std::max(maxlev, c.size());
+  std::vector<std::vector<int>> index(count);
+  B->item_start.push_back(0);
+  for (size_t lev = 0; lev < maxlev; ++lev)
+    for (int i = 0; i < count; ++i) {
+      if (lev >= chain[i].size()) continue;
+      const int id = (int)B->descs.size();
+      B->descs.push_back(chain[i][lev]);
+      B->dep.push_back(lev == 0 ? -1 : index[i].back());
+      index[i].push_back(id);
+      B->item_start.push_back(B->item_start.back() + B->descs.back().pa.ntiles);
+    }
+  // control words after the workspaces: head (8 B), error (4 B), done[ndesc]
+  B->ctrl_off = (ws + 255) & ~size_t(255);
+  B->ws_bytes = B->ctrl_off + 16 + B->descs.size() * sizeof(unsigned);
+  // tables of every descriptor
+  if (!T.host.bytes.empty()) {
+    cuda_ok(cudaMalloc(&T.arena, T.host.bytes.size()));
+    cuda_ok(cudaMemcpy(T.arena, T.host.bytes.data(), T.host.bytes.size(), cudaMemcpyHostToDevice));
+  }
+  for (auto& d : B->descs) {
+    auto fix = [&](const void*& p) { p = fix_ptr(T, p); };
+    const void* ch = d.pa.chunks;
+    fix(ch);
+    d.pa.chunks = reinterpret_cast<const int2*>(ch);
+    fix(d.pa.twiddle);
+    fix(d.pa.aux0);
+    fix(d.pa.aux1);
+    d.pa.src.info = reinterpret_cast<const long long*>(fix_ptr(T, d.pa.src.info));
+    d.pa.dst.info = reinterpret_cast<const long long*>(fix_ptr(T, d.pa.dst.info));
+    d.pa.gate = nullptr;
+    B->smem = std::max(B->smem, pass_smem_bytes(d.pa, B->real_bytes));
+  }
+  const size_t nd = B->descs.size();
+  cuda_ok(cudaMalloc(reinterpret_cast<void**>(&B->d_descs), nd * sizeof(PassArgs)));
+  cuda_ok(cudaMalloc(reinterpret_cast<void**>(&B->d_item_start), (nd + 1) * sizeof(long long)));
+  cuda_ok(cudaMalloc(reinterpret_cast<void**>(&B->d_dep), std::max<size_t>(nd, 1) * sizeof(int)));
+  cuda_ok(cudaMemcpy(B->d_item_start, B->item_start.data(), (nd + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+  if (nd) cuda_ok(cudaMemcpy(B->d_dep, B->dep.data(), nd * sizeof(int), cudaMemcpyHostToDevice));
+  cuda_ok(cudaMallocHost(reinterpret_cast<void**>(&B->h_descs), std::max<size_t>(nd, 1) * sizeof(PassArgs)));
+  B->grid = sms * batch_occupancy(B->real_bytes, B->smem);
+  return B.release();
+}
+
+static void* batch_slot(const pb_batch& B, int plan, int slot, void* const* buffers, void* ws) {
+  if (slot >= 0) return static_cast<unsigned char*>(ws) + B.ws_off[plan] + (size_t)slot * B.buf_bytes[plan];
+  const int set = -slot - 1;
+  return buffers[(size_t)set * B.count + plan];
+}
+
+static int batch_execute(pb_batch* B, void* const* buffers, void* ws, cudaStream_t s) {
+  if (!buffers || !ws) fail(PB_ENULL);
+  std::vector<const void*> now((size_t)(B->nops + 1) * B->count + 1);
+  for (size_t i = 0; i + 1 < now.size(); ++i) now[i] = buffers[i];
+  now.back() = ws;
+  const bool rebind = now != B->bound;
+  if (rebind) {
+    cuda_ok(cudaStreamSynchronize(s));  // the previous upload from the pinned staging has finished
+    for (size_t d = 0; d < B->descs.size(); ++d) {
+      PassArgs a = B->descs[d].pa;
+      a.in = batch_slot(*B, B->descs[d].plan, B->descs[d].src_slot, buffers, ws);
+      a.out = batch_slot(*B, B->descs[d].plan, B->descs[d].dst_slot, buffers, ws);
+      B->h_descs[d] = a;
+    }
+    cuda_ok(cudaMemcpyAsync(B->d_descs, B->h_descs, B->descs.size() * sizeof(PassArgs), cudaMemcpyHostToDevice, s));
+    if (B->graph) {
+      cudaGraphExecDestroy(B->graph);
+      B->graph = nullptr;
+    }
+    B->bound = now;
+  }
+  unsigned char* ctrl = static_cast<unsigned char*>(ws) + B->ctrl_off;
+  BatchArgs A{};
+  A.descs = B->d_descs;
+  A.item_start = B->d_item_start;
+  A.dep = B->d_dep;
+  A.ndesc = (int)B->descs.size();
+  A.total_items = B->item_start.back();
+  A.head = reinterpret_cast<unsigned long long*>(ctrl);
+  A.error = reinterpret_cast<int*>(ctrl + 8);
+  A.done = reinterpret_cast<unsigned*>(ctrl + 16);
+  A.spin_limit = 1LL << 24;
+  const size_t ctrl_bytes = 16 + B->descs.size() * sizeof(unsigned);
+  if (s == nullptr) {  // the legacy stream cannot be captured: launch directly
+    cuda_ok(cudaMemsetAsync(ctrl, 0, ctrl_bytes, s));
+    cuda_ok(launch_batch(A, B->real_bytes, B->smem, B->grid, s));
+    return PB_OK;
+  }
+  if (!B->graph || B->graph_stream != s) {
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    cudaGraph_t g;
+    cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = cudaMemsetAsync(ctrl, 0, ctrl_bytes, s);
+    cudaError_t e2 = (e1 == cudaSuccess) ? launch_batch(A, B->real_bytes, B->smem, B->grid, s) : e1;
+    cudaError_t e3 = cudaStreamEndCapture(s, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) fail(PB_ECUDA);
+    cudaError_t e4 = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e4 != cudaSuccess) fail(PB_ECUDA);
+    B->graph_stream = s;
+  }
+  cuda_ok(cudaGraphLaunch(B->graph, s));
+  return PB_OK;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_batch_create(pb_plan* const* plans, int32_t count, const int32_t* ops, int32_t nops, int32_t autotune,
+                    pb_batch** batch) {
+  return guard([&] {
+    if (!batch) return (int)PB_ENULL;
+    *batch = batch_create(plans, count, ops, nops, autotune);
+    return (int)PB_OK;
+  });
+}
+
+int pb_batch_workspace_bytes(const pb_batch* batch, int64_t* bytes) {
+  if (!batch || !bytes) return PB_ENULL;
+  *bytes = (int64_t)batch->ws_bytes;
+  return PB_OK;
+}
+
+int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, void* stream) {
+  return guard([&] {
+    if (!batch) return (int)PB_ENULL;
+    return batch_execute(batch, buffers, workspace, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int pb_batch_status(pb_batch* batch, void* workspace, void* stream) {
+  return guard([&] {
+    if (!batch || !workspace) return (int)PB_ENULL;
+    int err = 0;
+    cuda_ok(cudaMemcpyAsync(&err, static_cast<unsigned char*>(workspace) + batch->ctrl_off + 8, sizeof(int),
+                            cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    cuda_ok(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return err ? (int)PB_ETIMEOUT : (int)PB_OK;
+  });
+}
+
+int pb_batch_destroy(pb_batch* batch) {
+  delete batch;
   return PB_OK;
 }
 

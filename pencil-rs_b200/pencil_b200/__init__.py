@@ -17,6 +17,7 @@ from .plans import (  # noqa: F401
     MixedR2cPlan,
     MpiTopology,
     Pencil,
+    PlanBatch,
     R2cPlan,
     R2rPlan,
     SpatialRemapPlan,
@@ -24,6 +25,6 @@ from .plans import (  # noqa: F401
 
 __all__ = [
     "AllToAllvTransposePlan", "C2cPlan", "C2rPlan", "DhtPlan", "DistributedLayout", "InvalidSpectrum",
-    "LocalTransposePlan", "MixedC2cPlan", "MixedR2cPlan", "MpiTopology", "Pencil", "PencilError", "R2cPlan",
+    "LocalTransposePlan", "MixedC2cPlan", "MixedR2cPlan", "MpiTopology", "Pencil", "PencilError", "PlanBatch", "R2cPlan",
     "R2rPlan", "SpatialRemapPlan", "load",
 ]

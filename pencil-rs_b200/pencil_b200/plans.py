@@ -495,3 +495,55 @@ class SpatialRemapPlan:
             self.close()
         except Exception:
             pass
+
+
+class PlanBatch:
+    """A ragged batch of plans run as ONE persistent launch per execution.
+
+    The reference's collections (``forward_many``, collections.rs) loop over
+    arrays of one plan; here every plan may differ (shape, extra dims,
+    layout), and an operation chain such as ``("forward", "inverse")`` runs in
+    the same launch.  Executions on a non-default stream are replayed from a
+    CUDA graph.
+    """
+
+    _OPS = {"forward": L.FORWARD, "inverse": L.INVERSE, "backward": L.BACKWARD}
+
+    def __init__(self, plans, ops=("forward", "inverse"), autotune=True):
+        self.plans = list(plans)
+        self.ops = tuple(ops)
+        n = len(self.plans)
+        arr = (C.c_void_p * n)(*[p._h.value if isinstance(p._h, C.c_void_p) else p._h for p in self.plans])
+        opa = (C.c_int32 * len(ops))(*[self._OPS[o] for o in ops])
+        h = C.c_void_p()
+        L.check(L.load().pb_batch_create(arr, n, opa, len(ops), 1 if autotune else 0, C.byref(h)), "batch")
+        self._h = h
+        b = C.c_int64()
+        L.check(L.load().pb_batch_workspace_bytes(h, C.byref(b)), "batch workspace")
+        self.workspace_bytes = b.value
+
+    def allocate_workspace(self, device="cuda"):
+        return torch.empty(max(self.workspace_bytes, 1), dtype=torch.uint8, device=device)
+
+    def execute(self, buffers, workspace, stream=None):
+        """buffers[k][i]: plan i's input of op k and output of op k-1 (len(ops)+1 sets)."""
+        n = len(self.plans)
+        flat = (C.c_void_p * ((len(self.ops) + 1) * n))()
+        for k, row in enumerate(buffers):
+            for i, t in enumerate(row):
+                flat[k * n + i] = t.data_ptr()
+        L.check(L.load().pb_batch_execute(self._h, flat, _ptr(workspace), _stream_ptr(stream)), "batch execute")
+
+    def status(self, workspace, stream=None):
+        L.check(L.load().pb_batch_status(self._h, _ptr(workspace), _stream_ptr(stream)), "batch status")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().pb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
