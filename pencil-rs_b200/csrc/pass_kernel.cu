@@ -33,12 +33,13 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ in, C* __restric
   const int nb = m / RAD;
   const int total = nseq * nb;
   const int tw = m / (Ns * RAD);
+  const unsigned mnb = fdiv_magic(nb), mns = fdiv_magic(Ns);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int s = t / nb;
+    const int s = (int)fdiv(t, nb, mnb);
     const int j = t - s * nb;
     const C* src = in + s * ld;
     C* dst = out + s * ld;
-    const int k = j % Ns;
+    const int k = j - (int)fdiv(j, Ns, mns) * Ns;
     C v[RAD];
 #pragma unroll
     for (int r = 0; r < RAD; ++r) v[r] = src[j + r * nb];
@@ -62,12 +63,13 @@ __device__ void fft_stage_generic(const C* __restrict__ in, C* __restrict__ out,
   const int nb = m / RAD;
   const int total = nseq * nb;
   const int tw = m / (Ns * RAD);
+  const unsigned mnb = fdiv_magic(nb), mns = fdiv_magic(Ns);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int s = t / nb;
+    const int s = (int)fdiv(t, nb, mnb);
     const int j = t - s * nb;
     const C* src = in + s * ld;
     C* dst = out + s * ld;
-    const int k = j % Ns;
+    const int k = j - (int)fdiv(j, Ns, mns) * Ns;
     const int base = (j - k) * RAD + k;
     for (int q = 0; q < RAD; ++q) {
       C acc = mk<C, R>(R(0), R(0));
@@ -125,21 +127,6 @@ template <typename R>
 __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsigned char* smem) {
   using C = typename Cx<R>::T;
 
-  // ---- tile decode: (extra, outer coordinates, chunk of the tile axis)
-  const int ci = (int)(t % A.nchunks);
-  long long outer = t / A.nchunks;
-  const int2 ch = A.chunks[ci];
-  int g[MAXN];
-#pragma unroll
-  for (int x = 0; x < MAXN; ++x) g[x] = 0;
-  for (int i = A.nouter_axes - 1; i >= 0; --i) {
-    g[A.outer_axis[i]] = (int)(outer % A.outer_ext[i]);
-    outer /= A.outer_ext[i];
-  }
-  const long long e = outer;
-  g[A.b] = ch.x;
-  const int L = ch.y;
-
   // ---- shared memory carve-up
   const int nin = A.n_in, nout = A.n_out, m = A.m, ld = A.ld;
   long long* sA = reinterpret_cast<long long*>(smem);
@@ -150,26 +137,68 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   C* W = reinterpret_cast<C*>(smem + off);
   C* buf0 = W + ((m + 1) & ~1);
   C* buf1 = buf0 + A.buf_elems;
-
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int k = tid; k < nin; k += nt) {
-    int gg[MAXN];
+
+  int L;
+  if (A.tile_tab != nullptr) {
+    // host-precomputed addresses: lines contiguous in one source rank; the
+    // destination is either the same (direct) or transposed by the tile axis
+    const TileAddr ta = load_tile(reinterpret_cast<const TileAddr*>(A.tile_tab), t);
+    L = ta.lines;
+    for (int k = tid; k < nin; k += nt) {
+      sA[k] = ta.src0 + k;
+      sS[k] = ta.srcb;
+    }
+    if (A.dst_k_contig) {
+      for (int k = tid; k < nout; k += nt) {
+        dA[k] = ta.dst0 + k;
+        dS[k] = ta.dstb;
+      }
+    } else {
+      const PieceAddr* pt = reinterpret_cast<const PieceAddr*>(A.piece_tab) + t * A.npieces;
+      for (int k = tid; k < nout; k += nt) {
+        const int2 kp = A.ktab[k];
+        const PieceAddr pa = pt[kp.x];
+        dA[k] = pa.rowbase + (long long)kp.y * pa.stride;
+        dS[k] = 1;
+      }
+    }
+  } else {
+    // ---- tile decode: (extra, outer coordinates, chunk of the tile axis)
+    const int ci = (int)(t % A.nchunks);
+    long long outer = t / A.nchunks;
+    const int2 ch = A.chunks[ci];
+    int g[MAXN];
 #pragma unroll
-    for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
-    gg[A.a] = k;
-    int sb;
-    sA[k] = locate(A.src, e, gg, A.b, &sb);
-    sS[k] = sb;
-  }
-  for (int k = tid; k < nout; k += nt) {
-    int gg[MAXN];
+    for (int x = 0; x < MAXN; ++x) g[x] = 0;
+    for (int i = A.nouter_axes - 1; i >= 0; --i) {
+      g[A.outer_axis[i]] = (int)(outer % A.outer_ext[i]);
+      outer /= A.outer_ext[i];
+    }
+    const long long e = outer;
+    g[A.b] = ch.x;
+    L = ch.y;
+    for (int k = tid; k < nin; k += nt) {
+      int gg[MAXN];
 #pragma unroll
-    for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
-    gg[A.a] = k;
-    int sb;
-    dA[k] = locate(A.dst, e, gg, A.b, &sb);
-    dS[k] = sb;
+      for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
+      gg[A.a] = k;
+      int sb;
+      sA[k] = locate(A.src, e, gg, A.b, &sb);
+      sS[k] = sb;
+    }
+    for (int k = tid; k < nout; k += nt) {
+      int gg[MAXN];
+#pragma unroll
+      for (int x = 0; x < MAXN; ++x) gg[x] = g[x];
+      gg[A.a] = k;
+      int sb;
+      dA[k] = locate(A.dst, e, gg, A.b, &sb);
+      dS[k] = sb;
+    }
   }
+  const unsigned m_nin = fdiv_magic(nin), m_nout = fdiv_magic(nout), m_L = fdiv_magic(L), m_m = fdiv_magic(m);
+  const unsigned m_n = fdiv_magic(A.n), m_2n = fdiv_magic(2 * A.n), m_h = fdiv_magic(A.n / 2 + 1);
   const C* Wg = reinterpret_cast<const C*>(A.twiddle);
   if (Wg != nullptr)
     for (int i = tid; i < m; i += nt) W[i] = Wg[i];
@@ -184,12 +213,12 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     const int row = c2c ? ld : nin;
     if (A.src_k_contig) {
       for (int i = tid; i < total_in; i += nt) {
-        const int j = i / nin, k = i - j * nin;
+        const int j = (int)fdiv(i, nin, m_nin), k = i - j * nin;
         st[j * row + k] = in[sA[k] + (long long)j * sS[k]];
       }
     } else {
       for (int i = tid; i < total_in; i += nt) {
-        const int k = i / L, j = i - k * L;
+        const int k = (int)fdiv(i, L, m_L), j = i - k * L;
         st[j * row + k] = in[sA[k] + (long long)j * sS[k]];
       }
     }
@@ -198,12 +227,12 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     R* st = reinterpret_cast<R*>(buf1);
     if (A.src_k_contig) {
       for (int i = tid; i < total_in; i += nt) {
-        const int j = i / nin, k = i - j * nin;
+        const int j = (int)fdiv(i, nin, m_nin), k = i - j * nin;
         st[j * nin + k] = in[sA[k] + (long long)j * sS[k]];
       }
     } else {
       for (int i = tid; i < total_in; i += nt) {
-        const int k = i / L, j = i - k * L;
+        const int k = (int)fdiv(i, L, m_L), j = i - k * L;
         st[j * nin + k] = in[sA[k] + (long long)j * sS[k]];
       }
     }
@@ -238,14 +267,14 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   if (A.kind == P_R2C) {
     nseq = pairs;
     for (int i = tid; i < nseq * m; i += nt) {
-      const int s = i / m, q = i - s * m;
+      const int s = (int)fdiv(i, m, m_m), q = i - s * m;
       buf0[s * ld + q] = mk<C, R>(getv(s, 0, q), getv(s, 1, q));
     }
   } else if (A.kind == P_C2R) {
     nseq = pairs;
     const int h = n / 2 + 1;
     for (int i = tid; i < nseq * m; i += nt) {
-      const int s = i / m, q = i - s * m;
+      const int s = (int)fdiv(i, m, m_m), q = i - s * m;
       const int hq = q < h ? q : n - q;
       const bool edge = (hq == 0) || ((n & 1) == 0 && hq == n / 2);
       R w = R(1);
@@ -269,7 +298,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     const bool iv4 = (sub == S_DCT4 || sub == S_DST4);
     nseq = iv4 ? 2 * pairs : pairs;
     for (int i = tid; i < nseq * m; i += nt) {
-      const int s = i / m, q = i - s * m;
+      const int s = (int)fdiv(i, m, m_m), q = i - s * m;
       C z;
       switch (sub) {
         case S_DCT2:
@@ -352,7 +381,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   if (A.kind == P_R2C) {
     const int h = n / 2 + 1;
     for (int i = tid; i < L * h; i += nt) {
-      const int l = i / h, k = i - l * h;
+      const int l = (int)fdiv(i, h, m_h), k = i - l * h;
       const int p = l >> 1;
       const C a = res[p * ld + k];
       const C b = res[p * ld + (k == 0 ? 0 : n - k)];
@@ -365,7 +394,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   } else if (A.kind == P_C2R) {
     R* o = reinterpret_cast<R*>(other);
     for (int i = tid; i < L * n; i += nt) {
-      const int l = i / n, q = i - l * n;
+      const int l = (int)fdiv(i, n, m_n), q = i - l * n;
       const C z = res[(l >> 1) * ld + q];
       o[l * nout + q] = ((l & 1) ? z.y : z.x) * sc;
     }
@@ -373,9 +402,9 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     const int sub = A.sub;
     R* orl = reinterpret_cast<R*>(other);
     for (int i = tid; i < pairs * 2 * n; i += nt) {
-      const int p = i / (2 * n);
+      const int p = (int)fdiv(i, 2 * n, m_2n);
       const int rem = i - p * 2 * n;
-      const int c = rem / n, k = rem - c * n;
+      const int c = (int)fdiv(rem, n, m_n), k = rem - c * n;
       if (!A.out_complex && 2 * p + c >= L) continue;
       R v;
       switch (sub) {
@@ -463,14 +492,14 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     }
     if (A.dst_k_contig) {
       for (int i = tid; i < total_out; i += nt) {
-        const int j = i / nout, k = i - j * nout;
+        const int j = (int)fdiv(i, nout, m_nout), k = i - j * nout;
         C v = src[j * row + k];
         if (scale_here) v = scl(v, sc);
         out[dA[k] + (long long)j * dS[k]] = v;
       }
     } else {
       for (int i = tid; i < total_out; i += nt) {
-        const int k = i / L, j = i - k * L;
+        const int k = (int)fdiv(i, L, m_L), j = i - k * L;
         C v = src[j * row + k];
         if (scale_here) v = scl(v, sc);
         out[dA[k] + (long long)j * dS[k]] = v;
@@ -482,12 +511,12 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
     const int row = (A.kind == P_COPY) ? nin : nout;
     if (A.dst_k_contig) {
       for (int i = tid; i < total_out; i += nt) {
-        const int j = i / nout, k = i - j * nout;
+        const int j = (int)fdiv(i, nout, m_nout), k = i - j * nout;
         out[dA[k] + (long long)j * dS[k]] = src[j * row + k];
       }
     } else {
       for (int i = tid; i < total_out; i += nt) {
-        const int k = i / L, j = i - k * L;
+        const int k = (int)fdiv(i, L, m_L), j = i - k * L;
         out[dA[k] + (long long)j * dS[k]] = src[j * row + k];
       }
     }

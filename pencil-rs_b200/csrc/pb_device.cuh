@@ -48,4 +48,26 @@ __device__ __forceinline__ int rank_of_offset(const DevPencil& p, long long idx)
   return lo;
 }
 
+__device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) {
+  const longlong2* p = reinterpret_cast<const longlong2*>(tab + t);
+  const longlong2 r0 = p[0], r1 = p[1];
+  TileAddr a;
+  a.src0 = r0.x;
+  a.dst0 = r0.y;
+  a.srcb = (int)(r1.x & 0xffffffffLL);
+  a.dstb = (int)(r1.x >> 32);
+  a.lines = (int)(r1.y & 0xffffffffLL);
+  a.pad = 0;
+  return a;
+}
+
+// q = x / d for 32-bit unsigned x and d >= 1, with m = 0xffffffff / d
+// precomputed: one high multiply and one correction step.
+__device__ __forceinline__ unsigned fdiv(unsigned x, unsigned d, unsigned m) {
+  unsigned q = __umulhi(x, m);
+  if (x - q * d >= d) ++q;
+  return q;
+}
+__device__ __forceinline__ unsigned fdiv_magic(unsigned d) { return 0xffffffffu / d; }
+
 }  // namespace pb

@@ -772,10 +772,12 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
     A.ktab = reinterpret_cast<const int2*>(enc(P.host.add(kt.data(), kt.size() * sizeof(int2))));
   }
   A.npieces = npieces;
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int occ = pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
-  A.grid_ctas = sms * std::max(1, occ);
+  if (A.fast) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int occ = pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
+    A.grid_ctas = sms * std::max(1, occ);
+  }
 }
 
 // One fused pass for `st` under `op` from layout `src` to layout `dst`.
@@ -896,7 +898,20 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   A.ntiles = tiles;
   A.src = dev_pencil(P, P.host, P.cache, src, P.extra);
   A.dst = dev_pencil(P, P.host, P.cache, dst, P.extra);
-  if (A.fast) build_fast_tables(P, A, src, dst, chunks);
+  if (A.fast) {
+    build_fast_tables(P, A, src, dst, chunks);
+  } else {
+    // generic kernel: host-precomputed tile/row addresses whenever the layouts
+    // allow them (always on the canonical route); otherwise per-tile locate
+    const bool src_ok = src.perm[N - 1] == a && src.split_of(a) < 0;
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    if (src_ok && (direct || transposed)) {
+      A.dst_k_contig = direct ? 1 : 0;
+      build_fast_tables(P, A, src, dst, chunks);
+    }
+  }
   return s;
 }
 
@@ -2173,6 +2188,11 @@ static void autotune_pass(pb_plan& T, const pb_plan& plan, int mode, int step, v
     fix(st.pa.twiddle);
     fix(st.pa.aux0);
     fix(st.pa.aux1);
+    fix(st.pa.tile_tab);
+    fix(st.pa.piece_tab);
+    const void* kt = st.pa.ktab;
+    fix(kt);
+    st.pa.ktab = reinterpret_cast<const int2*>(kt);
     const void* si = st.pa.src.info;
     fix(si);
     st.pa.src.info = reinterpret_cast<const long long*>(si);
@@ -2318,6 +2338,9 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
     fix(d.pa.twiddle);
     fix(d.pa.aux0);
     fix(d.pa.aux1);
+    fix(d.pa.tile_tab);
+    fix(d.pa.piece_tab);
+    d.pa.ktab = reinterpret_cast<const int2*>(fix_ptr(T, d.pa.ktab));
     d.pa.src.info = reinterpret_cast<const long long*>(fix_ptr(T, d.pa.src.info));
     d.pa.dst.info = reinterpret_cast<const long long*>(fix_ptr(T, d.pa.dst.info));
     d.pa.gate = nullptr;

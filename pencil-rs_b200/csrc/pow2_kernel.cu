@@ -145,19 +145,6 @@ __device__ __forceinline__ void p2_load(typename Cx<R>::T (&v)[LPT][8], const Pa
   }
 }
 
-__device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) {
-  const longlong2* p = reinterpret_cast<const longlong2*>(tab + t);
-  const longlong2 r0 = p[0], r1 = p[1];
-  TileAddr a;
-  a.src0 = r0.x;
-  a.dst0 = r0.y;
-  a.srcb = (int)(r1.x & 0xffffffffLL);
-  a.dstb = (int)(r1.x >> 32);
-  a.lines = (int)(r1.y & 0xffffffffLL);
-  a.pad = 0;
-  return a;
-}
-
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
 __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
