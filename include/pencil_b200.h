@@ -213,6 +213,16 @@ int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capac
 #define PB_NO_ALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int pb_execute_no_alloc(pb_plan* plan, int32_t op, const void* in, void* out, void* stream);
 
+/* ---- spectral multipliers ---------------------------------------------- */
+/* out = m(k) * scale * in on the plan's FORWARD output layout (complex), k the
+ * integer wavevector of each element (FFT order; the R2C-reduced axis holds
+ * k = 0..n/2).  mode PB_MULT_K2: m = |k|^2; PB_MULT_POISSON: m = -1/|k|^2 with
+ * m(0) = 0.  A user-side operation in the reference (no counterpart); used by
+ * the spectral Poisson solve and the |k|^2-weighted loss. */
+#define PB_MULT_K2 0
+#define PB_MULT_POISSON 1
+int pb_spectral_multiply(const pb_plan* plan, int32_t mode, double scale, const void* in, void* out, void* stream);
+
 /* ---- ragged batches ---------------------------------------------------- */
 /* The collections API (crates/pencil-fft/src/distributed/collections.rs:1-17)
  * runs forward_many as a sequential loop over arrays of ONE plan.  A batch here

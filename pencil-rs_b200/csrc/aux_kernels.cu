@@ -312,3 +312,58 @@ cudaError_t launch_exchange(const ExchArgs& A, cudaStream_t stream) {
 }
 
 }  // namespace pb
+
+namespace pb {
+
+// ---------------------------------------------------------------------------
+// Spectral multiplier on a plan's spectral layout: out = m(k) * in for every
+// element, k the integer wavevector of the element (FFT order: index g maps to
+// g if g <= n/2 else g - n; the R2C-reduced axis holds k = 0..n/2).
+//   MULT_K2      m = |k|^2
+//   MULT_POISSON m = -1/|k|^2, m(0) = 0 (spectral Poisson solve)
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void spectral_kernel(const SpectralArgs A) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < A.total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const DevPencil& d = A.pen;
+    const int r = rank_of_offset(d, idx);
+    const long long* inf = d.info + (long long)r * info_words(d.N);
+    const long long local = idx - inf[0];
+    const long long len = inf[1];
+    const long long e = local / len;
+    long long pos = local - e * len;
+    double k2 = 0.0;
+    for (int q = d.N - 1; q >= 0; --q) {
+      const int ax = d.perm[q];
+      const long long ext = inf[2 + 2 * d.N + ax];
+      const long long c = pos % ext;
+      pos /= ext;
+      const long long g = inf[2 + ax] + c;
+      long long k = g;
+      if (ax != A.half_axis && g > d.shape[ax] / 2) k = g - d.shape[ax];
+      k2 += (double)(k * k);
+    }
+    double mult;
+    if (A.mode == 0)
+      mult = k2;
+    else
+      mult = (k2 == 0.0) ? 0.0 : -1.0 / k2;
+    const R f = (R)(mult * A.scale);
+    const R* in = reinterpret_cast<const R*>(A.in);
+    R* out = reinterpret_cast<R*>(A.out);
+    out[2 * idx] = in[2 * idx] * f;
+    out[2 * idx + 1] = in[2 * idx + 1] * f;
+  }
+}
+
+cudaError_t launch_spectral(const SpectralArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.total <= 0) return cudaSuccess;
+  if (real_bytes == 4)
+    spectral_kernel<float><<<grid_for(A.total, 256, 148LL * 32), 256, 0, stream>>>(A);
+  else
+    spectral_kernel<double><<<grid_for(A.total, 256, 148LL * 32), 256, 0, stream>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace pb

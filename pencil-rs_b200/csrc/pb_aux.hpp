@@ -64,6 +64,18 @@ struct BatchArgs {
   long long spin_limit;
 };
 
+// Elementwise multiplier m(k) on a spectral layout (aux_kernels.cu).
+struct SpectralArgs {
+  DevPencil pen;
+  const void* in;
+  void* out;
+  long long total;  // complex elements over all ranks and extras
+  int half_axis;    // R2C-reduced axis (k = index), or -1
+  int mode;         // 0: |k|^2, 1: -1/|k|^2 with 0 at k = 0
+  double scale;
+};
+
+cudaError_t launch_spectral(const SpectralArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_batch(const BatchArgs& B, int real_bytes, size_t smem, int grid, cudaStream_t stream);
 int batch_occupancy(int real_bytes, size_t smem);

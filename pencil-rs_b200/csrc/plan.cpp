@@ -305,6 +305,7 @@ struct pb_plan {
   int max_smem = 227 * 1024;
   bool force_generic = false;                // batch building: generic pass kernel only
   std::map<std::string, int> tuned_lines;    // batch building: autotuned lines per tile by pass shape
+  pb::DevPencil spectral_pen{};              // FORWARD output layout (spectral multipliers)
   ~pb_plan() {
     if (arena) cudaFree(arena);
   }
@@ -1036,6 +1037,7 @@ static void finalize(pb_plan& P) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
     P.max_smem = optin;
   for (int m = 0; m < M_COUNT; ++m) build_program(P, m);
+  P.spectral_pen = dev_pencil(P, P.host, P.cache, P.fout, P.extra);
   // upload tables
   if (!P.host.bytes.empty()) {
     cuda_ok(cudaMalloc(&P.arena, P.host.bytes.size()));
@@ -1070,6 +1072,7 @@ static void finalize(pb_plan& P) {
         fixpen(s.sa.pen);
       }
     }
+  fixpen(P.spectral_pen);
   // workspace: two intermediate buffers, then status words and statistics
   const size_t buf = (P.buf_bytes + 255) & ~size_t(255);
   P.buf_bytes = buf;
@@ -1606,6 +1609,29 @@ int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void*
   return guard([&] {
     if (!plan || !stage_ms) return (int)PB_ENULL;
     return run(plan, op, in, out, workspace, static_cast<cudaStream_t>(stream), stage_ms, capacity, count);
+  });
+}
+
+int pb_spectral_multiply(const pb_plan* plan, int32_t mode, double scale, const void* in, void* out, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (mode != PB_MULT_K2 && mode != PB_MULT_POISSON) return (int)PB_EINVALID_ARGUMENT;
+    const pb_plan& P = *plan;
+    // the complex spectral layout: FORWARD output (C2rPlan: its FORWARD input)
+    if (!P.fout_complex) return (int)PB_EINVALID_ARGUMENT;
+    const long long total = P.fout.total(P.extra);
+    if (total == 0) return (int)PB_OK;
+    if (!in || !out) return (int)PB_ENULL;
+    SpectralArgs A{};
+    A.pen = P.spectral_pen;
+    A.in = in;
+    A.out = out;
+    A.total = total;
+    A.half_axis = (P.boundary >= 0) ? P.stages[P.boundary].axis : -1;
+    A.mode = mode;
+    A.scale = scale;
+    cuda_ok(launch_spectral(A, P.real_bytes, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
   });
 }
 

@@ -77,6 +77,7 @@ SIGNATURES = {
     "pb_plan_steps": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),
+    "pb_spectral_multiply": ([_P, C.c_int32, C.c_double, _P, _P, _P], C.c_int),
     "pb_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_P)],
                         C.c_int),
     "pb_batch_workspace_bytes": ([_P, C.POINTER(C.c_int64)], C.c_int),

@@ -263,6 +263,16 @@ class _Plan:
                                           ms, cap, C.byref(cnt)), "execute_timed")
         return [ms[i] for i in range(cnt.value)]
 
+    def spectral_multiply(self, mode: int, scale: float, src, dst, stream=None):
+        """dst = m(k) * scale * src on the FORWARD output layout (mode 0: |k|^2,
+        1: -1/|k|^2 with 0 at k = 0)."""
+        n = self.info.output_elems if self.info.output_complex else self.info.input_elems
+        dt = self.output_dtype if self.info.output_complex else self.input_dtype
+        self._check_buf(src, dt, n, "source")
+        self._check_buf(dst, dt, n, "destination")
+        L.check(L.load().pb_spectral_multiply(self._h, int(mode), float(scale), _ptr(src), _ptr(dst),
+                                              _stream_ptr(stream)), "spectral_multiply")
+
     def step_kinds(self, op) -> list:
         """Launch kinds of one operation: "pass" (fused transform + transition)
         or "check" (C2R spectrum check)."""
