@@ -158,7 +158,7 @@ def reference_arm(args):
     return 0
 
 
-def batch_section(pb, L, torch, dev, steps=10, warmup=3):
+def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1):
     """Ragged batch: 64 C2C f32 grids, each axis length drawn (seed 4) from the
     55 numbers 2^a 3^b 5^c 7^d in [32, 256], 16 grids (25%) with an extra dim
     of 2, forward + inverse.  One graph-replayed persistent launch for the whole
@@ -170,9 +170,13 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3):
     rng = np.random.default_rng(4)
     shapes = [tuple(int(v) for v in rng.choice(smooth, 3)) for _ in range(64)]
     with_extra = set(int(i) for i in rng.choice(64, 16, replace=False))
-    gen = torch.Generator(device=dev).manual_seed(4)
+    from pencil_b200 import distributed as pbd
+    mine = list(pbd.shard(len(shapes), rank, world))  # grids are independent: no exchange across GPUs
+    gen = torch.Generator(device=dev).manual_seed(4 + rank)
     plans, xs, ws = [], [], []
-    for i, shp in enumerate(shapes):
+    shapes = [shapes[i] for i in mine]
+    for j, shp in enumerate(shapes):
+        i = mine[j]
         extra = (2,) if i in with_extra else ()
         plan = pb.C2cPlan.from_shape(pb.MpiTopology((1, 1)), shp, extra, dtype=torch.complex64)
         n = plan.info.input_elems
@@ -212,7 +216,7 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3):
                 fn()
             e1.record(stream)
             stream.synchronize()
-            times[name] = e0.elapsed_time(e1) / steps
+            times[name] = pbd.max_over_ranks(e0.elapsed_time(e1) / steps)
         batch.status(bws, stream)
     rt_b = rt_p = diff = 0.0
     worst_bound = 1.0
@@ -225,7 +229,9 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3):
     nbytes = 0
     for plan in plans:
         nbytes += 2 * 3 * 2 * plan.info.input_elems * 8  # 2 directions x 3 passes x (read + write)
-    return {"grids": 64, "with_extra": 16, "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
+    nbytes = pbd.sum_over_ranks(nbytes)
+    rt_b, rt_p, diff = (pbd.max_over_ranks(v) for v in (rt_b, rt_p, diff))
+    return {"grids": 64, "grids_per_gpu": len(mine), "with_extra": 16, "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
             "speedup": times["per_grid"] / times["batch"], "gbs_batch": nbytes / (times["batch"] * 1e-3) / 1e9,
             "launches_batch": 1, "launches_per_grid": 64 * (plans[0].info.passes_forward + plans[0].info.passes_inverse),
             "roundtrip_rel_l2_batch": rt_b, "roundtrip_rel_l2_per_grid": rt_p, "batch_vs_per_grid_rel_l2": diff,
@@ -384,7 +390,7 @@ def b200_arm(args):
 
     batch = None
     if not args.no_batch:
-        batch = batch_section(pb, L, torch, dev)
+        batch = batch_section(pb, L, torch, dev, rank=rank, world=world)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
