@@ -196,6 +196,12 @@ int pb_execute_timed(pb_plan* plan, int32_t op, const void* in, void* out, void*
  * spectrum check.  *count = number of launches. */
 int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capacity, int32_t* count);
 
+/* Kernel family of each launch of one operation, in order: 0 = generic fused
+ * pass (shared-memory Stockham, any length and kind), 1 = C2R spectrum check,
+ * 2 = register-resident power-of-two pass, 3 = register-fed mixed-radix pass
+ * (7-smooth lengths).  A diagnostic with no counterpart in the reference. */
+int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int32_t capacity, int32_t* count);
+
 /* Allocation-free execution.  No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they execute (host callbacks,
  * real-time loops, embedders whose device memory is a fixed pre-set budget).

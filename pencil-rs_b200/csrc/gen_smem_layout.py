@@ -1,0 +1,267 @@
+"""Generates smem_layout.hpp: the shared-memory sequence layout (padding shift
+and sequence stride) of the power-of-two and mixed-radix pass kernels, per
+line length and precision.
+
+Element i of a sequence sits at s*SEQ + i + (i >> SH) (SH = 0: no padding).
+For every candidate (SH, SEQ) this script replays each shared-memory access of
+a tile -- the Stockham exchanges, the twiddle reads, the natural-order writes
+and the transposed or R2C-split reads of the store, for every pass kind and
+store mode -- warp by warp, and counts wavefronts with the bank model
+
+    wavefronts(access) = max(ceil(active lanes * E / 128),
+                             max over bank groups of distinct elements)
+
+(E = 8 or 16 bytes per complex element: bank group = element mod 16 or mod 8;
+lanes reading the same element share it).  The layout with the fewest
+wavefronts summed over all kinds wins (the smaller SEQ on a tie).
+
+Run from this directory: ``python gen_smem_layout.py`` (a few minutes).
+The thread/sequence mappings replayed here are those of pow2_kernel.cu and
+mr_kernel.cuh; a change to either kernel's indexing needs a rerun.
+"""
+
+from __future__ import annotations
+
+import os
+from multiprocessing import get_context
+
+import numpy as np
+
+THREADS = 256
+POW2 = [32, 64, 128, 256, 512, 1024, 2048]
+MR = [35, 36, 40, 42, 45, 48, 49, 50, 54, 56, 60, 63, 70, 72, 75, 80, 81, 84, 90, 96, 98, 100, 105, 108, 112, 120,
+      125, 126, 135, 140, 144, 147, 150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
+      245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375, 378, 384, 392, 400, 405, 420,
+      432, 441, 448, 450, 480, 486, 490, 500, 504]
+SHIFTS = [0, 2, 3, 4, 5]
+KINDS = [("c2c", False), ("r2c", False), ("c2r", False), ("c2c", True), ("r2c", True), ("c2r", True)]
+
+
+def wavefronts(idx: np.ndarray, E: int) -> int:
+    """idx: (M, 32) element indices of M warp accesses, -1 for idle lanes."""
+    M = idx.shape[0]
+    G = 128 // E
+    s = np.sort(idx, axis=1)
+    valid = s >= 0
+    uniq = valid.copy()
+    uniq[:, 1:] &= s[:, 1:] != s[:, :-1]
+    cnt = np.zeros((M, G), dtype=np.int64)
+    rows = np.broadcast_to(np.arange(M)[:, None], (M, 32))
+    np.add.at(cnt, (rows[uniq], s[uniq] % G), 1)
+    minwf = -(-valid.sum(axis=1) * E // 128)
+    return int(np.maximum(cnt.max(axis=1), minwf).sum())
+
+
+def loop_lanes(count: int) -> np.ndarray:
+    """Work indices of each warp instruction of ``for (i = tid; i < count; i += 256)``."""
+    iters = -(-count // THREADS)
+    b = np.arange(iters * THREADS).reshape(-1, 32)
+    return np.where(b < count, b, -1)
+
+
+def padded(i, sh):
+    return i if sh == 0 else i + (i >> sh)
+
+
+# ---------------------------------------------------------------- pow2 kernel
+def p2_geom(N, rb):
+    T = N // 8
+    slots = THREADS // T
+    lpt = 2 if (rb == 4 and 64 <= N <= 512) else 1
+    return T, slots, lpt, slots * lpt
+
+
+def p2_cost(N, rb, sh, SEQ, kind, direct):
+    E = 2 * rb
+    T, slots, lpt, nseq = p2_geom(N, rb)
+    log = N.bit_length() - 1
+    lead = 8 if log % 3 == 0 else (2 if log % 3 == 1 else 4)
+    nst = log // 3 if log % 3 == 0 else log // 3 + 1
+    tid = np.arange(THREADS).reshape(-1, 32)
+    slot, t = tid // T, tid % T
+    tot = 0
+    for st in range(nst - 1):
+        R = lead if st == 0 else 8
+        NS = 1 if st == 0 else lead * 8 ** (st - 1)
+        for i in range(lpt):
+            base = (slot + slots * i) * SEQ
+            for q in range(8):
+                u, r = divmod(q, R)
+                jb = t + u * T
+                k = jb & (NS - 1)
+                tot += wavefronts(base + padded((jb - k) * R + k + r * NS, sh), E)
+            for m in range(8):
+                tot += wavefronts(base + padded(t + T * m, sh), E)
+    H = N // 2 + 1
+    if direct and kind != "r2c":
+        return tot
+    for i in range(lpt):
+        base = (slot + slots * i) * SEQ
+        for r in range(8):
+            tot += wavefronts(base + padded(t + T * r, sh), E)
+    if direct:  # R2C split store from shared memory
+        for i in range(lpt):
+            s = slot + slots * i
+            for k0 in range(0, H, T):
+                k = k0 + t
+                act = k < H
+                kk = np.where(act, k, 0)
+                tot += wavefronts(np.where(act, s * SEQ + padded(kk, sh), -1), E)
+                tot += wavefronts(np.where(act, s * SEQ + padded((N - kk) & (N - 1), sh), -1), E)
+        return tot
+    lmax = nseq if kind == "c2c" else 2 * nseq
+    pairs = max(lmax // 2, 1)
+    nout = H if kind == "r2c" else N
+    I = loop_lanes(pairs * nout)
+    act = I >= 0
+    Ia = np.where(act, I, 0)
+    j = 2 * (Ia & (pairs - 1))
+    k = Ia // pairs
+    if kind == "c2c":
+        tot += wavefronts(np.where(act, j * SEQ + padded(k, sh), -1), E)
+        tot += wavefronts(np.where(act, (j + 1) * SEQ + padded(k, sh), -1), E)
+    elif kind == "r2c":
+        tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded(k, sh), -1), E)
+        tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded((N - k) & (N - 1), sh), -1), E)
+    else:
+        tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded(k, sh), -1), E)
+    return tot
+
+
+# ---------------------------------------------------------- mixed-radix kernel
+def mr_factor(N):
+    r, m = [], N
+    while m % 8 == 0 and m > 1:
+        r.append(8)
+        m //= 8
+    if m % 4 == 0:
+        r.append(4)
+        m //= 4
+    if m % 2 == 0:
+        r.append(2)
+        m //= 2
+    for p in (7, 5, 3):
+        while m % p == 0:
+            r.append(p)
+            m //= p
+    return r
+
+
+def mr_nseq(N, rb):
+    fit = (3072 if rb == 4 else 1536) // N
+    if fit >= 64:
+        return 64
+    if fit < 2:
+        return 2
+    p = 1
+    while p * 2 <= fit:
+        p *= 2
+    return p
+
+
+def mr_sched(N, nseq):
+    r = mr_factor(N)
+    best, best_cost = 0, 1 << 30
+    for i, R in enumerate(r):
+        c = ((nseq * (N // R) + THREADS - 1) // THREADS) * R
+        if c < best_cost or (c == best_cost and R > r[best]):
+            best, best_cost = i, c
+    return [r[best]] + r[:best] + r[best + 1:]
+
+
+def mr_cost(N, rb, sh, SEQ, kind, direct):
+    E = 2 * rb
+    nseq = mr_nseq(N, rb)
+    rad = mr_sched(N, nseq)
+    tot = 0
+    ns = 1
+    for st, R in enumerate(rad):
+        NB = N // R
+        B = loop_lanes(nseq * NB)
+        act = B >= 0
+        s, jb = np.divmod(np.where(act, B, 0), NB)
+        k = jb % ns
+        last_to_hbm = st == len(rad) - 1 and direct and kind != "r2c"
+        for r in range(R):
+            if st > 0:
+                tot += wavefronts(np.where(act, s * SEQ + padded(jb + r * NB, sh), -1), E)
+                if r > 0:  # per-stage twiddle table: entry (r-1)*NS + k
+                    tot += wavefronts(np.where(act, (r - 1) * ns + k, -1), E)
+            if not last_to_hbm:
+                base = (jb - k) * R + k
+                tot += wavefronts(np.where(act, s * SEQ + padded(base + r * ns, sh), -1), E)
+        ns *= R
+    H = N // 2 + 1
+    if direct:
+        if kind == "r2c":
+            I = loop_lanes(2 * nseq * H)
+            act = I >= 0
+            Ia = np.where(act, I, 0)
+            l, k = Ia // H, Ia % H
+            tot += wavefronts(np.where(act, (l >> 1) * SEQ + padded(k, sh), -1), E)
+            tot += wavefronts(np.where(act, (l >> 1) * SEQ + padded((N - k) % N, sh), -1), E)
+        return tot
+    if kind == "c2c":
+        P = nseq // 2
+        I = loop_lanes(P * N)
+        act = I >= 0
+        Ia = np.where(act, I, 0)
+        p, k = Ia % P, Ia // P
+        tot += wavefronts(np.where(act, 2 * p * SEQ + padded(k, sh), -1), E)
+        tot += wavefronts(np.where(act, (2 * p + 1) * SEQ + padded(k, sh), -1), E)
+    else:
+        I = loop_lanes(nseq * (H if kind == "r2c" else N))
+        act = I >= 0
+        Ia = np.where(act, I, 0)
+        p, k = Ia % nseq, Ia // nseq
+        tot += wavefronts(np.where(act, p * SEQ + padded(k, sh), -1), E)
+        if kind == "r2c":
+            tot += wavefronts(np.where(act, p * SEQ + padded((N - k) % N, sh), -1), E)
+    return tot
+
+
+def best_layout(args):
+    family, N, rb = args
+    cost = p2_cost if family == "pow2" else mr_cost
+    best = None
+    for sh in SHIFTS:
+        lo = padded(N - 1, sh) + 1
+        for SEQ in range(lo, lo + 16):
+            c = sum(cost(N, rb, sh, SEQ, kind, direct) for kind, direct in KINDS)
+            key = (c, SEQ, sh)
+            if best is None or key < best:
+                best = key
+    return family, N, rb, best[2], best[1], best[0]
+
+
+def main():
+    jobs = [("pow2", N, rb) for N in POW2 for rb in (4, 8)] + [("mr", N, rb) for N in MR for rb in (4, 8)]
+    with get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        res = pool.map(best_layout, jobs)
+    table = {(f, N, rb): (sh, seq) for f, N, rb, sh, seq, _ in res}
+    out = ["// Generated by gen_smem_layout.py: shared-memory sequence layout (padding",
+           "// shift SH, sequence stride SEQ) of the pass kernels, chosen per length and",
+           "// precision by replaying the kernels' shared-memory accesses through a bank",
+           "// model.  Element i of sequence s sits at s*SEQ + i + (SH ? i >> SH : 0).",
+           "#pragma once", "", "namespace pb {", "", "struct SmemLayout {", "  int sh;", "  int seq;", "};", ""]
+    for family, lengths in (("pow2", POW2), ("mr", MR)):
+        out.append(f"// {family}: {{f32}}, {{f64}} per length")
+        out.append(f"__host__ __device__ constexpr SmemLayout {family}_layout(int N, int real_bytes) {{")
+        out.append("  switch (N) {")
+        for N in lengths:
+            a, b = table[(family, N, 4)], table[(family, N, 8)]
+            out.append(f"    case {N}: return real_bytes == 4 ? SmemLayout{{{a[0]}, {a[1]}}} : SmemLayout{{{b[0]}, {b[1]}}};")
+        out.append("    default: return SmemLayout{3, N + N / 8 + 1};")
+        out.append("  }")
+        out.append("}")
+        out.append("")
+    out.append("}  // namespace pb")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "smem_layout.hpp")
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+    for f, N, rb, sh, seq, c in sorted(res):
+        print(f, N, rb, sh, seq, c)
+
+
+if __name__ == "__main__":
+    main()

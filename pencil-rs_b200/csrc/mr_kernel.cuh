@@ -1,0 +1,562 @@
+// Mixed-radix fused pass for 7-smooth line lengths that are not powers of two
+// (35, 210, 384, ...): the C2C, R2C and C2R stages of the canonical route for
+// those lengths.  Power-of-two lengths take pow2_kernel.cu.
+//
+// The length N is a template parameter, so the radix schedule (radix 8 while
+// it divides, then 4 or 2, then 7, 5, 3, with the stage-0 radix chosen to fit
+// the tile to the threads) and every index division are compile-time.
+// Persistent CTAs of 256 threads walk the pass's tiles of NSEQ complex
+// sequences (one line each, or a pair of real lines for R2C/C2R).  Stage 0
+// reads its butterfly inputs from HBM straight into registers; the next tile's
+// inputs are loaded before the current tile is transformed, its descriptor two
+// tiles ahead and the piece rows of the transposed store one tile ahead, so the
+// loads overlap the arithmetic and no load waits on another.  Later stages
+// alternate between two shared-memory buffers (padded layout from
+// smem_layout.hpp), one barrier per stage; for a direct C2C or C2R store the
+// last stage writes straight to HBM.  Twiddles come from the table of N-th
+// roots (generated on the host in extended precision, rounded once), copied
+// once per CTA into a per-stage table whose entries the lanes of a stage read
+// consecutively.  The store is direct (transform axis contiguous in the
+// destination) or transposed through shared memory so that the lines of a
+// tile form runs of the destination's innermost axis (the fused pencil
+// transpose), with host-precomputed tile, piece and k tables as in the
+// power-of-two kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pb_aux.hpp"
+#include "pb_device.cuh"
+#include "pb_fft.cuh"
+#include "smem_layout.hpp"
+
+namespace pb {
+
+constexpr int MR_THREADS = 256;
+
+struct RadixList {
+  int n;
+  int r[24];
+};
+
+__host__ __device__ constexpr RadixList mr_factor(int N) {
+  RadixList L{0, {}};
+  int m = N;
+  while (m % 8 == 0 && m > 1) {
+    L.r[L.n++] = 8;
+    m /= 8;
+  }
+  if (m % 4 == 0) {
+    L.r[L.n++] = 4;
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    L.r[L.n++] = 2;
+    m /= 2;
+  }
+  while (m % 7 == 0) {
+    L.r[L.n++] = 7;
+    m /= 7;
+  }
+  while (m % 5 == 0) {
+    L.r[L.n++] = 5;
+    m /= 5;
+  }
+  while (m % 3 == 0) {
+    L.r[L.n++] = 3;
+    m /= 3;
+  }
+  return L;
+}
+
+// Radix schedule of N for tiles of NSEQ sequences: the factors of mr_factor
+// with the stage-0 radix moved to the front.  Stage 0 keeps U0*R0 values per
+// thread in registers (U0 = ceil(NSEQ*N/R0 / threads)), so R0 is the radix
+// that minimises that count (the larger radix on a tie).
+__host__ __device__ constexpr RadixList mr_sched(int N, int NSEQ) {
+  RadixList L = mr_factor(N);
+  int best = 0, best_cost = 1 << 30;
+  for (int i = 0; i < L.n; ++i) {
+    const int R = L.r[i];
+    const int cost = ((NSEQ * (N / R) + MR_THREADS - 1) / MR_THREADS) * R;
+    if (cost < best_cost || (cost == best_cost && R > L.r[best])) {
+      best = i;
+      best_cost = cost;
+    }
+  }
+  const int r0 = L.r[best];
+  for (int i = best; i > 0; --i) L.r[i] = L.r[i - 1];
+  L.r[0] = r0;
+  return L;
+}
+
+// Product of the first s radices of the schedule.
+__host__ __device__ constexpr int mr_ns(int N, int NSEQ, int s) {
+  const RadixList L = mr_sched(N, NSEQ);
+  int p = 1;
+  for (int i = 0; i < s; ++i) p *= L.r[i];
+  return p;
+}
+
+__host__ __device__ constexpr int mr_pow2floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+
+// Offset of stage ST's twiddles in the per-stage twiddle table: stage s >= 1
+// holds (R_s - 1)*NS_s entries, entry (r-1)*NS_s + k = W_N^{k*r*N/(NS_s*R_s)},
+// so the lanes of a stage read consecutive entries (N - R_0 entries in all).
+__host__ __device__ constexpr int mr_tw_off(int N, int NSEQ, int ST) {
+  const RadixList L = mr_sched(N, NSEQ);
+  int off = 0, ns = L.r[0];
+  for (int s = 1; s < ST; ++s) {
+    off += (L.r[s] - 1) * ns;
+    ns *= L.r[s];
+  }
+  return off;
+}
+
+// Complex elements per tile: 3072 (24 KB) in f32, 1536 (24 KB) in f64.
+template <typename R, int N>
+struct MRGeom {
+  static constexpr int NST = mr_factor(N).n;
+  static constexpr int TILE_ELEMS = sizeof(R) == 4 ? 3072 : 1536;
+  static constexpr int FIT = TILE_ELEMS / N;
+  static constexpr int NSEQ = FIT >= 64 ? 64 : (FIT < 2 ? 2 : mr_pow2floor(FIT));
+  // shared-memory layout (bank-conflict model of gen_smem_layout.py): element
+  // i of sequence s at s*SEQ + pad(i)
+  static constexpr SmemLayout LAY = mr_layout(N, (int)sizeof(R));
+  static constexpr int SH = LAY.sh;
+  static constexpr int SEQ = LAY.seq;
+  static constexpr int R0 = mr_sched(N, NSEQ).r[0];
+  static constexpr int NB0 = N / R0;
+  static constexpr int B0 = NSEQ * NB0;                         // stage-0 butterflies per tile
+  static constexpr int U0 = (B0 + MR_THREADS - 1) / MR_THREADS;  // per thread
+  static constexpr int NTW = N - R0;                             // per-stage twiddle entries
+  static __device__ __forceinline__ int pad(int i) { return SH == 0 ? i : i + (i >> SH); }
+};
+
+// Stockham stage ST >= 1 from shared buffer `in` to shared buffer `out`: for
+// butterfly jb of a sequence (k = jb mod NS), inputs jb + r*N/RAD times
+// W_N^{k*r*N/(NS*RAD)}, outputs (jb - k)*RAD + k + r*NS.
+template <typename R, int N, int ST, bool INV>
+__device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ in, typename Cx<R>::T* __restrict__ out,
+                                         const typename Cx<R>::T* __restrict__ Wst) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr RadixList RL = mr_sched(N, G::NSEQ);
+  constexpr int RAD = RL.r[ST];
+  constexpr int NS = mr_ns(N, G::NSEQ, ST);
+  constexpr int NB = N / RAD;
+  constexpr int TOT = G::NSEQ * NB;
+  constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
+  const C* __restrict__ tw = Wst + mr_tw_off(N, G::NSEQ, ST);
+#pragma unroll 1
+  for (int it = 0; it < ITER; ++it) {
+    const int b = threadIdx.x + it * MR_THREADS;
+    if (TOT % MR_THREADS != 0 && b >= TOT) break;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    const int k = jb % NS;
+    const C* src = in + s * G::SEQ;
+    C* dst = out + s * G::SEQ;
+    C v[RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) v[r] = src[G::pad(jb + r * NB)];
+#pragma unroll
+    for (int r = 1; r < RAD; ++r) v[r] = twmul<INV>(v[r], tw[(r - 1) * NS + k]);
+    Bfly<C, RAD, INV>::run(v);
+    const int base = (jb - k) * RAD + k;
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) dst[G::pad(base + r * NS)] = v[r];
+  }
+}
+
+// Stages ST .. END-1 of one tile (ST >= 1): stage i reads b0 when i is odd
+// and b1 when it is even (stage 0 writes b0), with a barrier after each.
+template <typename R, int N, bool INV, int ST, int END>
+__device__ __forceinline__ void mr_stages_upto(typename Cx<R>::T* b0, typename Cx<R>::T* b1,
+                                               const typename Cx<R>::T* Wst) {
+  if constexpr (ST < END) {
+    if constexpr (ST % 2 == 1)
+      mr_stage<R, N, ST, INV>(b0, b1, Wst);
+    else
+      mr_stage<R, N, ST, INV>(b1, b0, Wst);
+    __syncthreads();
+    mr_stages_upto<R, N, INV, ST + 1, END>(b0, b1, Wst);
+  }
+}
+
+// Fills the per-stage twiddle table from the table of N-th roots.
+template <typename R, int N, int ST>
+__device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const typename Cx<R>::T* __restrict__ Wg) {
+  using G = MRGeom<R, N>;
+  if constexpr (ST < G::NST) {
+    constexpr RadixList RL = mr_sched(N, G::NSEQ);
+    constexpr int RAD = RL.r[ST];
+    constexpr int NS = mr_ns(N, G::NSEQ, ST);
+    constexpr int TW = N / (NS * RAD);
+    constexpr int OFF = mr_tw_off(N, G::NSEQ, ST);
+    for (int i = threadIdx.x; i < (RAD - 1) * NS; i += MR_THREADS) {
+      const int r = i / NS + 1, k = i - (i / NS) * NS;
+      Wst[OFF + i] = Wg[k * TW * r];
+    }
+    mr_fill_twiddles<R, N, ST + 1>(Wst, Wg);
+  }
+}
+
+// Loads the stage-0 butterfly inputs of one tile into registers: butterfly b
+// (sequence b / NB0, index jb) takes elements jb + r*NB0 of its sequence.
+template <typename R, int N>
+__device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0], const PassArgs& A,
+                                        const TileAddr& ta) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NB = G::NB0;
+  constexpr int R0 = G::R0;
+  const R zero = R(0);
+  const int L = ta.lines;
+#pragma unroll
+  for (int u = 0; u < G::U0; ++u) {
+    const int b = threadIdx.x + u * MR_THREADS;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
+    if (A.kind == P_C2C) {
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok = live && s < L;
+      const long long base = ta.src0 + (long long)s * ta.srcb + jb;
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[u][r] = ok ? in[base + r * NB] : mk<C, R>(zero, zero);
+    } else if (A.kind == P_R2C) {
+      const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+      const bool ok0 = live && 2 * s < L, ok1 = live && 2 * s + 1 < L;
+      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb + jb;
+      const long long b1 = b0 + ta.srcb;
+#pragma unroll
+      for (int r = 0; r < R0; ++r)
+        v[u][r] = mk<C, R>(ok0 ? in[b0 + r * NB] : zero, ok1 ? in[b1 + r * NB] : zero);
+    } else {  // C2R: Hermitian extension of two half spectra
+      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+      const bool ok0 = live && 2 * s < L, ok1 = live && 2 * s + 1 < L;
+      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
+      const long long b1 = b0 + ta.srcb;
+      const R w_in = R(A.pre_factor);
+      const bool weighted = A.pre_mode == W_HALF_INTERIOR;
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int q = jb + r * NB;
+        const bool mirror = 2 * q > N;
+        const int hq = mirror ? N - q : q;
+        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
+        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
+        const bool edge = (hq == 0) || (2 * hq == N);
+        if (mirror) {
+          X.y = -X.y;
+          Y.y = -Y.y;
+        }
+        if (edge) {
+          X.y = zero;
+          Y.y = zero;
+        }
+        const R w = (weighted && !edge) ? w_in : R(1);
+        v[u][r] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
+      }
+    }
+  }
+}
+
+// Stage 0 (no twiddles) on the registers; outputs jb*R0 + r go to `out`.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                          typename Cx<R>::T* out) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NB = G::NB0;
+  constexpr int R0 = G::R0;
+#pragma unroll
+  for (int u = 0; u < G::U0; ++u) {
+    const int b = threadIdx.x + u * MR_THREADS;
+    if (G::B0 % MR_THREADS != 0 && b >= G::B0) break;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    C t[R0];
+#pragma unroll
+    for (int r = 0; r < R0; ++r) t[r] = v[u][r];
+    Bfly<C, R0, INV>::run(t);
+    C* dst = out + s * G::SEQ;
+#pragma unroll
+    for (int r = 0; r < R0; ++r) dst[G::pad(jb * R0 + r)] = t[r];
+  }
+}
+
+// Last stage with the direct C2C or C2R store: in the last Stockham stage
+// (NS = N/RAD) butterfly jb writes outputs jb + r*NB, so each output goes
+// straight to HBM, coalesced across the threads of a sequence.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const TileAddr& ta,
+                                                    const typename Cx<R>::T* __restrict__ in,
+                                                    const typename Cx<R>::T* __restrict__ W) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int ST = G::NST - 1;
+  constexpr RadixList RL = mr_sched(N, G::NSEQ);
+  constexpr int RAD = RL.r[ST];
+  constexpr int NB = N / RAD;
+  constexpr int TOT = G::NSEQ * NB;
+  constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
+  const int L = ta.lines;
+  const R sc = R(A.scale);
+  const C* __restrict__ tw = W + mr_tw_off(N, G::NSEQ, ST);
+#pragma unroll 1
+  for (int it = 0; it < ITER; ++it) {
+    const int b = threadIdx.x + it * MR_THREADS;
+    if (TOT % MR_THREADS != 0 && b >= TOT) break;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    const C* src = in + s * G::SEQ;
+    C v[RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) v[r] = src[G::pad(jb + r * NB)];
+#pragma unroll
+    for (int r = 1; r < RAD; ++r) v[r] = twmul<INV>(v[r], tw[(r - 1) * NB + jb]);  // k = jb, NS = NB
+    Bfly<C, RAD, INV>::run(v);
+    if (A.kind == P_C2C) {
+      if (s < L) {
+        C* __restrict__ out = reinterpret_cast<C*>(A.out) + ta.dst0 + (long long)s * ta.dstb + jb;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) out[r * NB] = scl(v[r], sc);
+      }
+    } else {
+      R* __restrict__ out = reinterpret_cast<R*>(A.out) + ta.dst0 + (long long)(2 * s) * ta.dstb + jb;
+      if (2 * s < L) {
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) out[r * NB] = v[r].x * sc;
+      }
+      if (2 * s + 1 < L) {
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) out[ta.dstb + r * NB] = v[r].y * sc;
+      }
+    }
+  }
+}
+
+// Stores the natural-order results `res` of one tile (R2C direct, or any
+// transposed store; element (k, line j) of a transposed store goes to
+// Atab[k] + j, each thread writing the pair of lines (j, j+1), as one 16-byte
+// vector where aligned in f32).
+template <typename R, int N>
+__device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
+                                         const long long* Atab) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NSEQ = G::NSEQ;
+  constexpr int SEQ = G::SEQ;
+  constexpr int H = N / 2 + 1;
+  const int tid = threadIdx.x;
+  const int kind = A.kind;
+  const int L = ta.lines;
+  const R sc = R(A.scale);
+  const R pf = R(A.post_factor);
+  const bool post_weighted = A.post_mode == W_HALF_INTERIOR;
+
+  if (A.dst_k_contig) {  // R2C: split the pair's spectrum, half spectrum of each line
+    C* __restrict__ out = reinterpret_cast<C*>(A.out);
+    for (int i = tid; i < 2 * NSEQ * H; i += MR_THREADS) {
+      const int l = i / H, k = i - l * H;
+      if (l >= L) continue;
+      const C* seq = res + (l >> 1) * SEQ;
+      const C a = seq[G::pad(k)];
+      const C b = seq[G::pad(k == 0 ? 0 : N - k)];
+      R f = sc * R(0.5);
+      if (post_weighted && k != 0 && 2 * k != N) f *= pf;
+      out[ta.dst0 + (long long)l * ta.dstb + k] = (l & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f)
+                                                         : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+    }
+    return;
+  }
+  if (kind == P_C2R) {
+    R* __restrict__ out = reinterpret_cast<R*>(A.out);
+    for (int i = tid; i < NSEQ * N; i += MR_THREADS) {
+      const int p = i % NSEQ, k = i / NSEQ;
+      if (2 * p >= L) continue;
+      const C z = res[p * SEQ + G::pad(k)];
+      const long long o = Atab[k] + 2 * p;
+      out[o] = z.x * sc;
+      if (2 * p + 1 < L) out[o + 1] = z.y * sc;
+    }
+    return;
+  }
+  constexpr int PAIRS = (NSEQ + 1) / 2;  // C2C: line pairs per k
+  const int total = (kind == P_R2C) ? NSEQ * H : PAIRS * N;
+  const int per_k = (kind == P_R2C) ? NSEQ : PAIRS;
+  C* __restrict__ out = reinterpret_cast<C*>(A.out);
+  for (int i = tid; i < total; i += MR_THREADS) {
+    const int p = i % per_k, k = i / per_k;
+    const int j = 2 * p;
+    if (j >= L) continue;
+    C v0, v1;
+    if (kind == P_C2C) {
+      v0 = scl(res[j * SEQ + G::pad(k)], sc);
+      v1 = (j + 1 < L) ? scl(res[(j + 1) * SEQ + G::pad(k)], sc) : v0;
+    } else {
+      const C* seq = res + p * SEQ;
+      const C a = seq[G::pad(k)];
+      const C b = seq[G::pad(k == 0 ? 0 : N - k)];
+      R f = sc * R(0.5);
+      if (post_weighted && k != 0 && 2 * k != N) f *= pf;
+      v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+      v1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
+    }
+    const long long o = Atab[k] + j;
+    if (j + 1 < L) {
+      if (sizeof(R) == 4 && (o & 1) == 0) {
+        float4 w;
+        w.x = (float)v0.x;
+        w.y = (float)v0.y;
+        w.z = (float)v1.x;
+        w.w = (float)v1.y;
+        *reinterpret_cast<float4*>(out + o) = w;
+      } else {
+        out[o] = v0;
+        out[o + 1] = v1;
+      }
+    } else {
+      out[o] = v0;
+    }
+  }
+}
+
+constexpr int MR_MAX_PIECES = 64;  // pieces of a transposed store (the plan allows at most 64)
+
+// Shared memory of one CTA: two buffers of NSEQ padded sequences, the twiddle
+// table, and the destination rows, k table and piece rows of the transposed
+// store.
+template <typename R, int N>
+__host__ __device__ constexpr size_t mr_smem_bytes() {
+  return (2 * (size_t)MRGeom<R, N>::NSEQ * MRGeom<R, N>::SEQ + ((N + 1) & ~1)) * 2 * sizeof(R) + (size_t)N * 16 +
+         (size_t)MR_MAX_PIECES * 16;
+}
+
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
+                                        typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                        typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
+                                        long long* Atab, const int2* ktab, PieceAddr* prow, const PieceAddr& my_piece,
+                                        int npieces) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  const int tid = threadIdx.x;
+  const bool direct = A.dst_k_contig != 0;
+  const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
+  mr_stage0<R, N, INV>(v, b0);
+  if (tid < npieces) prow[tid] = my_piece;
+  __syncthreads();
+  if (!direct) {
+    // destination row of each k of this tile (read after later barriers)
+    for (int k = tid; k < nout; k += MR_THREADS) {
+      const int2 kp = ktab[k];
+      const PieceAddr pa = prow[kp.x];
+      Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+    }
+  }
+  if (direct && A.kind != P_R2C) {
+    // stages 1 .. NST-2 in shared memory, the last one to HBM
+    mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
+    mr_last_stage_store<R, N, INV>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W);
+    return;
+  }
+  mr_stages_upto<R, N, INV, 1, G::NST>(b0, b1, W);
+  mr_store<R, N>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab);
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int BUF = G::NSEQ * G::SEQ;
+  extern __shared__ __align__(16) unsigned char smem[];
+  C* b0 = reinterpret_cast<C*>(smem);
+  C* b1 = b0 + BUF;
+  C* W = b1 + BUF;
+  long long* Atab = reinterpret_cast<long long*>(W + ((N + 1) & ~1));
+  int2* ktab = reinterpret_cast<int2*>(Atab + N);
+  PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + N);
+
+  if (A.gate != nullptr && *A.gate != 0) return;
+  const long long G0 = gridDim.x;
+  long long tile = blockIdx.x;
+  if (tile >= A.ntiles) return;
+  const int tid = threadIdx.x;
+  const bool direct = A.dst_k_contig != 0;
+  const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
+  const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
+  const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
+  const int npieces = direct ? 0 : A.npieces;
+  {
+    const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
+    mr_fill_twiddles<R, N, 1>(W, Wg);
+    if (!direct)
+      for (int k = tid; k < nout; k += MR_THREADS) ktab[k] = A.ktab[k];
+  }
+  TileAddr ta = load_tile(tiles, tile);
+  C v[G::U0][G::R0];
+  mr_load<R, N>(v, A, ta);
+  TileAddr t1 = ta;
+  if (tile + G0 < A.ntiles) t1 = load_tile(tiles, tile + G0);
+  PieceAddr my_piece{0, 0};
+  if (tid < npieces) my_piece = pieces[tile * npieces + tid];
+  __syncthreads();  // twiddles and k table in place
+
+  for (;;) {
+    const bool has_next = tile + G0 < A.ntiles;
+    TileAddr t2 = t1;
+    PieceAddr next_piece{0, 0};
+    C nv[G::U0][G::R0];
+    if (has_next) {
+      mr_load<R, N>(nv, A, t1);
+      if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
+      if (tid < npieces) next_piece = pieces[(tile + G0) * npieces + tid];
+    }
+    if (A.inv)
+      mr_tile<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    else
+      mr_tile<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    if (!has_next) break;
+    tile += G0;
+    ta = t1;
+    t1 = t2;
+    my_piece = next_piece;
+#pragma unroll
+    for (int u = 0; u < G::U0; ++u)
+#pragma unroll
+      for (int r = 0; r < G::R0; ++r) v[u][r] = nv[u][r];
+    __syncthreads();  // this tile's buffers and row tables are read before the next tile writes them
+  }
+}
+
+// Host entry points of one length (instantiated by mr_kernels.cu).
+template <typename R, int N>
+cudaError_t mr_launch(const PassArgs& A, cudaStream_t stream) {
+  constexpr size_t smem = mr_smem_bytes<R, N>();
+  cudaError_t err = cudaFuncSetAttribute(mr_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
+  if (grid > A.ntiles) grid = A.ntiles;
+  mr_kernel<R, N><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+template <typename R, int N>
+int mr_occupancy() {
+  constexpr size_t smem = mr_smem_bytes<R, N>();
+  int blocks = 0;
+  if (cudaFuncSetAttribute(mr_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_kernel<R, N>, MR_THREADS, smem) != cudaSuccess)
+    return 1;
+  return blocks > 0 ? blocks : 1;
+}
+
+}  // namespace pb

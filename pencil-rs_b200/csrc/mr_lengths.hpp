@@ -1,0 +1,38 @@
+// Line lengths served by the mixed-radix pass kernel (mr_kernel.cuh): the
+// 79 numbers 2^a 3^b 5^c 7^d in [35, 504] that are not powers of two.  The
+// kernels are split over MR_GROUPS translation units (mr_kernels.cu compiled
+// once per group) so that they build in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pb_internal.hpp"
+
+namespace pb {
+
+constexpr int kMrLengths[] = {35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  60,  63,  70,  72,  75,  80,
+                              81,  84,  90,  96,  98,  100, 105, 108, 112, 120, 125, 126, 135, 140, 144, 147,
+                              150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
+                              245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375,
+                              378, 384, 392, 400, 405, 420, 432, 441, 448, 450, 480, 486, 490, 500, 504};
+constexpr int kMrCount = sizeof(kMrLengths) / sizeof(kMrLengths[0]);
+constexpr int MR_GROUPS = 8;
+
+// Entry points of one (precision, length) instantiation.
+struct MrEntry {
+  cudaError_t (*launch)(const PassArgs&, cudaStream_t);
+  int (*occupancy)();
+  int nseq;  // complex sequences per tile
+};
+
+// Filled by group g: entries i with i % MR_GROUPS == g of both tables.
+void mr_fill_group0(MrEntry* f32, MrEntry* f64);
+void mr_fill_group1(MrEntry* f32, MrEntry* f64);
+void mr_fill_group2(MrEntry* f32, MrEntry* f64);
+void mr_fill_group3(MrEntry* f32, MrEntry* f64);
+void mr_fill_group4(MrEntry* f32, MrEntry* f64);
+void mr_fill_group5(MrEntry* f32, MrEntry* f64);
+void mr_fill_group6(MrEntry* f32, MrEntry* f64);
+void mr_fill_group7(MrEntry* f32, MrEntry* f64);
+
+}  // namespace pb

@@ -636,6 +636,7 @@ size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
 }
 
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.fast == 2) return launch_mr(A, real_bytes, stream);
   if (A.fast) return launch_pow2(A, real_bytes, stream);
   const size_t smem = pass_smem_bytes(A, real_bytes);
   if (A.ntiles <= 0) return cudaSuccess;

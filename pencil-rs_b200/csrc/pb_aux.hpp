@@ -82,6 +82,11 @@ int batch_occupancy(int real_bytes, size_t smem);
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int pow2_lines(int m, int kind, int real_bytes);
 int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes);
+// mixed-radix pass kernel (mr_kernel.cuh) for the lengths of mr_lengths.hpp
+bool mr_supported(int m, int real_bytes);
+cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream);
+int mr_lines(int m, int kind, int real_bytes);
+int mr_occupancy(int m, int real_bytes);
 size_t pass_smem_bytes(const PassArgs& A, int real_bytes);
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_remap(const RemapArgs& A, cudaStream_t stream);

@@ -776,7 +776,8 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
   if (A.fast) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int occ = pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
+    const int occ = A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
+                                : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
     A.grid_ctas = sms * std::max(1, occ);
   }
 }
@@ -859,6 +860,19 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.fast = 1;
       A.dst_k_contig = direct ? 1 : 0;
       L = pow2_lines(A.m, op.kind, P.real_bytes);
+      A.lines = L;
+    }
+  }
+  // register-fed mixed-radix kernel: the same layouts, 7-smooth lengths
+  if (!A.fast && !P.force_generic && (op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) &&
+      mr_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    if (direct || transposed) {
+      A.fast = 2;
+      A.dst_k_contig = direct ? 1 : 0;
+      L = mr_lines(A.m, op.kind, P.real_bytes);
       A.lines = L;
     }
   }
@@ -1642,6 +1656,21 @@ int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capac
     int n = 0;
     for (const Step& s : prog.steps) {
       if (kinds && n < capacity) kinds[n] = s.type;
+      ++n;
+    }
+    if (count) *count = n;
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int32_t capacity, int32_t* count) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    const Program& prog = plan->prog[user_mode(*plan, op)];
+    int n = 0;
+    for (const Step& s : prog.steps) {
+      const int k = s.type != 0 ? 1 : (s.pa.fast == 1 ? 2 : (s.pa.fast == 2 ? 3 : 0));
+      if (kernels && n < capacity) kernels[n] = k;
       ++n;
     }
     if (count) *count = n;

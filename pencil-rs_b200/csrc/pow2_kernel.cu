@@ -15,16 +15,21 @@
 // kernel.  Results are stored either directly (transform axis contiguous in
 // the destination) or through shared memory transposed so that the L lines of
 // a tile form contiguous runs of the destination's innermost axis (the fused
-// pencil transpose).  Tile and row addresses are precomputed on the host.
+// pencil transpose).  Tile and row addresses are precomputed on the host;
+// each CTA fetches tile descriptors two tiles ahead and the piece rows of the
+// transposed store one tile ahead, and keeps the k table in shared memory, so
+// no global load waits on the result of another.
 #include <cuda_runtime.h>
 
 #include "pb_aux.hpp"
 #include "pb_device.cuh"
 #include "pb_fft.cuh"
+#include "smem_layout.hpp"
 
 namespace pb {
 
 constexpr int P2_THREADS = 256;
+constexpr int P2_MAX_PIECES = 64;  // pieces of a transposed store (the plan allows at most 64)
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 __host__ __device__ constexpr int ipow8(int s) { return s == 0 ? 1 : 8 * ipow8(s - 1); }
@@ -45,10 +50,13 @@ struct P2Geom {
   static constexpr int SLOTS = P2_THREADS / T;
   static constexpr int LPT = (sizeof(R) == 4 && N >= 64 && N <= 512) ? 2 : 1;
   static constexpr int NSEQ = SLOTS * LPT;
-  static constexpr int SEQ = N + N / 8 + 1;  // padded sequence stride (complex units)
+  // shared-memory layout (bank-conflict model of gen_smem_layout.py): element
+  // i of sequence s at s*SEQ + pad(i)
+  static constexpr SmemLayout LAY = pow2_layout(N, (int)sizeof(R));
+  static constexpr int SH = LAY.sh;
+  static constexpr int SEQ = LAY.seq;
+  static __device__ __forceinline__ int pad(int i) { return SH == 0 ? i : i + (i >> SH); }
 };
-
-__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
 
 // One Stockham stage on the 8 register values of each of the thread's sequences.
 template <typename C, int N, int ST, bool INV, int LPT>
@@ -161,8 +169,11 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   C* sm = reinterpret_cast<C*>(smem);
   long long* Atab = reinterpret_cast<long long*>(sm + NSEQ * SEQ);
+  int2* ktab = reinterpret_cast<int2*>(Atab + NOUT);
+  PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + NOUT);
 
   if (A.gate != nullptr && *A.gate != 0) return;
+  const long long G0 = gridDim.x;
   long long tile = blockIdx.x;
   if (tile >= A.ntiles) return;
   const int tid = threadIdx.x;
@@ -170,6 +181,11 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   const int t = tid - slot * T;
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
+  const int npieces = DIRECT ? 0 : A.npieces;
+  // the k table of the transposed store, once per CTA (visible after the
+  // first barrier)
+  if (!DIRECT)
+    for (int k = tid; k < NOUT; k += P2_THREADS) ktab[k] = A.ktab[k];
 
   // twiddles of this thread, fixed for the whole kernel: stage ST > 0 (radix 8)
   // multiplies input r by W_N^{k*r*N/(NS*8)} with k = t mod NS
@@ -188,18 +204,25 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 
   const R sc = R(A.scale);
   const R pf = R(A.post_factor);
+  // tile descriptors are fetched two tiles ahead and piece rows one tile
+  // ahead, so the prefetch of a tile never waits on the load of its address
   TileAddr ta = load_tile(tiles, tile);
   C v[LPT][8];
   p2_load<R, N, KIND, LPT>(v, A, ta, slot, t);
+  TileAddr t1 = ta;
+  if (tile + G0 < A.ntiles) t1 = load_tile(tiles, tile + G0);
+  PieceAddr my_piece{0, 0};
+  if (tid < npieces) my_piece = pieces[tile * npieces + tid];
 
   for (;;) {
-    const long long next = tile + gridDim.x;
-    const bool has_next = next < A.ntiles;
-    TileAddr tn;
+    const bool has_next = tile + G0 < A.ntiles;
+    TileAddr t2 = t1;
+    PieceAddr next_piece{0, 0};
     C nv[LPT][8];
     if (has_next) {
-      tn = load_tile(tiles, next);
-      p2_load<R, N, KIND, LPT>(nv, A, tn, slot, t);
+      p2_load<R, N, KIND, LPT>(nv, A, t1, slot, t);
+      if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
+      if (tid < npieces) next_piece = pieces[(tile + G0) * npieces + tid];
     }
     const int L = ta.lines;
 
@@ -211,7 +234,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
         for (int i = 0; i < LPT; ++i) {
           const C* seq = sm + (slot + SLOTS * i) * SEQ;
 #pragma unroll
-          for (int m = 0; m < 8; ++m) v[i][m] = seq[pad8(t + T * m)];
+          for (int m = 0; m < 8; ++m) v[i][m] = seq[G::pad(t + T * m)];
         }
       }
       switch (st) {
@@ -233,10 +256,19 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
               case 1: o = p2_out_index<N, (S::NST > 1 ? 1 : 0)>(t, q); break;
               default: o = p2_out_index<N, (S::NST > 2 ? 2 : 0)>(t, q); break;
             }
-            seq[pad8(o)] = v[i][q];
+            seq[G::pad(o)] = v[i][q];
           }
         }
+        if (!DIRECT && st == 0 && tid < npieces) prow[tid] = my_piece;
         __syncthreads();
+        if (!DIRECT && st == 0) {
+          // destination row of each k of this tile (read after later barriers)
+          for (int k = tid; k < NOUT; k += P2_THREADS) {
+            const int2 kp = ktab[k];
+            const PieceAddr pa = prow[kp.x];
+            Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+          }
+        }
       }
     }
     // thread t now holds natural-order outputs t + T*r
@@ -272,15 +304,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
       for (int i = 0; i < LPT; ++i) {
         C* seq = sm + (slot + SLOTS * i) * SEQ;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) seq[pad8(t + T * r)] = v[i][r];
-      }
-      if (!DIRECT) {
-        const PieceAddr* pt = pieces + tile * A.npieces;
-        for (int k = tid; k < NOUT; k += P2_THREADS) {
-          const int2 kp = A.ktab[k];
-          const PieceAddr pa = pt[kp.x];
-          Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
-        }
+        for (int r = 0; r < 8; ++r) seq[G::pad(t + T * r)] = v[i][r];
       }
       __syncthreads();
       if (KIND == P_R2C && DIRECT) {
@@ -290,8 +314,8 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
           const int s = slot + SLOTS * i;
           const C* seq = sm + s * SEQ;
           for (int k = t; k < H; k += T) {
-            const C a = seq[pad8(k)];
-            const C b = seq[pad8((N - k) & (N - 1))];
+            const C a = seq[G::pad(k)];
+            const C b = seq[G::pad((N - k) & (N - 1))];
             R f = sc * R(0.5);
             if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
             if (2 * s < L) out[ta.dst0 + (long long)(2 * s) * ta.dstb + k] = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
@@ -315,12 +339,12 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
             C v0, v1;
             if (KIND == P_C2C) {
               // row j + 1 exists only when the tile holds that line (j + 1 < L <= NSEQ)
-              v0 = scl(sm[j * SEQ + pad8(k)], sc);
-              v1 = (j + 1 < L) ? scl(sm[(j + 1) * SEQ + pad8(k)], sc) : v0;
+              v0 = scl(sm[j * SEQ + G::pad(k)], sc);
+              v1 = (j + 1 < L) ? scl(sm[(j + 1) * SEQ + G::pad(k)], sc) : v0;
             } else {
               const C* seq = sm + (j >> 1) * SEQ;
-              const C a = seq[pad8(k)];
-              const C b = seq[pad8((N - k) & (N - 1))];
+              const C a = seq[G::pad(k)];
+              const C b = seq[G::pad((N - k) & (N - 1))];
               R f = sc * R(0.5);
               if (weighted && k != 0 && k != N / 2) f *= pf;
               v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
@@ -349,7 +373,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
             const int j = 2 * (idx & (PAIRS - 1));
             const int k = idx / PAIRS;
             if (j >= L) continue;
-            const C z = sm[(j >> 1) * SEQ + pad8(k)];
+            const C z = sm[(j >> 1) * SEQ + G::pad(k)];
             const long long o = Atab[k] + j;
             out[o] = z.x * sc;
             if (j + 1 < L) out[o + 1] = z.y * sc;
@@ -359,8 +383,10 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     }
 
     if (!has_next) break;
-    tile = next;
-    ta = tn;
+    tile += G0;
+    ta = t1;
+    t1 = t2;
+    my_piece = next_piece;
 #pragma unroll
     for (int i = 0; i < LPT; ++i)
 #pragma unroll
@@ -377,10 +403,12 @@ static int p2_lines(int kind) {
   return kind == P_C2C ? P2Geom<R, N>::NSEQ : 2 * P2Geom<R, N>::NSEQ;
 }
 
+// sequences, destination rows (8 B per k), k table (8 B per k), piece rows
 template <typename R, int N>
 static size_t p2_smem(int kind) {
   const int nout = (kind == P_R2C) ? N / 2 + 1 : N;
-  return (size_t)P2Geom<R, N>::NSEQ * P2Geom<R, N>::SEQ * sizeof(typename Cx<R>::T) + (size_t)nout * 8;
+  return (size_t)P2Geom<R, N>::NSEQ * P2Geom<R, N>::SEQ * sizeof(typename Cx<R>::T) + (size_t)nout * 16 +
+         (size_t)P2_MAX_PIECES * sizeof(PieceAddr);
 }
 
 template <typename R, int N, int KIND, bool INV, bool DIRECT>

@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -18,8 +19,14 @@ INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libpencil_b200.so")
 
-SOURCES = ["pass_kernel.cu", "pow2_kernel.cu", "aux_kernels.cu", "plan.cpp", "no_alloc.cu"]
-HEADERS = ["pb_internal.hpp", "pb_aux.hpp", "pb_device.cuh", "pb_fft.cuh"]
+# (source, object, preprocessor definitions): mr_kernels.cu is compiled once
+# per group of lengths (MR_GROUPS in mr_lengths.hpp) so the groups build in parallel
+MR_GROUPS = 8
+SOURCES = ([(s, s + ".o", []) for s in ("pass_kernel.cu", "pow2_kernel.cu", "aux_kernels.cu", "plan.cpp",
+                                         "no_alloc.cu", "mr_dispatch.cpp")]
+           + [("mr_kernels.cu", f"mr_kernels_g{g}.o", [f"-DMR_GROUP={g}"]) for g in range(MR_GROUPS)])
+HEADERS = ["pb_internal.hpp", "pb_aux.hpp", "pb_device.cuh", "pb_fft.cuh", "mr_kernel.cuh", "mr_lengths.hpp",
+           "smem_layout.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,19 +47,25 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "pencil_b200.h")]
-    objs = []
-    for src in SOURCES:
+    objs, cmds = [], []
+    for src, oname, defs in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(BUILD, src + ".o")
+        obj = os.path.join(BUILD, oname)
         objs.append(obj)
         if force or _stale(obj, [path] + hdrs):
             cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
-                   "-I", CSRC, "-c", path, "-o", obj]
+                   "-I", CSRC, *defs, "-c", path, "-o", obj]
             if src.endswith(".cu"):
                 cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=jobs) as pool:
+        for proc in list(pool.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), cmds)):
+            if proc.returncode != 0:
+                sys.stderr.write(proc.stderr or "")
+                raise subprocess.CalledProcessError(proc.returncode, proc.args)
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         if verbose:

@@ -282,6 +282,16 @@ class _Plan:
         L.check(L.load().pb_plan_steps(self._h, op, kinds, cap, C.byref(cnt)), "steps")
         return ["check" if kinds[i] == 1 else "pass" for i in range(cnt.value)]
 
+    def step_kernels(self, op) -> list:
+        """Kernel family of each launch of one operation: "generic", "check",
+        "pow2" (register-resident power-of-two pass) or "mixed_radix"."""
+        cap = 64
+        ks = (C.c_int32 * cap)()
+        cnt = C.c_int32()
+        L.check(L.load().pb_plan_step_kernels(self._h, op, ks, cap, C.byref(cnt)), "step kernels")
+        names = ("generic", "check", "pow2", "mixed_radix")
+        return [names[ks[i]] for i in range(cnt.value)]
+
     _forward_checks = False
     _reverse_checks = False
 
