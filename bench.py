@@ -158,7 +158,7 @@ def reference_arm(args):
     return 0
 
 
-def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1):
+def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids=64):
     """Ragged batch: 64 C2C f32 grids, each axis length drawn (seed 4) from the
     55 numbers 2^a 3^b 5^c 7^d in [32, 256], 16 grids (25%) with an extra dim
     of 2, forward + inverse.  One graph-replayed persistent launch for the whole
@@ -170,6 +170,7 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1):
     rng = np.random.default_rng(4)
     shapes = [tuple(int(v) for v in rng.choice(smooth, 3)) for _ in range(64)]
     with_extra = set(int(i) for i in rng.choice(64, 16, replace=False))
+    shapes = shapes[:ngrids]
     from pencil_b200 import distributed as pbd
     mine = list(pbd.shard(len(shapes), rank, world))  # grids are independent: no exchange across GPUs
     gen = torch.Generator(device=dev).manual_seed(4 + rank)
@@ -231,9 +232,10 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1):
         nbytes += 2 * 3 * 2 * plan.info.input_elems * 8  # 2 directions x 3 passes x (read + write)
     nbytes = pbd.sum_over_ranks(nbytes)
     rt_b, rt_p, diff = (pbd.max_over_ranks(v) for v in (rt_b, rt_p, diff))
-    return {"grids": 64, "grids_per_gpu": len(mine), "with_extra": 16, "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
+    return {"grids": len(shapes), "grids_per_gpu": len(mine), "with_extra": len(with_extra & set(range(len(shapes)))), "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
             "speedup": times["per_grid"] / times["batch"], "gbs_batch": nbytes / (times["batch"] * 1e-3) / 1e9,
-            "launches_batch": 1, "launches_per_grid": 64 * (plans[0].info.passes_forward + plans[0].info.passes_inverse),
+            "launches_batch": 1,
+            "launches_per_grid": int(pbd.sum_over_ranks(sum(p.info.passes_forward + p.info.passes_inverse for p in plans))),
             "roundtrip_rel_l2_batch": rt_b, "roundtrip_rel_l2_per_grid": rt_p, "batch_vs_per_grid_rel_l2": diff,
             "bound": worst_bound, "shapes_seed": 4}
 
@@ -310,6 +312,10 @@ def b200_arm(args):
     # per-launch device times of the same steps (roofline of the pass kernel)
     kinds_f = plan.step_kinds(L.FORWARD)
     kinds_i = plan.step_kinds(L.INVERSE)
+    families = sorted(set(plan.step_kernels(L.FORWARD) + plan.step_kernels(L.INVERSE)) - {"check"})
+    kernel_names = ", ".join({"pow2": "pb::pow2_kernel<float, 512, kind, sign, store>",
+                              "mixed_radix": "pb::mr_kernel<float, N>",
+                              "generic": "pb::pass_kernel<float>"}[f] for f in families)
     fwd_t, inv_t = [], []
     for _ in range(max(3, min(args.steps, 10))):
         fwd_t.append(plan.execute_timed(L.FORWARD, x, spec, ws, stream))
@@ -390,7 +396,7 @@ def b200_arm(args):
 
     batch = None
     if not args.no_batch:
-        batch = batch_section(pb, L, torch, dev, rank=rank, world=world)
+        batch = batch_section(pb, L, torch, dev, rank=rank, world=world, ngrids=args.batch_grids)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -398,7 +404,7 @@ def b200_arm(args):
 
     if rank == 0:
         traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic_pass_kernel_512cube.json")
+        tpath = os.path.join(ROOT, "profiles", "traffic_pow2_kernel_512cube.json")
         if os.path.exists(tpath):
             with open(tpath) as f:
                 traffic = json.load(f).get("bytes_per_launch")
@@ -417,7 +423,7 @@ def b200_arm(args):
                          "e2e_roundtrip_rel_l2": e2e_err},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "pb::pass_kernel<float>", "bytes_per_launch": per_pass,
+                         "kernel": kernel_names, "bytes_per_launch": per_pass,
                          "launch_ms_avg": pass_ms / launches, "spectrum_check_ms": check_ms,
                          "launch_ms": {"forward": dict(zip([f"{i}:{k}" for i, k in enumerate(kinds_f)],
                                                            per_pass_ms[:len(kinds_f)])),
@@ -446,6 +452,8 @@ def main():
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-grid ragged-batch comparison")
+    ap.add_argument("--batch-grids", type=int, default=64,
+                    help="grids of the ragged batch (the first K of the 64-grid workload; profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

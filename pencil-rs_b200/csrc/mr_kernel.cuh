@@ -471,12 +471,18 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
   mr_store<R, N>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab);
 }
 
+// Tiles first, first + step, ... (< end) of one pass: the persistent loop of
+// the standalone kernel (first = blockIdx.x, step = gridDim.x) and of a chunk
+// of the batch kernel (step = 1).  `setup` loads the per-stage twiddles and
+// the k table into shared memory (the batch skips it when the CTA's previous
+// chunk belonged to the same pass).  Ends with this CTA's last store still
+// reading shared memory: the caller places a barrier before reusing it.
 template <typename R, int N>
-__global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
+__device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
+                                       unsigned char* smem, bool setup) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int BUF = G::NSEQ * G::SEQ;
-  extern __shared__ __align__(16) unsigned char smem[];
   C* b0 = reinterpret_cast<C*>(smem);
   C* b1 = b0 + BUF;
   C* W = b1 + BUF;
@@ -484,19 +490,16 @@ __global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
   int2* ktab = reinterpret_cast<int2*>(Atab + N);
   PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + N);
 
-  if (A.gate != nullptr && *A.gate != 0) return;
-  const long long G0 = gridDim.x;
-  long long tile = blockIdx.x;
-  if (tile >= A.ntiles) return;
+  long long tile = first;
+  if (tile >= end) return;
   const int tid = threadIdx.x;
   const bool direct = A.dst_k_contig != 0;
   const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
   const int npieces = direct ? 0 : A.npieces;
-  {
-    const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
-    mr_fill_twiddles<R, N, 1>(W, Wg);
+  if (setup) {
+    mr_fill_twiddles<R, N, 1>(W, reinterpret_cast<const C*>(A.twiddle));
     if (!direct)
       for (int k = tid; k < nout; k += MR_THREADS) ktab[k] = A.ktab[k];
   }
@@ -504,27 +507,27 @@ __global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
   C v[G::U0][G::R0];
   mr_load<R, N>(v, A, ta);
   TileAddr t1 = ta;
-  if (tile + G0 < A.ntiles) t1 = load_tile(tiles, tile + G0);
+  if (tile + step < end) t1 = load_tile(tiles, tile + step);
   PieceAddr my_piece{0, 0};
   if (tid < npieces) my_piece = pieces[tile * npieces + tid];
   __syncthreads();  // twiddles and k table in place
 
   for (;;) {
-    const bool has_next = tile + G0 < A.ntiles;
+    const bool has_next = tile + step < end;
     TileAddr t2 = t1;
     PieceAddr next_piece{0, 0};
     C nv[G::U0][G::R0];
     if (has_next) {
       mr_load<R, N>(nv, A, t1);
-      if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
-      if (tid < npieces) next_piece = pieces[(tile + G0) * npieces + tid];
+      if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
+      if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
     if (A.inv)
       mr_tile<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     else
       mr_tile<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     if (!has_next) break;
-    tile += G0;
+    tile += step;
     ta = t1;
     t1 = t2;
     my_piece = next_piece;
@@ -534,6 +537,13 @@ __global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
       for (int r = 0; r < G::R0; ++r) v[u][r] = nv[u][r];
     __syncthreads();  // this tile's buffers and row tables are read before the next tile writes them
   }
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (A.gate != nullptr && *A.gate != 0) return;
+  mr_run<R, N>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
 }
 
 // Host entry points of one length (instantiated by mr_kernels.cu).

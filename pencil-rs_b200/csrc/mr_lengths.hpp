@@ -18,6 +18,15 @@ constexpr int kMrLengths[] = {35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  
 constexpr int kMrCount = sizeof(kMrLengths) / sizeof(kMrLengths[0]);
 constexpr int MR_GROUPS = 8;
 
+// Lengths whose passes the persistent batch kernel (pass_kernel.cu) runs with
+// the mixed-radix tile code, f32 only: the 7-smooth numbers in [32, 256],
+// powers of two included.  Other passes of a batch take the generic tile code.
+constexpr int kBatchMrLengths[] = {32,  35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  60,  63,  64,
+                                   70,  72,  75,  80,  81,  84,  90,  96,  98,  100, 105, 108, 112, 120,
+                                   125, 126, 128, 135, 140, 144, 147, 150, 160, 162, 168, 175, 180, 189,
+                                   192, 196, 200, 210, 216, 224, 225, 240, 243, 245, 250, 252, 256};
+constexpr int kBatchMrCount = sizeof(kBatchMrLengths) / sizeof(kBatchMrLengths[0]);
+
 // Entry points of one (precision, length) instantiation.
 struct MrEntry {
   cudaError_t (*launch)(const PassArgs&, cudaStream_t);

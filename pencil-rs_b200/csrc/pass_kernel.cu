@@ -23,6 +23,8 @@
 #include "pb_aux.hpp"
 #include "pb_device.cuh"
 #include "pb_fft.cuh"
+#include "mr_kernel.cuh"
+#include "mr_lengths.hpp"
 
 namespace pb {
 
@@ -537,12 +539,62 @@ __global__ void __launch_bounds__(256) pass_kernel(const PassArgs A) {
 // were dequeued before it by resident CTAs.  Waits are bounded; a wait that
 // gives up sets B.error and the item is skipped.
 // ---------------------------------------------------------------------------
+// Mixed-radix chunk inside the batch kernel: tiles [t0, t1) of a pass whose
+// length is in kBatchMrLengths, run by the standalone kernel's prefetching
+// loop.  The per-stage twiddles and the k table are loaded only when the
+// CTA's previous chunk belonged to another pass (`fresh`).  Not inlined: each
+// length is register-allocated on its own.
+template <typename R, int N>
+__device__ __noinline__ void mr_batch_chunk(const PassArgs& A, long long t0, long long t1, unsigned char* smem,
+                                            bool fresh) {
+  mr_run<R, N>(A, t0, 1, t1, smem, fresh);
+}
+
+template <int I>
+__device__ __forceinline__ void mr_batch_dispatch(const PassArgs& A, long long t0, long long t1, unsigned char* smem,
+                                                  bool fresh) {
+  if constexpr (I < kBatchMrCount) {
+    constexpr int N = kBatchMrLengths[I];
+    if (A.m == N) {
+      mr_batch_chunk<float, N>(A, t0, t1, smem, fresh);
+      return;
+    }
+    mr_batch_dispatch<I + 1>(A, t0, t1, smem, fresh);
+  }
+}
+
+template <int I>
+static int mr_batch_geom(int m, int kind, size_t* smem) {
+  if constexpr (I < kBatchMrCount) {
+    constexpr int N = kBatchMrLengths[I];
+    if (m == N) {
+      if (smem) *smem = mr_smem_bytes<float, N>();
+      return kind == P_C2C ? MRGeom<float, N>::NSEQ : 2 * MRGeom<float, N>::NSEQ;
+    }
+    return mr_batch_geom<I + 1>(m, kind, smem);
+  } else {
+    (void)m;
+    (void)kind;
+    (void)smem;
+    return 0;
+  }
+}
+
+bool mr_batch_supported(int m, int real_bytes) { return real_bytes == 4 && mr_batch_geom<0>(m, P_C2C, nullptr) > 0; }
+int mr_batch_lines(int m, int kind) { return mr_batch_geom<0>(m, kind, nullptr); }
+size_t mr_batch_smem(int m) {
+  size_t s = 0;
+  mr_batch_geom<0>(m, P_C2C, &s);
+  return s;
+}
+
 template <typename R>
-__global__ void __launch_bounds__(256) batch_kernel(const BatchArgs B) {
+__global__ void __launch_bounds__(256, 2) batch_kernel(const BatchArgs B) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ PassArgs sA;
   __shared__ long long s_item;
-  __shared__ int s_desc, s_ok;
+  __shared__ int s_desc, s_ok, s_prev, s_fresh;
+  if (threadIdx.x == 0) s_prev = -1;
   for (;;) {
     if (threadIdx.x == 0) {
       const long long it = (long long)atomicAdd(B.head, 1ULL);
@@ -575,19 +627,38 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchArgs B) {
           __threadfence();
         }
         s_ok = ok;
+        s_fresh = lo != s_prev;
+        if (ok) s_prev = lo;
       }
     }
     __syncthreads();
     const long long it = s_item;
     if (it >= B.total_items) break;
     const int d = s_desc;
-    {
+    if (s_fresh) {  // descriptors do not change during a launch
       const int* src = reinterpret_cast<const int*>(B.descs + d);
       int* dst = reinterpret_cast<int*>(&sA);
       for (int i = threadIdx.x; i < (int)(sizeof(PassArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    if (s_ok) pass_tile<R>(sA, it - B.item_start[d], smem);
+    if (s_ok) {
+      // item -> chunk of batch_chunk consecutive tiles of the pass
+      const long long t0 = (it - B.item_start[d]) * sA.batch_chunk;
+      const long long t1 = t0 + sA.batch_chunk < sA.ntiles ? t0 + sA.batch_chunk : sA.ntiles;
+      bool done_mr = false;
+      if constexpr (sizeof(R) == 4) {
+        if (sA.fast == 2) {
+          mr_batch_dispatch<0>(sA, t0, t1, smem, s_fresh != 0);
+          done_mr = true;
+        }
+      }
+      if (!done_mr) {
+        for (long long t = t0; t < t1; ++t) {
+          if (t > t0) __syncthreads();
+          pass_tile<R>(sA, t, smem);
+        }
+      }
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -628,6 +699,7 @@ int batch_occupancy(int real_bytes, size_t smem) {
 }
 
 size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
+  if (A.fast == 2 && mr_batch_supported(A.m, real_bytes)) return mr_batch_smem(A.m);
   const size_t cbytes = 2 * (size_t)real_bytes;
   size_t off = ((size_t)(A.n_in + A.n_out) * 12 + 15) & ~size_t(15);
   off += (size_t)((A.m + 1) & ~1) * cbytes;

@@ -87,6 +87,11 @@ bool mr_supported(int m, int real_bytes);
 cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int mr_lines(int m, int kind, int real_bytes);
 int mr_occupancy(int m, int real_bytes);
+// mixed-radix tile code inside the persistent batch kernel (f32, lengths of
+// kBatchMrLengths): support, lines per tile and shared memory per CTA
+bool mr_batch_supported(int m, int real_bytes);
+int mr_batch_lines(int m, int kind);
+size_t mr_batch_smem(int m);
 size_t pass_smem_bytes(const PassArgs& A, int real_bytes);
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_remap(const RemapArgs& A, cudaStream_t stream);

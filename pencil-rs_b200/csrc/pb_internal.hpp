@@ -113,6 +113,7 @@ struct PassArgs {
   const int2* ktab;       // per output index k: (piece, local index along the transform axis)
   int npieces;
   int grid_ctas;          // persistent grid size
+  int batch_chunk;        // batch kernel: tiles per work item
 };
 
 // Per-tile addresses (element offsets into the concatenated rank buffers).

@@ -303,7 +303,8 @@ struct pb_plan {
   size_t buf_bytes = 0;
   size_t status_off = 0, acc_off = 0, ws_bytes = 0;
   int max_smem = 227 * 1024;
-  bool force_generic = false;                // batch building: generic pass kernel only
+  bool force_generic = false;                // batch building: no standalone register kernels
+  bool batch_mr = false;                     // batch building: mixed-radix tiles where the batch kernel has them
   std::map<std::string, int> tuned_lines;    // batch building: autotuned lines per tile by pass shape
   pb::DevPencil spectral_pen{};              // FORWARD output layout (spectral multipliers)
   ~pb_plan() {
@@ -773,7 +774,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
     A.ktab = reinterpret_cast<const int2*>(enc(P.host.add(kt.data(), kt.size() * sizeof(int2))));
   }
   A.npieces = npieces;
-  if (A.fast) {
+  if (A.fast && !P.force_generic) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int occ = A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
@@ -873,6 +874,20 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.fast = 2;
       A.dst_k_contig = direct ? 1 : 0;
       L = mr_lines(A.m, op.kind, P.real_bytes);
+      A.lines = L;
+    }
+  }
+  // inside the persistent batch kernel: its mixed-radix tiles (f32, 7-smooth
+  // lengths up to 256), same layout conditions
+  if (!A.fast && P.force_generic && P.batch_mr && (op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) &&
+      mr_batch_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    if (direct || transposed) {
+      A.fast = 2;
+      A.dst_k_contig = direct ? 1 : 0;
+      L = mr_batch_lines(A.m, op.kind);
       A.lines = L;
     }
   }
@@ -2299,6 +2314,7 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
   pb_plan& T = *B->tables;
   T.real_bytes = B->real_bytes;
   T.force_generic = true;
+  T.batch_mr = B->real_bytes == 4;
   int dev = 0, sms = 148;
   cuda_ok(cudaGetDevice(&dev));
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2366,6 +2382,15 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
   }
   size_t maxlev = 0;
   for (auto& c : chain) maxlev = std::max(maxlev, c.size());
+  // work items are chunks of up to 32 consecutive tiles of one pass, as long
+  // as every level still has at least 4 items per resident CTA (2 per SM)
+  std::vector<int> level_chunk(maxlev, 1);
+  for (size_t lev = 0; lev < maxlev; ++lev) {
+    long long tiles = 0;
+    for (int i = 0; i < count; ++i)
+      if (lev < chain[i].size()) tiles += chain[i][lev].pa.ntiles;
+    level_chunk[lev] = (int)std::max(1LL, std::min(32LL, tiles / (4LL * 2 * sms)));
+  }
   std::vector<std::vector<int>> index(count);
   B->item_start.push_back(0);
   for (size_t lev = 0; lev < maxlev; ++lev)
@@ -2373,9 +2398,11 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
       if (lev >= chain[i].size()) continue;
       const int id = (int)B->descs.size();
       B->descs.push_back(chain[i][lev]);
+      PassArgs& pa = B->descs.back().pa;
+      pa.batch_chunk = level_chunk[lev];
       B->dep.push_back(lev == 0 ? -1 : index[i].back());
       index[i].push_back(id);
-      B->item_start.push_back(B->item_start.back() + B->descs.back().pa.ntiles);
+      B->item_start.push_back(B->item_start.back() + (pa.ntiles + pa.batch_chunk - 1) / pa.batch_chunk);
     }
   // control words after the workspaces: head (8 B), error (4 B), done[ndesc]
   B->ctrl_off = (ws + 255) & ~size_t(255);
