@@ -389,18 +389,51 @@ __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, 
     return;
   }
   constexpr int PAIRS = (NSEQ + 1) / 2;  // C2C: line pairs per k
-  const int total = (kind == P_R2C) ? NSEQ * H : PAIRS * N;
-  const int per_k = (kind == P_R2C) ? NSEQ : PAIRS;
   C* __restrict__ out = reinterpret_cast<C*>(A.out);
-  for (int i = tid; i < total; i += MR_THREADS) {
-    const int p = i % per_k, k = i / per_k;
+  // destination in 8-byte units: element o of an f32 complex buffer is
+  // 16-byte aligned when a8 + o is even (buffers are 8-byte aligned)
+  const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
+  if (kind == P_C2C) {
+    // pairs aligned to 16 bytes in the destination: (2p, 2p+1) on an even
+    // row base, (2p-1, 2p) on an odd one, where lane p = 0 stores the two
+    // unpaired ends 0 and 2*PAIRS-1 of the row
+    for (int i = tid; i < PAIRS * N; i += MR_THREADS) {
+      const int p = i % PAIRS, k = i / PAIRS;
+      const long long base = Atab[k];
+      const int j0 = 2 * p - (sizeof(R) == 4 ? (int)((a8 + base) & 1) : 0);
+      if (j0 >= 0) {
+        if (j0 >= L) continue;
+        const C v0 = scl(res[j0 * SEQ + G::pad(k)], sc);
+        if (j0 + 1 < L) {
+          const C v1 = scl(res[(j0 + 1) * SEQ + G::pad(k)], sc);
+          if (sizeof(R) == 4) {
+            float4 w;
+            w.x = (float)v0.x;
+            w.y = (float)v0.y;
+            w.z = (float)v1.x;
+            w.w = (float)v1.y;
+            *reinterpret_cast<float4*>(out + base + j0) = w;
+          } else {
+            out[base + j0] = v0;
+            out[base + j0 + 1] = v1;
+          }
+        } else {
+          out[base + j0] = v0;
+        }
+      } else {
+        out[base] = scl(res[G::pad(k)], sc);
+        constexpr int JE = 2 * PAIRS - 1;
+        if (JE < L) out[base + JE] = scl(res[JE * SEQ + G::pad(k)], sc);
+      }
+    }
+    return;
+  }
+  for (int i = tid; i < NSEQ * H; i += MR_THREADS) {
+    const int p = i % NSEQ, k = i / NSEQ;
     const int j = 2 * p;
     if (j >= L) continue;
     C v0, v1;
-    if (kind == P_C2C) {
-      v0 = scl(res[j * SEQ + G::pad(k)], sc);
-      v1 = (j + 1 < L) ? scl(res[(j + 1) * SEQ + G::pad(k)], sc) : v0;
-    } else {
+    {
       const C* seq = res + p * SEQ;
       const C a = seq[G::pad(k)];
       const C b = seq[G::pad(k == 0 ? 0 : N - k)];
@@ -411,7 +444,7 @@ __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, 
     }
     const long long o = Atab[k] + j;
     if (j + 1 < L) {
-      if (sizeof(R) == 4 && (o & 1) == 0) {
+      if (sizeof(R) == 4 && ((a8 + o) & 1) == 0) {
         float4 w;
         w.x = (float)v0.x;
         w.y = (float)v0.y;

@@ -1325,6 +1325,14 @@ static void* slot_ptr(const pb_plan& P, int slot, const void* in, void* out, voi
   return static_cast<unsigned char*>(ws) + (size_t)slot * P.buf_bytes;
 }
 
+// A buffer must be aligned to the elements it holds (2 * real bytes for
+// complex data): the kernels issue element-sized and wider vector accesses,
+// and a misaligned one faults the device, so this is a preflight error.
+static void check_aligned(const void* p, bool complex_data, int real_bytes) {
+  const uintptr_t a = (uintptr_t)(complex_data ? 2 * real_bytes : real_bytes);
+  if (p != nullptr && reinterpret_cast<uintptr_t>(p) % a != 0) fail(PB_EINVALID_ARGUMENT);
+}
+
 static int run(pb_plan* P, int op, const void* in, void* out, void* ws, cudaStream_t s, float* ms, int cap,
                int* count) {
   const int mode = user_mode(*P, op);
@@ -1332,6 +1340,15 @@ static int run(pb_plan* P, int op, const void* in, void* out, void* ws, cudaStre
   if ((!in || !out) && P->extra > 0) fail(PB_ENULL);
   const bool needs_ws = prog.steps.size() > 1 || prog.has_stats;
   if (needs_ws && !ws) fail(PB_ENULL);
+  if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) fail(PB_EINVALID_ARGUMENT);
+  for (const Step& st : prog.steps) {
+    if (st.type == 0) {
+      check_aligned(slot_ptr(*P, st.src_slot, in, out, ws), st.pa.in_complex != 0, P->real_bytes);
+      check_aligned(slot_ptr(*P, st.dst_slot, in, out, ws), st.pa.out_complex != 0, P->real_bytes);
+    } else {
+      check_aligned(slot_ptr(*P, st.src_slot, in, out, ws), true, P->real_bytes);
+    }
+  }
   int* status = ws ? reinterpret_cast<int*>(static_cast<unsigned char*>(ws) + P->status_off) : nullptr;
   if (prog.has_stats) cuda_ok(cudaMemsetAsync(status, 0, P->ws_bytes - P->status_off, s));
   std::vector<cudaEvent_t> ev;
@@ -2452,6 +2469,11 @@ static int batch_execute(pb_batch* B, void* const* buffers, void* ws, cudaStream
   now.back() = ws;
   const bool rebind = now != B->bound;
   if (rebind) {
+    if (reinterpret_cast<uintptr_t>(ws) % 256 != 0) fail(PB_EINVALID_ARGUMENT);
+    for (const auto& d : B->descs) {
+      check_aligned(batch_slot(*B, d.plan, d.src_slot, buffers, ws), d.pa.in_complex != 0, B->real_bytes);
+      check_aligned(batch_slot(*B, d.plan, d.dst_slot, buffers, ws), d.pa.out_complex != 0, B->real_bytes);
+    }
     cuda_ok(cudaStreamSynchronize(s));  // the previous upload from the pinned staging has finished
     for (size_t d = 0; d < B->descs.size(); ++d) {
       PassArgs a = B->descs[d].pa;

@@ -329,19 +329,53 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
         // where the destination address allows it
         constexpr int PAIRS = LMAX >= 2 ? LMAX / 2 : 1;
         constexpr int TOTAL = PAIRS * NOUT;
-        if (KIND == P_C2C || KIND == P_R2C) {
+        // destination in 8-byte units: element o of an f32 complex buffer is
+        // 16-byte aligned when a8 + o is even (buffers are 8-byte aligned)
+        const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
+        if (KIND == P_C2C) {
+          // the pairs are aligned to 16 bytes in the destination: (2p, 2p+1)
+          // on an even row base, (2p-1, 2p) on an odd one, where lane p = 0
+          // stores the two unpaired ends 0 and 2*PAIRS-1 of the row
           C* __restrict__ out = reinterpret_cast<C*>(A.out);
-          const bool weighted = KIND == P_R2C && A.post_mode == W_HALF_INTERIOR;
+          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
+            const int p = idx & (PAIRS - 1);
+            const int k = idx / PAIRS;
+            const long long base = Atab[k];
+            const int j0 = 2 * p - (sizeof(R) == 4 ? (int)((a8 + base) & 1) : 0);
+            if (j0 >= 0) {
+              if (j0 >= L) continue;
+              const C v0 = scl(sm[j0 * SEQ + G::pad(k)], sc);
+              if (j0 + 1 < L) {  // row j0 + 1 exists only when the tile holds that line
+                const C v1 = scl(sm[(j0 + 1) * SEQ + G::pad(k)], sc);
+                if (sizeof(R) == 4) {
+                  float4 w;
+                  w.x = (float)v0.x;
+                  w.y = (float)v0.y;
+                  w.z = (float)v1.x;
+                  w.w = (float)v1.y;
+                  *reinterpret_cast<float4*>(out + base + j0) = w;
+                } else {
+                  out[base + j0] = v0;
+                  out[base + j0 + 1] = v1;
+                }
+              } else {
+                out[base + j0] = v0;
+              }
+            } else {
+              out[base] = scl(sm[G::pad(k)], sc);
+              constexpr int JE = 2 * PAIRS - 1;
+              if (JE < L) out[base + JE] = scl(sm[JE * SEQ + G::pad(k)], sc);
+            }
+          }
+        } else if (KIND == P_R2C) {
+          C* __restrict__ out = reinterpret_cast<C*>(A.out);
+          const bool weighted = A.post_mode == W_HALF_INTERIOR;
           for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
             const int j = 2 * (idx & (PAIRS - 1));
             const int k = idx / PAIRS;
             if (j >= L) continue;
             C v0, v1;
-            if (KIND == P_C2C) {
-              // row j + 1 exists only when the tile holds that line (j + 1 < L <= NSEQ)
-              v0 = scl(sm[j * SEQ + G::pad(k)], sc);
-              v1 = (j + 1 < L) ? scl(sm[(j + 1) * SEQ + G::pad(k)], sc) : v0;
-            } else {
+            {
               const C* seq = sm + (j >> 1) * SEQ;
               const C a = seq[G::pad(k)];
               const C b = seq[G::pad((N - k) & (N - 1))];
@@ -352,7 +386,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
             }
             const long long o = Atab[k] + j;
             if (j + 1 < L) {
-              if (sizeof(R) == 4 && (o & 1) == 0) {
+              if (sizeof(R) == 4 && ((a8 + o) & 1) == 0) {
                 float4 w;
                 w.x = (float)v0.x;
                 w.y = (float)v0.y;

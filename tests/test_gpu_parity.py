@@ -451,3 +451,45 @@ def test_pow2_vjp_adjoint_identity_f64(family):
         lhs = _dot(to_host(ax), to_host(y))
         rhs = _dot(to_host(x), to_host(aty))
         assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (op, lhs, rhs)
+
+
+def test_misaligned_buffers_are_rejected_before_any_launch():
+    """A complex buffer not aligned to its element (8 B in f32) is a preflight
+    error: the kernels' vector accesses would fault on it."""
+    import ctypes as C
+    from pencil_b200 import _lib as L
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology((2, 2)), (16, 32, 64), (), dtype=torch.complex64)
+    n = plan.info.input_elems
+    raw = torch.zeros(2 * n + 8, dtype=torch.float32, device="cuda")  # float storage, 4-byte steps
+    dst = plan.allocate_output()
+    ws = plan.allocate_workspace()
+    lib = L.load()
+    bad = C.c_void_p(raw.data_ptr() + 4)
+    rc = lib.pb_execute(plan._h, L.FORWARD, bad, C.c_void_p(dst.data_ptr()), C.c_void_p(ws.data_ptr()), None)
+    assert L.STATUS_NAMES[rc] == "InvalidArgument"
+    rc = lib.pb_execute(plan._h, L.FORWARD, C.c_void_p(raw.data_ptr()), C.c_void_p(dst.data_ptr() + 4),
+                        C.c_void_p(ws.data_ptr()), None)
+    assert L.STATUS_NAMES[rc] == "InvalidArgument"
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(dst) == 0  # nothing ran
+
+
+@pytest.mark.parametrize("shape,dims", [((64, 128, 256), (2, 3)), ((48, 40, 36), (2, 2)), ((64, 96, 128), (4, 2))])
+def test_outputs_only_8_byte_aligned_match_aligned_outputs(shape, dims):
+    """Transposed C2C stores write 16-byte pairs aligned to the actual address;
+    an output that starts 8 bytes past a 16-byte boundary gives the same bits."""
+    torch.manual_seed(5)
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), dtype=torch.complex64)
+    x = torch.randn(plan.info.input_elems, dtype=torch.complex64, device="cuda")
+    ref = plan.allocate_output()
+    plan.forward(x, ref)
+    shifted = torch.zeros(plan.info.output_elems + 1, dtype=torch.complex64, device="cuda")[1:]
+    assert shifted.data_ptr() % 16 == 8
+    plan.forward(x, shifted)
+    back_ref, back = plan.allocate_input(), torch.zeros(plan.info.input_elems + 1, dtype=torch.complex64,
+                                                          device="cuda")[1:]
+    plan.inverse(ref, back_ref)
+    plan.inverse(ref, back)
+    torch.cuda.synchronize()
+    assert torch.equal(shifted, ref)
+    assert torch.equal(back, back_ref)
