@@ -5,6 +5,7 @@
 
 #include "pb_aux.hpp"
 #include "pb_device.cuh"
+#include "pb_fft.cuh"
 
 namespace pb {
 
@@ -147,15 +148,17 @@ __device__ __forceinline__ bool plane_point(const StatsArgs& A, long long group,
   const long long s_red = inf[2 + red], ext_red = inf[2 + 2 * p.N + red];
   if (kp < s_red || kp >= s_red + ext_red) return false;
   long long off = inf[0] + e * inf[1] + (kp - s_red) * inf[2 + p.N + red];
-  long long rest = i;
+  // a rank's plane holds fewer than 2^32 points (launch_stats checks it), so
+  // the coordinate split runs in 32-bit arithmetic
+  unsigned rest = (unsigned)i;
   for (int q = p.N - 1; q >= 0; --q) {
     const int ax = p.perm[q];
     if (ax == red) continue;
-    const long long ext = inf[2 + 2 * p.N + ax];
+    const unsigned ext = (unsigned)inf[2 + 2 * p.N + ax];
     if (ext == 0) return false;
-    const long long c = rest % ext;
-    rest /= ext;
-    off += c * inf[2 + p.N + ax];
+    const unsigned quo = rest / ext;
+    off += (long long)(rest - quo * ext) * inf[2 + p.N + ax];
+    rest = quo;
   }
   if (rest != 0) return false;  // beyond this rank's plane
   const R* d = reinterpret_cast<const R*>(A.data);
@@ -227,6 +230,7 @@ __global__ void __launch_bounds__(256) stats_kernel(const StatsArgs A) {
     scale = acc[0];
     scaled = scale != 0.0 && isfinite(scale);
   }
+#pragma unroll 4
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.max_points;
        i += (long long)gridDim.x * blockDim.x) {
     double re, im;
@@ -280,9 +284,11 @@ static unsigned grid_for(long long total, int threads, long long cap = 148LL * 1
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream) {
   const long long groups = A.extra * A.nplanes * A.pen.nranks;
   if (groups <= 0 || A.max_points <= 0) return cudaSuccess;
-  if (groups > 65535) return cudaErrorInvalidValue;
+  if (groups > 65535 || A.max_points >= (1LL << 32)) return cudaErrorInvalidValue;
   const int threads = 256;
-  const unsigned bx = grid_for(A.max_points, threads, 64);
+  // few blocks per rank plane: every block ends with contended atomics on the
+  // plane's accumulators and on the finishing counter
+  const unsigned bx = grid_for(A.max_points, threads, 8);
   const dim3 grid(bx, (unsigned)groups);
   if (real_bytes == 4) {
     stats_kernel<float, 0><<<grid, threads, 0, stream>>>(A);
@@ -321,48 +327,82 @@ namespace pb {
 // g if g <= n/2 else g - n; the R2C-reduced axis holds k = 0..n/2).
 //   MULT_K2      m = |k|^2
 //   MULT_POISSON m = -1/|k|^2, m(0) = 0 (spectral Poisson solve)
+// One warp per memory row (a run of the innermost memory axis of one rank and
+// extra index): the row's outer coordinates and their |k|^2 are computed once
+// per row in 32-bit arithmetic, the lanes stride along the row.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ long long wave_index(long long g, int n, bool half) {
+  return (!half && g > n / 2) ? g - n : g;
+}
+
 template <typename R>
-__global__ void spectral_kernel(const SpectralArgs A) {
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < A.total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const DevPencil& d = A.pen;
-    const int r = rank_of_offset(d, idx);
-    const long long* inf = d.info + (long long)r * info_words(d.N);
-    const long long local = idx - inf[0];
-    const long long len = inf[1];
-    const long long e = local / len;
-    long long pos = local - e * len;
-    double k2 = 0.0;
-    for (int q = d.N - 1; q >= 0; --q) {
-      const int ax = d.perm[q];
-      const long long ext = inf[2 + 2 * d.N + ax];
-      const long long c = pos % ext;
-      pos /= ext;
-      const long long g = inf[2 + ax] + c;
-      long long k = g;
-      if (ax != A.half_axis && g > d.shape[ax] / 2) k = g - d.shape[ax];
-      k2 += (double)(k * k);
+__global__ void __launch_bounds__(256) spectral_kernel(const SpectralArgs A) {
+  using C = typename Cx<R>::T;
+  const DevPencil& d = A.pen;
+  const int r = blockIdx.y;
+  const long long* inf = d.info + (long long)r * info_words(d.N);
+  const long long len = inf[1];
+  if (len == 0) return;
+  const int N = d.N;
+  const int inner = d.perm[N - 1];
+  const unsigned ext_in = (unsigned)inf[2 + 2 * N + inner];
+  if (ext_in == 0) return;
+  const unsigned rows_per_e = (unsigned)(len / ext_in);
+  const unsigned lane = threadIdx.x & 31;
+  const long long row = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const long long nrows = (long long)rows_per_e * A.extra;
+  if (row >= nrows) return;
+  const unsigned e = (unsigned)(row / rows_per_e);
+  unsigned rest = (unsigned)(row - (long long)e * rows_per_e);
+  double k2_outer = 0.0;
+  for (int q = N - 2; q >= 0; --q) {
+    const int ax = d.perm[q];
+    const unsigned ext = (unsigned)inf[2 + 2 * N + ax];
+    const unsigned quo = rest / ext;
+    const long long g = inf[2 + ax] + (rest - quo * ext);
+    rest = quo;
+    const long long k = wave_index(g, d.shape[ax], ax == A.half_axis);
+    k2_outer += (double)(k * k);
+  }
+  const long long start_in = inf[2 + inner];
+  const bool half_in = inner == A.half_axis;
+  const long long first = inf[0] + (long long)e * len + (row - (long long)e * rows_per_e) * ext_in;
+  const C* __restrict__ in = reinterpret_cast<const C*>(A.in) + first;
+  C* __restrict__ out = reinterpret_cast<C*>(A.out) + first;
+  const R sc = (R)A.scale;
+  // |k|^2 is an integer below 2^24 here, exact in either precision; the
+  // multiplier is formed in the data's precision
+  if (A.mode == 0) {
+    for (unsigned c = lane; c < ext_in; c += 32) {
+      const long long k = wave_index(start_in + c, d.shape[inner], half_in);
+      const R f = (R)(k2_outer + (double)(k * k)) * sc;
+      const C v = in[c];
+      out[c] = mk<C, R>(v.x * f, v.y * f);
     }
-    double mult;
-    if (A.mode == 0)
-      mult = k2;
-    else
-      mult = (k2 == 0.0) ? 0.0 : -1.0 / k2;
-    const R f = (R)(mult * A.scale);
-    const R* in = reinterpret_cast<const R*>(A.in);
-    R* out = reinterpret_cast<R*>(A.out);
-    out[2 * idx] = in[2 * idx] * f;
-    out[2 * idx + 1] = in[2 * idx + 1] * f;
+  } else {
+    for (unsigned c = lane; c < ext_in; c += 32) {
+      const long long k = wave_index(start_in + c, d.shape[inner], half_in);
+      const R k2 = (R)(k2_outer + (double)(k * k));
+      R inv_k2;
+      if constexpr (sizeof(R) == 4)
+        inv_k2 = __frcp_rn(k2);  // correctly rounded 1/k2
+      else
+        inv_k2 = R(1) / k2;
+      const R f = (k2 == R(0)) ? R(0) : -inv_k2 * sc;
+      const C v = in[c];
+      out[c] = mk<C, R>(v.x * f, v.y * f);
+    }
   }
 }
 
 cudaError_t launch_spectral(const SpectralArgs& A, int real_bytes, cudaStream_t stream) {
-  if (A.total <= 0) return cudaSuccess;
+  if (A.total <= 0 || A.max_rows <= 0) return cudaSuccess;
+  if (A.pen.nranks > 65535 || (A.max_rows + 7) / 8 > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)((A.max_rows + 7) / 8), (unsigned)A.pen.nranks);
   if (real_bytes == 4)
-    spectral_kernel<float><<<grid_for(A.total, 256, 148LL * 32), 256, 0, stream>>>(A);
+    spectral_kernel<float><<<grid, 256, 0, stream>>>(A);
   else
-    spectral_kernel<double><<<grid_for(A.total, 256, 148LL * 32), 256, 0, stream>>>(A);
+    spectral_kernel<double><<<grid, 256, 0, stream>>>(A);
   return cudaGetLastError();
 }
 

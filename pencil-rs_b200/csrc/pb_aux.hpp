@@ -73,6 +73,8 @@ struct SpectralArgs {
   int half_axis;    // R2C-reduced axis (k = index), or -1
   int mode;         // 0: |k|^2, 1: -1/|k|^2 with 0 at k = 0
   double scale;
+  long long extra;     // product of the extra dims
+  long long max_rows;  // largest number of memory rows (innermost-axis runs) of one rank, all extras
 };
 
 cudaError_t launch_spectral(const SpectralArgs& A, int real_bytes, cudaStream_t stream);

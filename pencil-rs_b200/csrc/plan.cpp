@@ -1668,8 +1668,22 @@ int pb_spectral_multiply(const pb_plan* plan, int32_t mode, double scale, const 
     const long long total = P.fout.total(P.extra);
     if (total == 0) return (int)PB_OK;
     if (!in || !out) return (int)PB_ENULL;
+    check_aligned(in, true, P.real_bytes);
+    check_aligned(out, true, P.real_bytes);
     SpectralArgs A{};
     A.pen = P.spectral_pen;
+    A.extra = P.extra;
+    {
+      const int inner = P.fout.perm[P.fout.N - 1];
+      long long mx = 0;
+      for (int r = 0; r < P.fout.nranks(); ++r) {
+        long long lo[MAXN], ext[MAXN];
+        P.fout.local(r, lo, ext);
+        if (ext[inner] == 0) continue;
+        mx = std::max(mx, P.extra * (P.fout.local_len(r) / ext[inner]));
+      }
+      A.max_rows = mx;
+    }
     A.in = in;
     A.out = out;
     A.total = total;
