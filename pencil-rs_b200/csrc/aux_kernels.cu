@@ -9,6 +9,8 @@
 
 namespace pb {
 
+static unsigned grid_for(long long total, int threads, long long cap);
+
 // ---------------------------------------------------------------------------
 // element copy of `bytes` bytes (4, 8, 16 on the fast paths)
 // ---------------------------------------------------------------------------
@@ -61,6 +63,48 @@ __global__ void remap_kernel(const RemapArgs A) {
     copy_elem(reinterpret_cast<const unsigned char*>(A.in), reinterpret_cast<unsigned char*>(A.out), so, idx,
               A.elem_bytes);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled permute copy (transposes between pencil layouts, affine remap): a
+// 32x32 tile is read along the source's contiguous axis, transposed in shared
+// memory and written along the destination's contiguous axis; each warp moves
+// one 32-element run per step, so both sides are coalesced.  Row tiles (the
+// same contiguous axis in both layouts) are straight runs.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) xpose_kernel(const XposeArgs A) {
+  __shared__ T tile[XT][XT + 1];
+  const T* __restrict__ in = reinterpret_cast<const T*>(A.in);
+  T* __restrict__ out = reinterpret_cast<T*>(A.out);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+    const XTile X = A.tiles[t];
+    if (A.row) {
+      for (int i = threadIdx.x; i < X.ns; i += blockDim.x)
+        out[X.dst0 + (long long)i * X.dst_ss] = in[X.src0 + (long long)i * X.src_ss];
+      continue;
+    }
+    if (lane < X.ns)
+      for (int id = warp; id < X.nd; id += 8) tile[id][lane] = in[X.src0 + (long long)lane * X.src_ss + (long long)id * X.src_sd];
+    __syncthreads();
+    if (lane < X.nd)
+      for (int is = warp; is < X.ns; is += 8)
+        out[X.dst0 + (long long)is * X.dst_ss + (long long)lane * X.dst_sd] = tile[lane][is];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_xpose(const XposeArgs& A, cudaStream_t stream) {
+  if (A.ntiles <= 0) return cudaSuccess;
+  const unsigned grid = grid_for(A.ntiles, 1, 148LL * 16);
+  switch (A.elem_bytes) {
+    case 4: xpose_kernel<unsigned int><<<grid, 256, 0, stream>>>(A); break;
+    case 8: xpose_kernel<uint2><<<grid, 256, 0, stream>>>(A); break;
+    case 16: xpose_kernel<uint4><<<grid, 256, 0, stream>>>(A); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -274,7 +318,7 @@ __global__ void __launch_bounds__(256) stats_kernel(const StatsArgs A) {
   }
 }
 
-static unsigned grid_for(long long total, int threads, long long cap = 148LL * 16) {
+static unsigned grid_for(long long total, int threads, long long cap) {
   long long b = (total + threads - 1) / threads;
   if (b < 1) b = 1;
   if (b > cap) b = cap;

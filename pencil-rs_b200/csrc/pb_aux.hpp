@@ -77,6 +77,30 @@ struct SpectralArgs {
   long long max_rows;  // largest number of memory rows (innermost-axis runs) of one rank, all extras
 };
 
+// One tile of a permute copy (layout-changing transposes and the affine
+// remap): element (is, id), is < ns, id < nd, moves from
+// src0 + is*src_ss + id*src_sd to dst0 + is*dst_ss + id*dst_sd.  A tile lies
+// inside one source rank, one destination rank and one wrap segment of the
+// remap, so these offsets are affine.  row = 1: a single run (nd = 1) of up to
+// XROW elements along an axis contiguous in both layouts.
+struct XTile {
+  long long src0, dst0;
+  int src_ss, src_sd, dst_ss, dst_sd;
+  int ns, nd;
+};
+constexpr int XT = 32;      // tile edge (elements)
+constexpr int XROW = 1024;  // run length of a row tile
+
+struct XposeArgs {
+  const XTile* tiles;
+  long long ntiles;
+  const void* in;
+  void* out;
+  int elem_bytes;  // 4, 8 or 16
+  int row;         // 1: row tiles (the innermost axis is the same in both layouts)
+};
+
+cudaError_t launch_xpose(const XposeArgs& A, cudaStream_t stream);
 cudaError_t launch_spectral(const SpectralArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream);
 cudaError_t launch_batch(const BatchArgs& B, int real_bytes, size_t smem, int grid, cudaStream_t stream);

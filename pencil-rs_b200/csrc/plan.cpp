@@ -429,6 +429,94 @@ struct HostLayout {
   }
 };
 
+// Tiles of the permute copy dst[x] = src[s(x)], s_a(x) = (sign_a*x_a + off_a)
+// mod n_a, from layout S to layout D (identity signs and offsets: a transpose).
+// Along every axis the destination coordinates are cut where the destination
+// rank changes, where s crosses a source rank boundary and where s wraps, so
+// inside a tile both addresses are affine in the tile coordinates.  Tiles span
+// the source's contiguous axis (is) and the destination's (id), XT x XT
+// elements, or runs of up to XROW elements when the two coincide.
+static std::vector<XTile> build_xtiles(const Pencil& S, const Pencil& D, long long extra, const int* sign,
+                                       const long long* off, int* row_out) {
+  const int N = D.N;
+  HostLayout hs(S, extra), hd(D, extra);
+  std::vector<long long> cuts[MAXN];
+  for (int a = 0; a < N; ++a) {
+    const long long n = D.shape[a];
+    std::vector<long long> c{0, n};
+    const int td = D.split_of(a);
+    if (td >= 0)
+      for (int q = 1; q < D.grid[td]; ++q) c.push_back(Pencil::part(n, D.grid[td], q));
+    std::vector<long long> sb{0};  // source segment starts, 0 = the wrap
+    const int ts = S.split_of(a);
+    if (ts >= 0)
+      for (int q = 1; q < S.grid[ts]; ++q) sb.push_back(Pencil::part(n, S.grid[ts], q));
+    for (long long b : sb) {
+      // x where s(x) enters the segment starting (sign +1) or leaves the one
+      // ending (sign -1) at source index b
+      long long x = sign[a] > 0 ? (b - off[a]) % n : (off[a] - b + 1) % n;
+      if (x < 0) x += n;
+      c.push_back(x);
+    }
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    cuts[a] = c;
+  }
+  const int as = S.perm[N - 1], ad = D.perm[N - 1];
+  const bool row = as == ad;
+  if (row_out) *row_out = row ? 1 : 0;
+  // chunks along the tile axes: segments of the cuts, split into XT (or XROW)
+  auto chunks = [&](int a, long long edge) {
+    std::vector<std::pair<long long, int>> v;
+    for (size_t i = 0; i + 1 < cuts[a].size(); ++i)
+      for (long long x = cuts[a][i]; x < cuts[a][i + 1]; x += edge)
+        v.push_back({x, (int)std::min<long long>(edge, cuts[a][i + 1] - x)});
+    return v;
+  };
+  const auto cs = chunks(as, row ? XROW : XT);
+  const auto cd = row ? std::vector<std::pair<long long, int>>{{0, 1}} : chunks(ad, XT);
+  std::vector<int> outer;
+  for (int a = 0; a < N; ++a)
+    if (a != as && a != ad) outer.push_back(a);
+  long long nouter = 1;
+  for (int a : outer) nouter *= D.shape[a];
+  std::vector<XTile> tiles;
+  tiles.reserve((size_t)(extra * nouter * (long long)cs.size() * (long long)cd.size()));
+  long long x[MAXN] = {}, sx[MAXN] = {};
+  for (long long e = 0; e < extra; ++e)
+    for (long long o = 0; o < nouter; ++o) {
+      long long rem = o;
+      for (int i = (int)outer.size() - 1; i >= 0; --i) {
+        x[outer[i]] = rem % D.shape[outer[i]];
+        rem /= D.shape[outer[i]];
+      }
+      for (const auto& c1 : cs)
+        for (const auto& c2 : cd) {
+          x[as] = c1.first;
+          if (!row) x[ad] = c2.first;
+          for (int a = 0; a < N; ++a) {
+            long long v = (sign[a] > 0 ? x[a] : -x[a]) + off[a];
+            v %= D.shape[a];
+            if (v < 0) v += D.shape[a];
+            sx[a] = v;
+          }
+          int rs = 0, rd = 0;
+          XTile t;
+          t.src0 = hs.offset(e, sx, &rs);
+          t.dst0 = hd.offset(e, x, &rd);
+          if (hs.stride[rs][ad] > INT_MAX || hd.stride[rd][as] > INT_MAX) fail(PB_EUNSUPPORTED);
+          t.src_ss = (int)(sign[as] * hs.stride[rs][as]);
+          t.dst_ss = (int)hd.stride[rd][as];
+          t.src_sd = row ? 0 : (int)(sign[ad] * hs.stride[rs][ad]);
+          t.dst_sd = row ? 0 : (int)hd.stride[rd][ad];
+          t.ns = c1.second;
+          t.nd = c2.second;
+          tiles.push_back(t);
+        }
+    }
+  return tiles;
+}
+
 // exp(-2 pi i q/m) (negative exponent) in extended precision, rounded once.
 static size_t roots_table(pb_plan& P, int m) {
   const std::string key = "W" + std::to_string(m) + "r" + std::to_string(P.real_bytes);
@@ -1788,8 +1876,8 @@ struct pb_transpose {
   int elem_bytes = 0;
   bool alltoallv = false;
   std::unique_ptr<pb_plan> tables;  // owns the device arena
-  bool use_pass = false;
-  pb::Step pass;
+  bool use_tiles = false;  // 4/8/16-byte elements: tiled permute copy
+  pb::XposeArgs xt{};
   pb::RemapArgs gather{};
   std::vector<pb::SegDesc> send_segs, recv_segs;
   std::vector<long long> recv_off, send_off;
@@ -1803,6 +1891,8 @@ struct pb_transpose {
 struct pb_remap {
   std::unique_ptr<pb_plan> tables;
   pb::RemapArgs args{};
+  bool use_tiles = false;  // 4/8/16-byte elements: tiled permute copy
+  pb::XposeArgs xt{};
 };
 
 namespace pb {
@@ -1827,14 +1917,21 @@ static void build_copy(pb_transpose& T) {
     P.max_smem = optin;
   const int N = T.src.N;
   std::vector<Step> steps;
+  size_t tile_tab = 0;
   if (T.elem_bytes == 4 || T.elem_bytes == 8 || T.elem_bytes == 16) {
-    P.real_bytes = (T.elem_bytes == 16) ? 8 : 4;
-    const bool cplx = T.elem_bytes != 4;
-    Stage id;
-    id.axis = T.src.perm[N - 1];
-    LocalOp op;
-    steps.push_back(make_pass(P, id, op, T.src, T.dst, cplx, cplx));
-    T.use_pass = true;
+    int sign[MAXN];
+    long long off[MAXN];
+    for (int x = 0; x < N; ++x) {
+      sign[x] = 1;
+      off[x] = 0;
+    }
+    int row = 0;
+    const std::vector<XTile> tiles = build_xtiles(T.src, T.dst, T.extra, sign, off, &row);
+    tile_tab = P.host.add(tiles.data(), tiles.size() * sizeof(XTile));
+    T.xt.ntiles = (long long)tiles.size();
+    T.xt.elem_bytes = T.elem_bytes;
+    T.xt.row = row;
+    T.use_tiles = true;
   }
   RemapArgs& G = T.gather;
   G.src = dev_pencil(P, P.host, P.cache, T.src, T.extra);
@@ -1854,7 +1951,7 @@ static void build_copy(pb_transpose& T) {
     soff_tab = P.host.add(T.send_off.data(), T.send_off.size() * sizeof(long long));
   }
   upload_steps(P, steps);
-  if (T.use_pass) T.pass = steps[0];
+  if (T.use_tiles) T.xt.tiles = reinterpret_cast<const XTile*>(fix_ptr(P, enc(tile_tab)));
   auto fixpen = [&](DevPencil& d) { d.info = reinterpret_cast<const long long*>(fix_ptr(P, d.info)); };
   fixpen(G.src);
   fixpen(G.dst);
@@ -2033,12 +2130,13 @@ int pb_transpose_execute(pb_transpose* plan, const void* src, void* dst, void* s
     if (plan->extra == 0) return (int)PB_OK;
     if (!src || !dst) return (int)PB_ENULL;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (plan->use_pass) {
-      PassArgs A = plan->pass.pa;
-      A.in = src;
-      A.out = dst;
-      A.gate = nullptr;
-      cuda_ok(launch_pass(A, plan->tables->real_bytes, s));
+    if (plan->use_tiles) {
+      check_aligned(src, false, plan->elem_bytes);
+      check_aligned(dst, false, plan->elem_bytes);
+      XposeArgs X = plan->xt;
+      X.in = src;
+      X.out = dst;
+      cuda_ok(launch_xpose(X, s));
     } else {
       RemapArgs G = plan->gather;
       G.in = src;
@@ -2137,10 +2235,23 @@ int pb_remap_create(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_
       if (o < 0) o += S.shape[x];
       G.offset[x] = o;
     }
+    size_t tile_tab = 0;
+    if ((elem_bytes == 4 || elem_bytes == 8 || elem_bytes == 16) && extra_count > 0) {
+      int sign[MAXN];
+      for (int x = 0; x < S.N; ++x) sign[x] = signs[x];
+      int row = 0;
+      const std::vector<XTile> tiles = build_xtiles(S, D, extra_count, sign, G.offset, &row);
+      tile_tab = P.host.add(tiles.data(), tiles.size() * sizeof(XTile));
+      R->xt.ntiles = (long long)tiles.size();
+      R->xt.elem_bytes = elem_bytes;
+      R->xt.row = row;
+      R->use_tiles = true;
+    }
     std::vector<Step> none;
     upload_steps(P, none);
     G.src.info = reinterpret_cast<const long long*>(fix_ptr(P, G.src.info));
     G.dst.info = reinterpret_cast<const long long*>(fix_ptr(P, G.dst.info));
+    if (R->use_tiles) R->xt.tiles = reinterpret_cast<const XTile*>(fix_ptr(P, enc(tile_tab)));
     *plan = R.release();
     return (int)PB_OK;
   });
@@ -2151,6 +2262,15 @@ int pb_remap_apply(pb_remap* plan, const void* src, void* dst, void* stream) {
     if (!plan) return (int)PB_ENULL;
     if (plan->args.total == 0) return (int)PB_OK;
     if (!src || !dst) return (int)PB_ENULL;
+    if (plan->use_tiles) {
+      check_aligned(src, false, plan->xt.elem_bytes);
+      check_aligned(dst, false, plan->xt.elem_bytes);
+      XposeArgs X = plan->xt;
+      X.in = src;
+      X.out = dst;
+      cuda_ok(launch_xpose(X, static_cast<cudaStream_t>(stream)));
+      return (int)PB_OK;
+    }
     RemapArgs G = plan->args;
     G.in = src;
     G.out = dst;
