@@ -185,6 +185,14 @@ int pb_execute(pb_plan* plan, int32_t op, const void* in, void* out, void* works
 /* Waits for `stream` and reports the spectrum check of the last C2R-bearing
  * execution that used `workspace`: PB_OK or PB_EINVALID_SPECTRUM. */
 int pb_execute_status(pb_plan* plan, void* workspace, void* stream);
+
+/* Asynchronous form of pb_execute_status for streaming callers (no
+ * counterpart in the reference, whose check returns synchronously):
+ * enqueues on `stream` a copy of the two status words of the last execution
+ * on `workspace` (spectrum rejected, value not finite) into host memory
+ * `status` (2 x int32; pinned for an asynchronous copy).  After synchronizing
+ * the stream the caller treats any non-zero word as PB_EINVALID_SPECTRUM. */
+int pb_execute_status_async(pb_plan* plan, void* workspace, int32_t* status, void* stream);
 /* forward_with_timing & co. (distributed.rs:1545-1600, TransformTiming 290-325):
  * synchronous; stage_ms[i] = device time of kernel launch i (pass or check),
  * *count = number of launches. */

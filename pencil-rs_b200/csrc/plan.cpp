@@ -1812,6 +1812,15 @@ int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int3
   });
 }
 
+int pb_execute_status_async(pb_plan* plan, void* workspace, int32_t* status, void* stream) {
+  return guard([&] {
+    if (!plan || !workspace || !status) return (int)PB_ENULL;
+    cuda_ok(cudaMemcpyAsync(status, static_cast<unsigned char*>(workspace) + plan->status_off, 2 * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    return (int)PB_OK;
+  });
+}
+
 int pb_execute_status(pb_plan* plan, void* workspace, void* stream) {
   return guard([&] {
     if (!plan || !workspace) return (int)PB_ENULL;

@@ -76,6 +76,7 @@ SIGNATURES = {
     "pb_execute_no_alloc": ([_P, C.c_int32, _P, _P, _P], C.c_int),
     "pb_plan_steps": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "pb_plan_step_kernels": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+    "pb_execute_status_async": ([_P, _P, _P, _P], C.c_int),
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),
     "pb_spectral_multiply": ([_P, C.c_int32, C.c_double, _P, _P, _P], C.c_int),
