@@ -66,6 +66,10 @@ __host__ __device__ constexpr RadixList mr_factor(int N) {
     L.r[L.n++] = 3;
     m /= 3;
   }
+  while (m % 11 == 0) {
+    L.r[L.n++] = 11;
+    m /= 11;
+  }
   return L;
 }
 
@@ -510,7 +514,18 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
 // the k table into shared memory (the batch skips it when the CTA's previous
 // chunk belonged to the same pass).  Ends with this CTA's last store still
 // reading shared memory: the caller places a barrier before reusing it.
+// the real-to-real kinds (mr_r2r.cuh)
 template <typename R, int N>
+__device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                            const PassArgs& A, const TileAddr& ta);
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& ta,
+                                            typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                            typename Cx<R>::T* b0, typename Cx<R>::T* b1,
+                                            const typename Cx<R>::T* W, long long* Atab, const int2* ktab,
+                                            PieceAddr* prow, const PieceAddr& my_piece, int npieces);
+
+template <typename R, int N, bool R2R = false>
 __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
                                        unsigned char* smem, bool setup) {
   using C = typename Cx<R>::T;
@@ -527,7 +542,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   if (tile >= end) return;
   const int tid = threadIdx.x;
   const bool direct = A.dst_k_contig != 0;
-  const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
+  const int nout = R2R ? A.n_out : ((A.kind == P_R2C) ? N / 2 + 1 : N);
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
   const int npieces = direct ? 0 : A.npieces;
@@ -538,7 +553,10 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   }
   TileAddr ta = load_tile(tiles, tile);
   C v[G::U0][G::R0];
-  mr_load<R, N>(v, A, ta);
+  if constexpr (R2R)
+    mr_load_r2r<R, N>(v, A, ta);
+  else
+    mr_load<R, N>(v, A, ta);
   TileAddr t1 = ta;
   if (tile + step < end) t1 = load_tile(tiles, tile + step);
   PieceAddr my_piece{0, 0};
@@ -551,14 +569,24 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
     PieceAddr next_piece{0, 0};
     C nv[G::U0][G::R0];
     if (has_next) {
-      mr_load<R, N>(nv, A, t1);
+      if constexpr (R2R)
+        mr_load_r2r<R, N>(nv, A, t1);
+      else
+        mr_load<R, N>(nv, A, t1);
       if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
       if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
-    if (A.inv)
-      mr_tile<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
-    else
-      mr_tile<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    if constexpr (R2R) {
+      if (A.inv)
+        mr_tile_r2r<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+      else
+        mr_tile_r2r<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    } else {
+      if (A.inv)
+        mr_tile<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+      else
+        mr_tile<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    }
     if (!has_next) break;
     tile += step;
     ta = t1;

@@ -27,6 +27,16 @@ constexpr int kBatchMrLengths[] = {32,  35,  36,  40,  42,  45,  48,  49,  50,  
                                    192, 196, 200, 210, 216, 224, 225, 240, 243, 245, 250, 252, 256};
 constexpr int kBatchMrCount = sizeof(kBatchMrLengths) / sizeof(kBatchMrLengths[0]);
 
+// FFT lengths of the real-to-real kinds on the mixed-radix kernel
+// (mr_r2r.cuh): the mixed-radix lengths, the powers of two 32..512, and 770
+// (= 2(384 + 1), the DST-I extension of a 384-point axis; radix 11).
+constexpr int kMrR2rLengths[] = {32,  35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  60,  63,  64,  70,  72,  75,
+                                 80,  81,  84,  90,  96,  98,  100, 105, 108, 112, 120, 125, 126, 128, 135, 140, 144,
+                                 147, 150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
+                                 245, 250, 252, 256, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375,
+                                 378, 384, 392, 400, 405, 420, 432, 441, 448, 450, 480, 486, 490, 500, 504, 512, 770};
+constexpr int kMrR2rCount = sizeof(kMrR2rLengths) / sizeof(kMrR2rLengths[0]);
+
 // Entry points of one (precision, length) instantiation.
 struct MrEntry {
   cudaError_t (*launch)(const PassArgs&, cudaStream_t);
@@ -43,5 +53,14 @@ void mr_fill_group4(MrEntry* f32, MrEntry* f64);
 void mr_fill_group5(MrEntry* f32, MrEntry* f64);
 void mr_fill_group6(MrEntry* f32, MrEntry* f64);
 void mr_fill_group7(MrEntry* f32, MrEntry* f64);
+// the real-to-real tables (kMrR2rLengths), filled by mr_r2r_kernels.cu
+void mr_r2r_fill_group0(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group1(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group2(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group3(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group4(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group5(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group6(MrEntry* f32, MrEntry* f64);
+void mr_r2r_fill_group7(MrEntry* f32, MrEntry* f64);
 
 }  // namespace pb

@@ -1,0 +1,257 @@
+// Real-to-real kinds on the mixed-radix pass kernel: the DHT, DCT-II/III,
+// DST-II/III (Makhoul's n-point FFT), DCT-I (even extension, 2(n-1) points)
+// and DST-I (odd extension, 2(n+1) points), for real data (two lines per
+// complex FFT) and complex data (one line per FFT: real and imaginary parts
+// are the pair).  The kinds are the reference's FFTW REDFT/RODFT definitions
+// (crates/pencil-fft/src/r2r.rs:697-848) and the Hartley transform
+// (dht.rs:201-353), computed as in the generic pass kernel: the
+// pre-processing runs in the register-fed stage-0 load, the post-processing in
+// the store.  The type-IV kinds stay on the generic kernel.
+#pragma once
+
+#include "mr_kernel.cuh"
+
+namespace pb {
+
+// Element idx of the tile's pair s: lines (2s, 2s+1) of real data as (x, y),
+// or complex line s; the adjoint pre-weight of idx applied.
+template <typename R>
+struct R2rSource {
+  using C = typename Cx<R>::T;
+  const R* inr;
+  const C* inc;
+  long long b0, b1;
+  bool ok0, ok1, cplx;
+  int n, pre_mode;
+  R pre_f;
+  __device__ __forceinline__ C get(int idx) const {
+    const R zero = R(0);
+    C z;
+    if (cplx)
+      z = ok0 ? inc[b0 + idx] : mk<C, R>(zero, zero);
+    else
+      z = mk<C, R>(ok0 ? inr[b0 + idx] : zero, ok1 ? inr[b1 + idx] : zero);
+    if (pre_mode != W_NONE && weight_hit(pre_mode, idx, n)) z = scl(z, pre_f);
+    return z;
+  }
+};
+
+// Stage-0 butterfly inputs of one tile (FFT input q of each pair).
+template <typename R, int N>
+__device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                            const PassArgs& A, const TileAddr& ta) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NB = G::NB0;
+  constexpr int R0 = G::R0;
+  const R zero = R(0);
+  const int L = ta.lines;
+  const int n = A.n;
+  const int sub = A.sub;
+  const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
+#pragma unroll
+  for (int u = 0; u < G::U0; ++u) {
+    const int b = threadIdx.x + u * MR_THREADS;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
+    R2rSource<R> src;
+    src.cplx = A.in_complex != 0;
+    src.inr = reinterpret_cast<const R*>(A.in);
+    src.inc = reinterpret_cast<const C*>(A.in);
+    if (src.cplx) {
+      src.ok0 = live && s < L;
+      src.ok1 = false;
+      src.b0 = ta.src0 + (long long)s * ta.srcb;
+      src.b1 = 0;
+    } else {
+      src.ok0 = live && 2 * s < L;
+      src.ok1 = live && 2 * s + 1 < L;
+      src.b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
+      src.b1 = src.b0 + ta.srcb;
+    }
+    src.n = n;
+    src.pre_mode = A.pre_mode;
+    src.pre_f = R(A.pre_factor);
+#pragma unroll
+    for (int r = 0; r < R0; ++r) {
+      const int q = jb + r * NB;
+      C z;
+      switch (sub) {
+        case S_DCT2:
+        case S_DST2: {
+          const int idx = (2 * q < n) ? 2 * q : 2 * (n - 1 - q) + 1;
+          z = src.get(idx);
+          if (sub == S_DST2 && (idx & 1)) z = mk<C, R>(-z.x, -z.y);
+        } break;
+        case S_DCT3:
+        case S_DST3: {
+          const C uu = src.get(sub == S_DST3 ? n - 1 - q : q);
+          const C vv = (q > 0) ? src.get(sub == S_DST3 ? q - 1 : n - q) : mk<C, R>(zero, zero);
+          const C w = aux0[q];
+          const C Vx = cmul(w, mk<C, R>(uu.x, -vv.x));
+          const C Vy = cmul(w, mk<C, R>(uu.y, -vv.y));
+          z = mk<C, R>(Vx.x - Vy.y, Vx.y + Vy.x);
+        } break;
+        case S_DCT1: z = src.get(q <= n - 1 ? q : N - q); break;
+        case S_DST1:
+          if (q == 0 || q == n + 1) {
+            z = mk<C, R>(zero, zero);
+          } else if (q <= n) {
+            z = src.get(q - 1);
+          } else {
+            const C t = src.get(N - q - 1);
+            z = mk<C, R>(-t.x, -t.y);
+          }
+          break;
+        default: z = src.get(q); break;  // DHT
+      }
+      v[u][r] = z;
+    }
+  }
+}
+
+// Outputs k of both lines of a pair (x: first line / real part, y: second
+// line / imaginary part), from the natural-order FFT results `seq`.
+template <typename R, int N>
+__device__ __forceinline__ typename Cx<R>::T r2r_output(int sub, const typename Cx<R>::T* seq, int k, int n,
+                                                       const typename Cx<R>::T* __restrict__ aux0) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  const R h = R(0.5);
+  switch (sub) {
+    case S_DCT2:
+    case S_DST2: {
+      const int kk = (sub == S_DST2) ? n - 1 - k : k;
+      const C a = seq[G::pad(kk)];
+      const C b = seq[G::pad(kk == 0 ? 0 : n - kk)];
+      const C V0 = mk<C, R>((a.x + b.x) * h, (a.y - b.y) * h);
+      const C V1 = mk<C, R>((a.y + b.y) * h, (b.x - a.x) * h);
+      const C w = aux0[kk];
+      return mk<C, R>(R(2) * (w.x * V0.x - w.y * V0.y), R(2) * (w.x * V1.x - w.y * V1.y));
+    }
+    case S_DCT3:
+    case S_DST3: {
+      const C z = seq[G::pad((k & 1) ? n - 1 - (k >> 1) : (k >> 1))];
+      return (sub == S_DST3 && (k & 1)) ? mk<C, R>(-z.x, -z.y) : z;
+    }
+    case S_DCT1: return seq[G::pad(k)];
+    case S_DST1: {
+      const C z = seq[G::pad(k + 1)];
+      return mk<C, R>(-z.y, z.x);
+    }
+    default: {  // DHT
+      const C a = seq[G::pad(k)];
+      const C b = seq[G::pad(k == 0 ? 0 : n - k)];
+      const C V0 = mk<C, R>((a.x + b.x) * h, (a.y - b.y) * h);
+      const C V1 = mk<C, R>((a.y + b.y) * h, (b.x - a.x) * h);
+      return mk<C, R>(V0.x - V0.y, V1.x - V1.y);
+    }
+  }
+}
+
+// Post-processing and store of one tile: direct (transform axis contiguous
+// in the destination) or transposed through the row table.
+template <typename R, int N>
+__device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
+                                             const long long* Atab) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NSEQ = G::NSEQ;
+  constexpr int SEQ = G::SEQ;
+  const int tid = threadIdx.x;
+  const int L = ta.lines;
+  const int n = A.n_out;
+  const int sub = A.sub;
+  const bool cplx = A.out_complex != 0;
+  const R sc = R(A.scale);
+  const R pf = R(A.post_factor);
+  const int post_mode = A.post_mode;
+  const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
+  const bool direct = A.dst_k_contig != 0;
+  for (int i = tid; i < NSEQ * n; i += MR_THREADS) {
+    int s, k;
+    if (direct) {
+      s = i / n;
+      k = i - s * n;
+    } else {
+      s = i % NSEQ;
+      k = i / NSEQ;
+    }
+    if (cplx ? s >= L : 2 * s >= L) continue;
+    C v = r2r_output<R, N>(sub, res + s * SEQ, k, n, aux0);
+    R f = sc;
+    if (post_mode != W_NONE && weight_hit(post_mode, k, n)) f *= pf;
+    v = scl(v, f);
+    if (cplx) {
+      C* __restrict__ out = reinterpret_cast<C*>(A.out);
+      out[direct ? ta.dst0 + (long long)s * ta.dstb + k : Atab[k] + s] = v;
+    } else {
+      R* __restrict__ out = reinterpret_cast<R*>(A.out);
+      if (direct) {
+        const long long o = ta.dst0 + (long long)(2 * s) * ta.dstb + k;
+        out[o] = v.x;
+        if (2 * s + 1 < L) out[o + ta.dstb] = v.y;
+      } else {
+        const long long o = Atab[k] + 2 * s;
+        out[o] = v.x;
+        if (2 * s + 1 < L) out[o + 1] = v.y;
+      }
+    }
+  }
+}
+
+// Transform and store of one tile whose stage-0 inputs are in `v`.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& ta,
+                                            typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                            typename Cx<R>::T* b0, typename Cx<R>::T* b1,
+                                            const typename Cx<R>::T* W, long long* Atab, const int2* ktab,
+                                            PieceAddr* prow, const PieceAddr& my_piece, int npieces) {
+  using G = MRGeom<R, N>;
+  const int tid = threadIdx.x;
+  mr_stage0<R, N, INV>(v, b0);
+  if (tid < npieces) prow[tid] = my_piece;
+  __syncthreads();
+  if (!A.dst_k_contig) {
+    for (int k = tid; k < A.n_out; k += MR_THREADS) {
+      const int2 kp = ktab[k];
+      const PieceAddr pa = prow[kp.x];
+      Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+    }
+  }
+  mr_stages_upto<R, N, INV, 1, G::NST>(b0, b1, W);
+  mr_store_r2r<R, N>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab);
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(MR_THREADS, 2) mr_r2r_kernel(const PassArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (A.gate != nullptr && *A.gate != 0) return;
+  mr_run<R, N, true>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
+}
+
+template <typename R, int N>
+cudaError_t mr_r2r_launch(const PassArgs& A, cudaStream_t stream) {
+  constexpr size_t smem = mr_smem_bytes<R, N>();
+  cudaError_t err = cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
+  if (grid > A.ntiles) grid = A.ntiles;
+  mr_r2r_kernel<R, N><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+template <typename R, int N>
+int mr_r2r_occupancy() {
+  constexpr size_t smem = mr_smem_bytes<R, N>();
+  int blocks = 0;
+  if (cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_r2r_kernel<R, N>, MR_THREADS, smem) != cudaSuccess)
+    return 1;
+  return blocks > 0 ? blocks : 1;
+}
+
+}  // namespace pb

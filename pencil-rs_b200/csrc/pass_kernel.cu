@@ -113,16 +113,6 @@ __device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const P
   return in;
 }
 
-__device__ __forceinline__ bool weight_hit(int mode, int idx, int n) {
-  switch (mode) {
-    case W_FIRST: return idx == 0;
-    case W_LAST: return idx == n - 1;
-    case W_INTERIOR: return idx > 0 && idx < n - 1;
-    case W_HALF_INTERIOR: return idx != 0 && !((n & 1) == 0 && idx == n / 2);
-    default: return false;
-  }
-}
-
 // One tile of a pass: gather, transform, scatter.  `smem` is the block's
 // dynamic shared memory (pass_smem_bytes(A) bytes).
 template <typename R>
@@ -708,6 +698,7 @@ size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
 }
 
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.fast == 3) return launch_mr_r2r(A, real_bytes, stream);
   if (A.fast == 2) return launch_mr(A, real_bytes, stream);
   if (A.fast) return launch_pow2(A, real_bytes, stream);
   const size_t smem = pass_smem_bytes(A, real_bytes);

@@ -108,6 +108,12 @@ int batch_occupancy(int real_bytes, size_t smem);
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int pow2_lines(int m, int kind, int real_bytes);
 int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes);
+// real-to-real kinds on the mixed-radix kernel (mr_r2r.cuh), FFT lengths of
+// kMrR2rLengths
+bool mr_r2r_supported(int m, int real_bytes);
+cudaError_t launch_mr_r2r(const PassArgs& A, int real_bytes, cudaStream_t stream);
+int mr_r2r_lines(int m, int complex_data, int real_bytes);
+int mr_r2r_occupancy(int m, int real_bytes);
 // mixed-radix pass kernel (mr_kernel.cuh) for the lengths of mr_lengths.hpp
 bool mr_supported(int m, int real_bytes);
 cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream);

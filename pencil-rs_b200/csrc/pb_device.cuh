@@ -70,4 +70,15 @@ __device__ __forceinline__ unsigned fdiv(unsigned x, unsigned d, unsigned m) {
 }
 __device__ __forceinline__ unsigned fdiv_magic(unsigned d) { return 0xffffffffu / d; }
 
+// Whether element idx of a length-n line carries the adjoint weight of `mode`.
+__device__ __forceinline__ bool weight_hit(int mode, int idx, int n) {
+  switch (mode) {
+    case W_FIRST: return idx == 0;
+    case W_LAST: return idx == n - 1;
+    case W_INTERIOR: return idx > 0 && idx < n - 1;
+    case W_HALF_INTERIOR: return idx != 0 && !((n & 1) == 0 && idx == n / 2);
+    default: return false;
+  }
+}
+
 }  // namespace pb

@@ -75,9 +75,22 @@ __device__ __forceinline__ C twmul(C v, C w) {
   return c;
 }
 
+// cos(2 pi i / 11), sin(2 pi i / 11) for i = 1..5 (double precision; the
+// other indices follow from cos(2 pi (11-i)/11) = cos(2 pi i/11) and
+// sin(2 pi (11-i)/11) = -sin(2 pi i/11))
+__host__ __device__ constexpr double kcos11(int i) {
+  return i == 1 ? 0.8412535328311812 : i == 2 ? 0.41541501300188644 : i == 3 ? -0.142314838273285
+         : i == 4 ? -0.654860733945285 : -0.9594929736144974;
+}
+__host__ __device__ constexpr double ksin11(int i) {
+  return i == 1 ? 0.5406408174555976 : i == 2 ? 0.9096319953545183 : i == 3 ? 0.9898214418809328
+         : i == 4 ? 0.7557495743542583 : 0.28173255684142967;
+}
+
 // cos(2 pi i / R), sin(2 pi i / R) for the odd small radices (exact doubles).
 __host__ __device__ constexpr double kcos(int R, int i) {
-  return R == 3 ? (i == 0 ? 1.0 : -0.5)
+  return R == 11 ? (i == 0 ? 1.0 : kcos11(i <= 5 ? i : 11 - i))
+         : R == 3 ? (i == 0 ? 1.0 : -0.5)
          : R == 5 ? (i == 0 ? 1.0 : (i == 1 || i == 4) ? 0.30901699437494745 : -0.8090169943749475)
                   : (i == 0 ? 1.0
                      : (i == 1 || i == 6) ? 0.6234898018587335
@@ -85,7 +98,8 @@ __host__ __device__ constexpr double kcos(int R, int i) {
                                           : -0.9009688679024191);
 }
 __host__ __device__ constexpr double ksin(int R, int i) {
-  return R == 3 ? (i == 0 ? 0.0 : i == 1 ? 0.8660254037844386 : -0.8660254037844386)
+  return R == 11 ? (i == 0 ? 0.0 : i <= 5 ? ksin11(i) : -ksin11(11 - i))
+         : R == 3 ? (i == 0 ? 0.0 : i == 1 ? 0.8660254037844386 : -0.8660254037844386)
          : R == 5 ? (i == 0   ? 0.0
                      : i == 1 ? 0.9510565162951535
                      : i == 2 ? 0.5877852522924731
@@ -188,5 +202,7 @@ template <typename C, bool INV>
 struct Bfly<C, 5, INV> : BflyOdd<C, 5, INV> {};
 template <typename C, bool INV>
 struct Bfly<C, 7, INV> : BflyOdd<C, 7, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 11, INV> : BflyOdd<C, 11, INV> {};
 
 }  // namespace pb

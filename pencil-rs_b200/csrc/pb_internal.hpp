@@ -85,7 +85,7 @@ struct PassArgs {
   double scale;
   int src_k_contig;  // transform axis has unit stride in the source
   int dst_k_contig;  // transform axis has unit stride in the destination
-  int fast;          // 1: register-resident power-of-two kernel (pow2_kernel.cu), 2: mixed-radix (mr_kernel.cuh)
+  int fast;          // 1: power-of-two kernel (pow2_kernel.cu), 2: mixed-radix (mr_kernel.cuh), 3: its R2R kinds (mr_r2r.cuh)
   int nstages;
   int radix[MAXSTAGES];
   int ld;          // leading dimension (complex units) of a sequence in smem

@@ -865,8 +865,9 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
   if (A.fast && !P.force_generic) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int occ = A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
-                                : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
+    const int occ = A.fast == 3   ? mr_r2r_occupancy(A.m, P.real_bytes)
+                    : A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
+                                  : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
     A.grid_ctas = sms * std::max(1, occ);
   }
 }
@@ -962,6 +963,20 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.fast = 2;
       A.dst_k_contig = direct ? 1 : 0;
       L = mr_lines(A.m, op.kind, P.real_bytes);
+      A.lines = L;
+    }
+  }
+  // real-to-real kinds on the mixed-radix kernel (all but the type-IV kinds):
+  // the same layout conditions, FFT lengths of kMrR2rLengths
+  if (!A.fast && !P.force_generic && op.kind == P_R2R && op.sub != S_DCT4 && op.sub != S_DST4 &&
+      mr_r2r_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    if (direct || transposed) {
+      A.fast = 3;
+      A.dst_k_contig = direct ? 1 : 0;
+      L = mr_r2r_lines(A.m, in_complex ? 1 : 0, P.real_bytes);
       A.lines = L;
     }
   }
@@ -1803,7 +1818,7 @@ int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int3
     const Program& prog = plan->prog[user_mode(*plan, op)];
     int n = 0;
     for (const Step& s : prog.steps) {
-      const int k = s.type != 0 ? 1 : (s.pa.fast == 1 ? 2 : (s.pa.fast == 2 ? 3 : 0));
+      const int k = s.type != 0 ? 1 : (s.pa.fast == 1 ? 2 : (s.pa.fast >= 2 ? 3 : 0));
       if (kernels && n < capacity) kernels[n] = k;
       ++n;
     }
