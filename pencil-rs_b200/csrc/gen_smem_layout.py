@@ -33,6 +33,9 @@ MR = [35, 36, 40, 42, 45, 48, 49, 50, 54, 56, 60, 63, 70, 72, 75, 80, 81, 84, 90
       125, 126, 135, 140, 144, 147, 150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
       245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375, 378, 384, 392, 400, 405, 420,
       432, 441, 448, 450, 480, 486, 490, 500, 504]
+# the mixed-radix kernel also runs the real-to-real kinds on powers of two and
+# on 770 (mr_lengths.hpp, kMrR2rLengths)
+MR_ALL = sorted(MR + [32, 64, 128, 256, 512, 770])
 SHIFTS = [0, 2, 3, 4, 5]
 KINDS = [("c2c", False), ("r2c", False), ("c2r", False), ("c2c", True), ("r2c", True), ("c2r", True)]
 
@@ -129,22 +132,33 @@ def p2_cost(N, rb, sh, SEQ, kind, direct):
 
 
 # ---------------------------------------------------------- mixed-radix kernel
-def mr_factor(N):
-    r, m = [], N
-    while m % 8 == 0 and m > 1:
-        r.append(8)
-        m //= 8
-    if m % 4 == 0:
-        r.append(4)
-        m //= 4
-    if m % 2 == 0:
-        r.append(2)
-        m //= 2
-    for p in (7, 5, 3):
-        while m % p == 0:
-            r.append(p)
-            m //= p
-    return r
+RADICES = [16, 15, 14, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2]
+
+
+def mr_factor(N, max_radix=16):
+    """Stage radices of mr_kernel.cuh (up to max_radix; 11 always allowed):
+    fewest stages, then smallest largest radix."""
+    inf = 1 << 20
+    st, mx, ch = {}, {}, {}
+    for m in range(2, N + 1):
+        if N % m:
+            continue
+        st[m], mx[m], ch[m] = inf, inf, 0
+        for r in RADICES:
+            if m % r or (r > max_radix and r != 11):
+                continue
+            rest = m // r
+            if rest > 1 and st[rest] >= inf:
+                continue
+            sx = (0 if rest == 1 else st[rest]) + 1
+            xx = r if (rest == 1 or mx[rest] < r) else mx[rest]
+            if sx < st[m] or (sx == st[m] and xx < mx[m]):
+                st[m], mx[m], ch[m] = sx, xx, r
+    out, m = [], N
+    while m > 1 and ch[m] > 0:
+        out.append(ch[m])
+        m //= ch[m]
+    return out
 
 
 def mr_nseq(N, rb):
@@ -159,8 +173,13 @@ def mr_nseq(N, rb):
     return p
 
 
-def mr_sched(N, nseq):
-    r = mr_factor(N)
+def mr_max_radix(N, nseq, rb):
+    """Radix cap of mr_kernel.cuh (MRGeom::MAX_RADIX)."""
+    return 16 if (rb == 4 and N & (N - 1)) else 8
+
+
+def mr_sched(N, nseq, rb):
+    r = mr_factor(N, mr_max_radix(N, nseq, rb))
     best, best_cost = 0, 1 << 30
     for i, R in enumerate(r):
         c = ((nseq * (N // R) + THREADS - 1) // THREADS) * R
@@ -172,7 +191,7 @@ def mr_sched(N, nseq):
 def mr_cost(N, rb, sh, SEQ, kind, direct):
     E = 2 * rb
     nseq = mr_nseq(N, rb)
-    rad = mr_sched(N, nseq)
+    rad = mr_sched(N, nseq, rb)
     tot = 0
     ns = 1
     for st, R in enumerate(rad):
@@ -235,7 +254,7 @@ def best_layout(args):
 
 
 def main():
-    jobs = [("pow2", N, rb) for N in POW2 for rb in (4, 8)] + [("mr", N, rb) for N in MR for rb in (4, 8)]
+    jobs = [("pow2", N, rb) for N in POW2 for rb in (4, 8)] + [("mr", N, rb) for N in MR_ALL for rb in (4, 8)]
     with get_context("spawn").Pool(os.cpu_count() or 1) as pool:
         res = pool.map(best_layout, jobs)
     table = {(f, N, rb): (sh, seq) for f, N, rb, sh, seq, _ in res}
@@ -244,7 +263,7 @@ def main():
            "// precision by replaying the kernels' shared-memory accesses through a bank",
            "// model.  Element i of sequence s sits at s*SEQ + i + (SH ? i >> SH : 0).",
            "#pragma once", "", "namespace pb {", "", "struct SmemLayout {", "  int sh;", "  int seq;", "};", ""]
-    for family, lengths in (("pow2", POW2), ("mr", MR)):
+    for family, lengths in (("pow2", POW2), ("mr", MR_ALL)):
         out.append(f"// {family}: {{f32}}, {{f64}} per length")
         out.append(f"__host__ __device__ constexpr SmemLayout {family}_layout(int N, int real_bytes) {{")
         out.append("  switch (N) {")

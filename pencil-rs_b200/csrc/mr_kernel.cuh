@@ -2,9 +2,10 @@
 // (35, 210, 384, ...): the C2C, R2C and C2R stages of the canonical route for
 // those lengths.  Power-of-two lengths take pow2_kernel.cu.
 //
-// The length N is a template parameter, so the radix schedule (radix 8 while
-// it divides, then 4 or 2, then 7, 5, 3, with the stage-0 radix chosen to fit
-// the tile to the threads) and every index division are compile-time.
+// The length N is a template parameter, so the radix schedule (the fewest
+// stages over radices 2..16, composite radices butterflied in registers, with
+// the stage-0 radix chosen to fit the tile to the threads) and every index
+// division are compile-time.
 // Persistent CTAs of 256 threads walk the pass's tiles of NSEQ complex
 // sequences (one line each, or a pair of real lines for R2C/C2R).  Stage 0
 // reads its butterfly inputs from HBM straight into registers; the next tile's
@@ -39,37 +40,38 @@ struct RadixList {
   int r[24];
 };
 
-__host__ __device__ constexpr RadixList mr_factor(int N) {
+constexpr int kMrMaxLen = 1024;
+
+// Factorisation of N (<= 1024) into stage radices up to max_radix (11, a
+// prime, is always allowed): the fewest stages (each is one shared-memory
+// round trip), then the smallest largest radix (registers per butterfly).
+// Dynamic programming over the divisors of N.
+__host__ __device__ constexpr RadixList mr_factor(int N, int max_radix) {
+  // radices of a stage: single butterflies (2, 3, 4, 5, 7, 8, 11) and the
+  // register composites of pb_fft.cuh (6, 9, 10, 12, 14, 15, 16)
+  const int radices[14] = {16, 15, 14, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  int st[kMrMaxLen + 1] = {}, mx[kMrMaxLen + 1] = {}, ch[kMrMaxLen + 1] = {};
+  constexpr int kInf = 1 << 20;
+  for (int m = 2; m <= N; ++m) {
+    if (N % m != 0) continue;
+    st[m] = kInf;
+    mx[m] = kInf;
+    for (int i = 0; i < 14; ++i) {
+      const int r = radices[i];
+      if (m % r != 0 || (r > max_radix && r != 11)) continue;
+      const int rest = m / r;
+      if (rest > 1 && st[rest] >= kInf) continue;
+      const int sx = (rest == 1 ? 0 : st[rest]) + 1;
+      const int xx = (rest == 1 || mx[rest] < r) ? r : mx[rest];
+      if (sx < st[m] || (sx == st[m] && xx < mx[m])) {
+        st[m] = sx;
+        mx[m] = xx;
+        ch[m] = r;
+      }
+    }
+  }
   RadixList L{0, {}};
-  int m = N;
-  while (m % 8 == 0 && m > 1) {
-    L.r[L.n++] = 8;
-    m /= 8;
-  }
-  if (m % 4 == 0) {
-    L.r[L.n++] = 4;
-    m /= 4;
-  }
-  if (m % 2 == 0) {
-    L.r[L.n++] = 2;
-    m /= 2;
-  }
-  while (m % 7 == 0) {
-    L.r[L.n++] = 7;
-    m /= 7;
-  }
-  while (m % 5 == 0) {
-    L.r[L.n++] = 5;
-    m /= 5;
-  }
-  while (m % 3 == 0) {
-    L.r[L.n++] = 3;
-    m /= 3;
-  }
-  while (m % 11 == 0) {
-    L.r[L.n++] = 11;
-    m /= 11;
-  }
+  for (int m = N; m > 1 && ch[m] > 0; m /= ch[m]) L.r[L.n++] = ch[m];
   return L;
 }
 
@@ -77,8 +79,8 @@ __host__ __device__ constexpr RadixList mr_factor(int N) {
 // with the stage-0 radix moved to the front.  Stage 0 keeps U0*R0 values per
 // thread in registers (U0 = ceil(NSEQ*N/R0 / threads)), so R0 is the radix
 // that minimises that count (the larger radix on a tie).
-__host__ __device__ constexpr RadixList mr_sched(int N, int NSEQ) {
-  RadixList L = mr_factor(N);
+__host__ __device__ constexpr RadixList mr_sched(int N, int NSEQ, int max_radix) {
+  RadixList L = mr_factor(N, max_radix);
   int best = 0, best_cost = 1 << 30;
   for (int i = 0; i < L.n; ++i) {
     const int R = L.r[i];
@@ -94,9 +96,8 @@ __host__ __device__ constexpr RadixList mr_sched(int N, int NSEQ) {
   return L;
 }
 
-// Product of the first s radices of the schedule.
-__host__ __device__ constexpr int mr_ns(int N, int NSEQ, int s) {
-  const RadixList L = mr_sched(N, NSEQ);
+// Product of the first s radices of a schedule.
+__host__ __device__ constexpr int mr_ns(const RadixList& L, int s) {
   int p = 1;
   for (int i = 0; i < s; ++i) p *= L.r[i];
   return p;
@@ -111,8 +112,7 @@ __host__ __device__ constexpr int mr_pow2floor(int x) {
 // Offset of stage ST's twiddles in the per-stage twiddle table: stage s >= 1
 // holds (R_s - 1)*NS_s entries, entry (r-1)*NS_s + k = W_N^{k*r*N/(NS_s*R_s)},
 // so the lanes of a stage read consecutive entries (N - R_0 entries in all).
-__host__ __device__ constexpr int mr_tw_off(int N, int NSEQ, int ST) {
-  const RadixList L = mr_sched(N, NSEQ);
+__host__ __device__ constexpr int mr_tw_off(const RadixList& L, int ST) {
   int off = 0, ns = L.r[0];
   for (int s = 1; s < ST; ++s) {
     off += (L.r[s] - 1) * ns;
@@ -124,7 +124,6 @@ __host__ __device__ constexpr int mr_tw_off(int N, int NSEQ, int ST) {
 // Complex elements per tile: 3072 (24 KB) in f32, 1536 (24 KB) in f64.
 template <typename R, int N>
 struct MRGeom {
-  static constexpr int NST = mr_factor(N).n;
   static constexpr int TILE_ELEMS = sizeof(R) == 4 ? 3072 : 1536;
   static constexpr int FIT = TILE_ELEMS / N;
   static constexpr int NSEQ = FIT >= 64 ? 64 : (FIT < 2 ? 2 : mr_pow2floor(FIT));
@@ -133,7 +132,13 @@ struct MRGeom {
   static constexpr SmemLayout LAY = mr_layout(N, (int)sizeof(R));
   static constexpr int SH = LAY.sh;
   static constexpr int SEQ = LAY.seq;
-  static constexpr int R0 = mr_sched(N, NSEQ).r[0];
+  // the stage radices: composites up to 16 in f32 and 8 in f64 (register
+  // budget; fewer stages won over full thread use in a per-length sweep), and
+  // radix 8 for powers of two (two radix-16 stages leave half the threads idle)
+  static constexpr int MAX_RADIX = (sizeof(R) == 4 && (N & (N - 1)) != 0) ? 16 : 8;
+  static constexpr RadixList RL = mr_sched(N, NSEQ, MAX_RADIX);
+  static constexpr int NST = RL.n;
+  static constexpr int R0 = RL.r[0];
   static constexpr int NB0 = N / R0;
   static constexpr int B0 = NSEQ * NB0;                         // stage-0 butterflies per tile
   static constexpr int U0 = (B0 + MR_THREADS - 1) / MR_THREADS;  // per thread
@@ -149,13 +154,12 @@ __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ i
                                          const typename Cx<R>::T* __restrict__ Wst) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
-  constexpr RadixList RL = mr_sched(N, G::NSEQ);
-  constexpr int RAD = RL.r[ST];
-  constexpr int NS = mr_ns(N, G::NSEQ, ST);
+  constexpr int RAD = G::RL.r[ST];
+  constexpr int NS = mr_ns(G::RL, ST);
   constexpr int NB = N / RAD;
   constexpr int TOT = G::NSEQ * NB;
   constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
-  const C* __restrict__ tw = Wst + mr_tw_off(N, G::NSEQ, ST);
+  const C* __restrict__ tw = Wst + mr_tw_off(G::RL, ST);
 #pragma unroll 1
   for (int it = 0; it < ITER; ++it) {
     const int b = threadIdx.x + it * MR_THREADS;
@@ -197,11 +201,10 @@ template <typename R, int N, int ST>
 __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const typename Cx<R>::T* __restrict__ Wg) {
   using G = MRGeom<R, N>;
   if constexpr (ST < G::NST) {
-    constexpr RadixList RL = mr_sched(N, G::NSEQ);
-    constexpr int RAD = RL.r[ST];
-    constexpr int NS = mr_ns(N, G::NSEQ, ST);
+    constexpr int RAD = G::RL.r[ST];
+    constexpr int NS = mr_ns(G::RL, ST);
     constexpr int TW = N / (NS * RAD);
-    constexpr int OFF = mr_tw_off(N, G::NSEQ, ST);
+    constexpr int OFF = mr_tw_off(G::RL, ST);
     for (int i = threadIdx.x; i < (RAD - 1) * NS; i += MR_THREADS) {
       const int r = i / NS + 1, k = i - (i / NS) * NS;
       Wst[OFF + i] = Wg[k * TW * r];
@@ -305,14 +308,13 @@ __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const Til
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int ST = G::NST - 1;
-  constexpr RadixList RL = mr_sched(N, G::NSEQ);
-  constexpr int RAD = RL.r[ST];
+  constexpr int RAD = G::RL.r[ST];
   constexpr int NB = N / RAD;
   constexpr int TOT = G::NSEQ * NB;
   constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
   const int L = ta.lines;
   const R sc = R(A.scale);
-  const C* __restrict__ tw = W + mr_tw_off(N, G::NSEQ, ST);
+  const C* __restrict__ tw = W + mr_tw_off(G::RL, ST);
 #pragma unroll 1
   for (int it = 0; it < ITER; ++it) {
     const int b = threadIdx.x + it * MR_THREADS;

@@ -114,6 +114,43 @@ __host__ __device__ constexpr double ksin(int R, int i) {
                               : -0.7818314824680298);
 }
 
+// cos and sin of 2*pi*num/den as compile-time constants: the argument is
+// reduced with exact integer symmetries to [0, pi/4] and evaluated by its
+// Taylor series (15 terms, far below double rounding on that interval).
+__host__ __device__ constexpr double ktaylor_sin(double x) {
+  double term = x, sum = x;
+  for (int i = 1; i < 15; ++i) {
+    term *= -x * x / ((2.0 * i) * (2.0 * i + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr double ktaylor_cos(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int i = 1; i < 15; ++i) {
+    term *= -x * x / ((2.0 * i - 1.0) * (2.0 * i));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double kPi = 3.14159265358979323846264338327950288;
+// cos(2 pi t / d) for 0 <= t <= d/2 (angle in [0, pi]); 8t compared with d
+// picks the octant, so the series argument stays within pi/4
+__host__ __device__ constexpr double kcos_half(long long t, long long d) {
+  return (8 * t <= d)       ? ktaylor_cos(2.0 * kPi * (double)t / (double)d)
+         : (8 * t <= 3 * d) ? ktaylor_sin(kPi / 2.0 - 2.0 * kPi * (double)t / (double)d)
+         : (8 * t <= 5 * d) ? -ktaylor_sin(2.0 * kPi * (double)t / (double)d - kPi / 2.0)
+                            : -ktaylor_cos(kPi - 2.0 * kPi * (double)t / (double)d);
+}
+__host__ __device__ constexpr double kcos2pi(long long num, long long den) {
+  const long long t = ((num % den) + den) % den;
+  return 2 * t <= den ? kcos_half(t, den) : kcos_half(den - t, den);
+}
+__host__ __device__ constexpr double ksin2pi(long long num, long long den) {
+  // sin(2 pi t/d) = cos(2 pi (t - d/4)/d) = cos(2 pi (4t - d)/(4d))
+  return kcos2pi(4 * num - den, 4 * den);
+}
+
 template <typename C, int RAD, bool INV>
 struct Bfly;
 
@@ -204,5 +241,61 @@ template <typename C, bool INV>
 struct Bfly<C, 7, INV> : BflyOdd<C, 7, INV> {};
 template <typename C, bool INV>
 struct Bfly<C, 11, INV> : BflyOdd<C, 11, INV> {};
+
+// Composite radix R1*R2 in registers (Cooley-Tukey, decimation in time):
+// Y[n2][k1] = DFT_R1(x[R2*n1 + n2]) * W^{n2*k1}, X[k1 + R1*k2] = DFT_R2(Y[.][k1]),
+// W = exp(-+2 pi i/(R1*R2)) with compile-time constants.
+template <typename C, int R1, int R2, bool INV>
+struct BflyComp {
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(v[0].x);
+    constexpr int NN = R1 * R2;
+    C y[R2][R1];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) {
+      C t[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
+      Bfly<C, R1, INV>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        const int e = (n2 * k1) % NN;
+        if (e == 0) {
+          y[n2][k1] = t[k1];
+        } else if (4 * e == NN) {  // W = -+i
+          y[n2][k1] = rot<INV>(t[k1]);
+        } else if (2 * e == NN) {  // W = -1
+          y[n2][k1] = mk<C, R>(-t[k1].x, -t[k1].y);
+        } else {
+          const R c = R(kcos2pi(e, NN)), sn = R(ksin2pi(e, NN));
+          y[n2][k1] = cmul(t[k1], mk<C, R>(c, INV ? sn : -sn));
+        }
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      C t[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) t[n2] = y[n2][k1];
+      Bfly<C, R2, INV>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+  }
+};
+template <typename C, bool INV>
+struct Bfly<C, 6, INV> : BflyComp<C, 2, 3, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 9, INV> : BflyComp<C, 3, 3, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 10, INV> : BflyComp<C, 2, 5, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 12, INV> : BflyComp<C, 4, 3, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 14, INV> : BflyComp<C, 2, 7, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 15, INV> : BflyComp<C, 3, 5, INV> {};
+template <typename C, bool INV>
+struct Bfly<C, 16, INV> : BflyComp<C, 4, 4, INV> {};
 
 }  // namespace pb
