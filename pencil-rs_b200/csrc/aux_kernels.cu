@@ -80,9 +80,13 @@ __global__ void __launch_bounds__(256) xpose_kernel(const XposeArgs A) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long long t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
     const XTile X = A.tiles[t];
-    if (A.row) {
-      for (int i = threadIdx.x; i < X.ns; i += blockDim.x)
-        out[X.dst0 + (long long)i * X.dst_ss] = in[X.src0 + (long long)i * X.src_ss];
+    if (A.row) {  // nd runs of ns elements, one step of (src_sd, dst_sd) apart
+      const int n = X.ns * X.nd;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int id = i / X.ns, is = i - id * X.ns;
+        out[X.dst0 + (long long)is * X.dst_ss + (long long)id * X.dst_sd] =
+            in[X.src0 + (long long)is * X.src_ss + (long long)id * X.src_sd];
+      }
       continue;
     }
     if (lane < X.ns)

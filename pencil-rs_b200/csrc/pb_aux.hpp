@@ -81,15 +81,17 @@ struct SpectralArgs {
 // remap): element (is, id), is < ns, id < nd, moves from
 // src0 + is*src_ss + id*src_sd to dst0 + is*dst_ss + id*dst_sd.  A tile lies
 // inside one source rank, one destination rank and one wrap segment of the
-// remap, so these offsets are affine.  row = 1: a single run (nd = 1) of up to
-// XROW elements along an axis contiguous in both layouts.
+// remap, so these offsets are affine.  row = 1: the innermost axis is the same
+// in both layouts; a tile is nd runs of ns elements along it, the runs one
+// step of a second axis apart (ns*nd <= XROW_ELEMS when nd > 1).
 struct XTile {
   long long src0, dst0;
   int src_ss, src_sd, dst_ss, dst_sd;
   int ns, nd;
 };
 constexpr int XT = 32;      // tile edge (elements)
-constexpr int XROW = 1024;  // run length of a row tile
+constexpr int XROW = 1024;  // longest run of a row tile
+constexpr int XROW_ELEMS = 2048;  // elements of a row tile
 
 struct XposeArgs {
   const XTile* tiles;

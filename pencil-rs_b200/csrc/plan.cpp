@@ -517,6 +517,98 @@ static std::vector<XTile> build_xtiles(const Pencil& S, const Pencil& D, long lo
   return tiles;
 }
 
+// Element offsets that are affine over a box: base + e*estride + sum_a x_a*stride[a].
+struct AffineMap {
+  long long base = 0, estride = 0;
+  long long stride[MAXN] = {};
+};
+
+// Rank r's local array of a layout as an affine map in global coordinates.
+static AffineMap rank_map(const HostLayout& h, int r) {
+  AffineMap m;
+  m.base = h.base[r];
+  m.estride = h.len[r];
+  for (int a = 0; a < h.p.N; ++a) {
+    m.stride[a] = h.stride[r][a];
+    m.base -= h.lo[r][a] * h.stride[r][a];
+  }
+  return m;
+}
+
+// A segment-layout block at buf_off: the box [lo, lo + ext) row-major in the
+// global axis order, one block of len elements per extra index.
+static AffineMap segment_map(int N, long long buf_off, long long len, const long long* lo, const long long* ext) {
+  AffineMap m;
+  m.base = buf_off;
+  m.estride = len;
+  long long rm = 1;
+  for (int a = N - 1; a >= 0; --a) {
+    m.stride[a] = rm;
+    m.base -= lo[a] * rm;
+    rm *= ext[a];
+  }
+  return m;
+}
+
+// Tiles of the copy D(e, x) <- S(e, x) over the box [lo, lo + ext) x extra,
+// spanning axis `as` (contiguous in S) and `ad` (contiguous in D), XT x XT
+// elements, or runs of up to XROW elements when as == ad.
+static void box_xtiles(int N, const long long* lo, const long long* ext, long long extra, const AffineMap& S,
+                       const AffineMap& D, int as, int ad, std::vector<XTile>& out) {
+  for (int a = 0; a < N; ++a)
+    if (ext[a] <= 0) return;
+  const bool row = as == ad;
+  if (std::llabs(S.stride[ad]) > INT_MAX || std::llabs(D.stride[as]) > INT_MAX || std::llabs(S.stride[as]) > INT_MAX ||
+      std::llabs(D.stride[ad]) > INT_MAX)
+    fail(PB_EUNSUPPORTED);
+  // row tiles step their runs along a second axis (the destination's next one)
+  int ar = ad;
+  if (row) {
+    ar = -1;
+    for (int a = N - 1; a >= 0 && ar < 0; --a)
+      if (a != as) ar = a;
+  }
+  if (ar >= 0 && (std::llabs(S.stride[ar]) > INT_MAX || std::llabs(D.stride[ar]) > INT_MAX)) fail(PB_EUNSUPPORTED);
+  std::vector<int> outer;
+  for (int a = 0; a < N; ++a)
+    if (a != as && a != ar) outer.push_back(a);
+  long long nouter = 1;
+  for (int a : outer) nouter *= ext[a];
+  const long long es = row ? XROW : XT;
+  long long x[MAXN] = {};
+  for (long long e = 0; e < extra; ++e)
+    for (long long o = 0; o < nouter; ++o) {
+      long long rem = o;
+      for (int i = (int)outer.size() - 1; i >= 0; --i) {
+        x[outer[i]] = lo[outer[i]] + rem % ext[outer[i]];
+        rem /= ext[outer[i]];
+      }
+      for (long long i = 0; i < ext[as]; i += es) {
+        const int ns = (int)std::min<long long>(es, ext[as] - i);
+        const long long ed = row ? std::max<long long>(1, XROW_ELEMS / ns) : XT;
+        const long long rext = ar >= 0 ? ext[ar] : 1;
+        for (long long j = 0; j < rext; j += ed) {
+          x[as] = lo[as] + i;
+          if (ar >= 0) x[ar] = lo[ar] + j;
+          XTile t;
+          t.src0 = S.base + e * S.estride;
+          t.dst0 = D.base + e * D.estride;
+          for (int a = 0; a < N; ++a) {
+            t.src0 += x[a] * S.stride[a];
+            t.dst0 += x[a] * D.stride[a];
+          }
+          t.src_ss = (int)S.stride[as];
+          t.dst_ss = (int)D.stride[as];
+          t.src_sd = ar >= 0 ? (int)S.stride[ar] : 0;
+          t.dst_sd = ar >= 0 ? (int)D.stride[ar] : 0;
+          t.ns = ns;
+          t.nd = (int)std::min<long long>(ed, rext - j);
+          out.push_back(t);
+        }
+      }
+    }
+}
+
 // exp(-2 pi i q/m) (negative exponent) in extended precision, rounded once.
 static size_t roots_table(pb_plan& P, int m) {
   const std::string key = "W" + std::to_string(m) + "r" + std::to_string(P.real_bytes);
@@ -1905,6 +1997,10 @@ struct pb_transpose {
   pb::RemapArgs gather{};
   std::vector<pb::SegDesc> send_segs, recv_segs;
   std::vector<long long> recv_off, send_off;
+  // tiled staging (4/8/16-byte elements): pack, exchange and unpack as copies
+  std::vector<pb::XTile> pack_tiles, exch_tiles, unpack_tiles;
+  int pack_row = 0, unpack_row = 0;
+  pb::XposeArgs xt_pack{}, xt_exch{}, xt_unpack{};
   long long send_total = 0, recv_total = 0;
   const pb::SegDesc* d_send = nullptr;
   const pb::SegDesc* d_recv = nullptr;
@@ -1968,14 +2064,32 @@ static void build_copy(pb_transpose& T) {
   }
   // segment tables (alltoallv only)
   size_t send_tab = 0, recv_tab = 0, roff_tab = 0, soff_tab = 0;
+  size_t pack_tab = 0, exch_tab = 0, unpack_tab = 0;
+  const bool staged_tiles = T.alltoallv && T.use_tiles;
   if (T.alltoallv) {
     send_tab = P.host.add(T.send_segs.data(), T.send_segs.size() * sizeof(SegDesc));
     recv_tab = P.host.add(T.recv_segs.data(), T.recv_segs.size() * sizeof(SegDesc));
     roff_tab = P.host.add(T.recv_off.data(), T.recv_off.size() * sizeof(long long));
     soff_tab = P.host.add(T.send_off.data(), T.send_off.size() * sizeof(long long));
   }
+  if (staged_tiles) {
+    pack_tab = P.host.add(T.pack_tiles.data(), T.pack_tiles.size() * sizeof(XTile));
+    exch_tab = P.host.add(T.exch_tiles.data(), T.exch_tiles.size() * sizeof(XTile));
+    unpack_tab = P.host.add(T.unpack_tiles.data(), T.unpack_tiles.size() * sizeof(XTile));
+  }
   upload_steps(P, steps);
   if (T.use_tiles) T.xt.tiles = reinterpret_cast<const XTile*>(fix_ptr(P, enc(tile_tab)));
+  if (staged_tiles) {
+    auto setup = [&](XposeArgs& X, size_t tab, const std::vector<XTile>& v, int row) {
+      X.tiles = reinterpret_cast<const XTile*>(fix_ptr(P, enc(tab)));
+      X.ntiles = (long long)v.size();
+      X.elem_bytes = T.elem_bytes;
+      X.row = row;
+    };
+    setup(T.xt_pack, pack_tab, T.pack_tiles, T.pack_row);
+    setup(T.xt_exch, exch_tab, T.exch_tiles, 1);
+    setup(T.xt_unpack, unpack_tab, T.unpack_tiles, T.unpack_row);
+  }
   auto fixpen = [&](DevPencil& d) { d.info = reinterpret_cast<const long long*>(fix_ptr(P, d.info)); };
   fixpen(G.src);
   fixpen(G.dst);
@@ -2096,6 +2210,43 @@ static void build_segments(pb_transpose& T, int changed) {
       }
     }
   }
+  if (T.elem_bytes != 4 && T.elem_bytes != 8 && T.elem_bytes != 16) return;
+  // tiles of the staged copies: pack (rank r's source array -> its send
+  // segments), exchange (send segment -> receive segment, contiguous runs),
+  // unpack (receive segments -> rank r's destination array)
+  HostLayout hs(S, T.extra), hd(D, T.extra);
+  T.pack_row = S.perm[N - 1] == N - 1;
+  T.unpack_row = D.perm[N - 1] == N - 1;
+  for (int r = 0; r < R; ++r)
+    for (int p = 0; p < P; ++p) {
+      const size_t k = (size_t)r * P + p;
+      if (slen[k] > 0 && T.extra > 0) {
+        const long long* lo = sreg[k].data();
+        const long long* ext = sreg[k].data() + MAXN;
+        box_xtiles(N, lo, ext, T.extra, rank_map(hs, r),
+                   segment_map(N, send_base[r] + sdisp[k] * T.extra, slen[k], lo, ext), S.perm[N - 1], N - 1,
+                   T.pack_tiles);
+      }
+      if (rlen[k] > 0 && T.extra > 0) {
+        const long long* lo = rreg[k].data();
+        const long long* ext = rreg[k].data() + MAXN;
+        box_xtiles(N, lo, ext, T.extra, segment_map(N, recv_base[r] + rdisp[k] * T.extra, rlen[k], lo, ext),
+                   rank_map(hd, r), N - 1, D.perm[N - 1], T.unpack_tiles);
+      }
+    }
+  for (size_t i = 0; i < T.recv_segs.size(); ++i) {
+    const long long n = T.recv_segs[i].len * T.extra;
+    for (long long j = 0; j < n; j += XROW) {
+      XTile t{};
+      t.src0 = T.send_off[i] + j;
+      t.dst0 = T.recv_off[i] + j;
+      t.src_ss = 1;
+      t.dst_ss = 1;
+      t.ns = (int)std::min<long long>(XROW, n - j);
+      t.nd = 1;
+      T.exch_tiles.push_back(t);
+    }
+  }
 }
 
 static int transpose_create(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra, int32_t elem,
@@ -2177,6 +2328,15 @@ int pb_transpose_pack(pb_transpose* plan, const void* src, void* send, void* str
     if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
     if (plan->send_segs.empty()) return (int)PB_OK;
     if (!src || !send) return (int)PB_ENULL;
+    if (plan->use_tiles) {
+      check_aligned(src, false, plan->elem_bytes);
+      check_aligned(send, false, plan->elem_bytes);
+      XposeArgs X = plan->xt_pack;
+      X.in = src;
+      X.out = send;
+      cuda_ok(launch_xpose(X, static_cast<cudaStream_t>(stream)));
+      return (int)PB_OK;
+    }
     SegArgs A{};
     A.pen = plan->gather.src;
     A.segs = plan->d_send;
@@ -2197,6 +2357,15 @@ int pb_transpose_exchange(pb_transpose* plan, const void* send, void* receive, v
     if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
     if (plan->recv_off.empty()) return (int)PB_OK;
     if (!send || !receive) return (int)PB_ENULL;
+    if (plan->use_tiles) {
+      check_aligned(send, false, plan->elem_bytes);
+      check_aligned(receive, false, plan->elem_bytes);
+      XposeArgs X = plan->xt_exch;
+      X.in = send;
+      X.out = receive;
+      cuda_ok(launch_xpose(X, static_cast<cudaStream_t>(stream)));
+      return (int)PB_OK;
+    }
     ExchArgs A{};
     A.recv_off = plan->d_recv_off;
     A.send_off = plan->d_send_off;
@@ -2216,6 +2385,15 @@ int pb_transpose_unpack(pb_transpose* plan, const void* receive, void* dst, void
     if (!plan->alltoallv) return (int)PB_EINVALID_ARGUMENT;
     if (plan->recv_segs.empty()) return (int)PB_OK;
     if (!receive || !dst) return (int)PB_ENULL;
+    if (plan->use_tiles) {
+      check_aligned(receive, false, plan->elem_bytes);
+      check_aligned(dst, false, plan->elem_bytes);
+      XposeArgs X = plan->xt_unpack;
+      X.in = receive;
+      X.out = dst;
+      cuda_ok(launch_xpose(X, static_cast<cudaStream_t>(stream)));
+      return (int)PB_OK;
+    }
     SegArgs A{};
     A.pen = plan->gather.dst;
     A.segs = plan->d_recv;
