@@ -52,6 +52,11 @@ struct Pencil {
   int grid[MAXM] = {};
   int dec[MAXM] = {};
   int perm[MAXN] = {};
+  // > 0: rows of the innermost memory axis (never split) are `pitch` elements
+  // apart instead of its extent.  Only layouts inside a plan's workspace have
+  // one; the caller's layouts are the reference's, unpadded.
+  long long pitch = 0;
+  long long inner_span(const long long* ext) const { return pitch > 0 ? pitch : ext[perm[N - 1]]; }
 
   int nranks() const {
     int s = 1;
@@ -92,7 +97,7 @@ struct Pencil {
     long long lo[MAXN], ext[MAXN];
     local(r, lo, ext);
     long long s = 1;
-    for (int x = 0; x < N; ++x) s *= ext[x];
+    for (int x = 0; x < N; ++x) s *= (x == perm[N - 1]) ? inner_span(ext) : ext[x];
     return s;
   }
   long long total(long long extra) const {
@@ -109,7 +114,7 @@ struct Pencil {
     return true;
   }
   bool same_layout(const Pencil& o) const {
-    if (!same_distribution(o)) return false;
+    if (!same_distribution(o) || pitch != o.pitch) return false;
     for (int x = 0; x < N; ++x)
       if (perm[x] != o.perm[x]) return false;
     return true;
@@ -318,7 +323,7 @@ static std::string pencil_key(const Pencil& p, long long extra) {
   std::string k = "P";
   for (int x = 0; x < p.N; ++x) k += std::to_string(p.shape[x]) + "," + std::to_string(p.perm[x]) + ";";
   for (int t = 0; t < p.M; ++t) k += std::to_string(p.grid[t]) + "," + std::to_string(p.dec[t]) + ";";
-  return k + "e" + std::to_string(extra);
+  return k + "p" + std::to_string(p.pitch) + "e" + std::to_string(extra);
 }
 
 // DevPencil with its rank table (base, len, start, stride, extent per rank).
@@ -352,7 +357,7 @@ static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size
       long long lo[MAXN], ext[MAXN];
       p.local(r, lo, ext);
       long long len = 1;
-      for (int x = 0; x < p.N; ++x) len *= ext[x];
+      for (int x = 0; x < p.N; ++x) len *= (x == p.perm[p.N - 1]) ? p.inner_span(ext) : ext[x];
       long long* row = &info[(size_t)r * w];
       row[0] = base;
       row[1] = len;
@@ -360,7 +365,7 @@ static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size
       for (int q = p.N - 1; q >= 0; --q) {
         const int ax = p.perm[q];
         row[2 + p.N + ax] = stride;
-        stride *= ext[ax];
+        stride *= (q == p.N - 1) ? p.inner_span(ext) : ext[ax];
       }
       for (int x = 0; x < p.N; ++x) {
         row[2 + x] = lo[x];
@@ -395,11 +400,11 @@ struct HostLayout {
     for (int r = 0; r < R; ++r) {
       p.local(r, lo[r].data(), ext[r].data());
       long long l = 1;
-      for (int x = 0; x < p.N; ++x) l *= ext[r][x];
+      for (int x = 0; x < p.N; ++x) l *= (x == p.perm[p.N - 1]) ? p.inner_span(ext[r].data()) : ext[r][x];
       long long s = 1;
       for (int q = p.N - 1; q >= 0; --q) {
         stride[r][p.perm[q]] = s;
-        s *= ext[r][p.perm[q]];
+        s *= (q == p.N - 1) ? p.inner_span(ext[r].data()) : ext[r][p.perm[q]];
       }
       base[r] = b;
       len[r] = l;
@@ -1185,6 +1190,18 @@ static Step make_stats(pb_plan& P, const Pencil& pen, int red_axis, bool normali
   return s;
 }
 
+// Workspace layouts whose rows are not a whole number of 32-byte sectors get
+// their rows padded to the next sector: the transposed stores of the pass
+// writing them then fill whole sectors, tile by tile, instead of sharing the
+// sectors at tile edges with the tiles of other blocks.
+static void row_pitch(Pencil& p, int elem_bytes) {
+  const int inner = p.perm[p.N - 1];
+  if (p.split_of(inner) >= 0 || 32 % elem_bytes != 0) return;
+  const long long per = 32 / elem_bytes;
+  const long long n = p.shape[inner];
+  if (n % per != 0) p.pitch = (n + per - 1) / per * per;
+}
+
 static void build_program(pb_plan& P, int mode) {
   Program& prog = P.prog[mode];
   prog.steps.clear();
@@ -1225,6 +1242,7 @@ static void build_program(pb_plan& P, int mode) {
       const Stage& nx = P.stages[active[k + 1]];
       dst = fwd ? nx.in : nx.out;
       dst_complex = fwd ? !nx.real_in : !nx.real_out;
+      row_pitch(dst, dst_complex ? 2 * P.real_bytes : P.real_bytes);
     }
     // logical line length of the stage (real length for the R2C boundary)
     const long long n_axis = (st.kind == SK_R2C) ? P.real_len : st.in.shape[st.axis];

@@ -58,34 +58,6 @@ struct P2Geom {
   static __device__ __forceinline__ int pad(int i) { return SH == 0 ? i : i + (i >> SH); }
 };
 
-// One Stockham stage on the 8 register values of each of the thread's sequences.
-template <typename C, int N, int ST, bool INV, int LPT>
-__device__ __forceinline__ void p2_stage(C (&v)[LPT][8], const C (&tw)[Sched<N>::NST][7]) {
-  using S = Sched<N>;
-  constexpr int RAD = S::radix(ST);
-  constexpr int NS = S::ns(ST);
-  constexpr int U = 8 / RAD;
-#pragma unroll
-  for (int i = 0; i < LPT; ++i) {
-    C out[8];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      C b[RAD];
-#pragma unroll
-      for (int r = 0; r < RAD; ++r) b[r] = v[i][u + r * U];
-      if (NS > 1) {
-#pragma unroll
-        for (int r = 1; r < RAD; ++r) b[r] = twmul<INV>(b[r], tw[ST][r - 1]);
-      }
-      Bfly<C, RAD, INV>::run(b);
-#pragma unroll
-      for (int r = 0; r < RAD; ++r) out[u * RAD + r] = b[r];
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[i][q] = out[q];
-  }
-}
-
 // Output position of value q (= u*RAD + r) of stage ST for thread t.
 template <int N, int ST>
 __device__ __forceinline__ int p2_out_index(int t, int q) {
@@ -98,58 +70,216 @@ __device__ __forceinline__ int p2_out_index(int t, int q) {
   return (jb - k) * RAD + k + r * NS;
 }
 
-// Loads the thread's sequences of one tile into registers.
-template <typename R, int N, int KIND, int LPT>
-__device__ __forceinline__ void p2_load(typename Cx<R>::T (&v)[LPT][8], const PassArgs& A, const TileAddr& ta,
-                                        int slot, int t) {
+// Thread mappings.  A thread holds LPT sets of 8 values; set i is butterfly
+// bfly[i] of sequence seq[i].  The middle stages use the line-major mapping
+// (slot = tid / T, t = tid % T: sequences slot + SLOTS*i, butterfly t).  The
+// last stage of a transposed store and the first stage of C2R use others so
+// that no shared-memory round is needed around them:
+//  * P2_LAST_X (transposed C2C): g = tid % SLOTS, b = tid / SLOTS; sequences
+//    LPT*g + i, butterfly b.  The thread then holds lines LPT*g .. LPT*g+LPT-1
+//    of output rows k = b + T*r and stores them from registers; a warp covers
+//    whole runs of the destination rows.
+//  * P2_LAST_R (transposed R2C, LPT = 2): s = tid % NSEQ, c = tid / NSEQ;
+//    sequence s, butterflies c and T - c (0 and T/2 for c = 0).  Output k of
+//    the last stage sits in butterfly k mod T, so the thread holds both Z[k]
+//    and Z[N-k] of every k it outputs and splits the two real lines in
+//    registers.
+//  * P2_FIRST_H (C2R, LPT = 2): s = tid / (T/2), c = tid % (T/2); sequence s,
+//    butterflies c and T - c (0 and T/2 for c = 0).  Input q of the first
+//    stage sits in butterfly q mod T; the Hermitian extension reads bin q or
+//    N - q, so both butterflies read the same 8 bins per line, each loaded
+//    once and kept raw until the tile before it is done.
+enum { P2_LAST_NAT = 0, P2_LAST_X = 1, P2_LAST_R = 2 };
+
+template <typename R, int N, int KIND, bool DIRECT>
+struct P2Modes {
+  static constexpr int LPT = P2Geom<R, N>::LPT;
+  static constexpr int LAST = (!DIRECT && KIND == P_C2C) ? P2_LAST_X
+                              : ((!DIRECT && KIND == P_R2C && LPT == 2) ? P2_LAST_R : P2_LAST_NAT);
+  static constexpr bool FIRST_H = KIND == P_C2R && LPT == 2;
+};
+
+// Raw loads of one tile's input for one thread.  Nothing reads them before the
+// tile in flight is finished, so the loads overlap that tile's arithmetic.
+// With the mirror-paired C2R mapping a holds bins c + T*m and b bins
+// T*(m+1) - c (T/2 + T*m for c = 0) of lines 2s (x) and 2s+1 (y); nx, ny are
+// the real parts of bin N/2, which only c = 0 needs.
+template <typename R, int KIND, int LPT, bool FH>
+struct P2Raw {
+  typename Cx<R>::T a[LPT][8];
+};
+template <typename R, int KIND, int LPT>
+struct P2Raw<R, KIND, LPT, true> {
+  typename Cx<R>::T xa[4], xb[4], ya[4], yb[4];
+  R nx, ny;
+};
+
+template <typename R, int N, int KIND, int LPT, bool FH>
+__device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const PassArgs& A, const TileAddr& ta,
+                                         int slot, int t) {
   using C = typename Cx<R>::T;
   constexpr int T = N / 8;
   constexpr int SLOTS = P2_THREADS / T;
   const R zero = R(0);
+  const C z = mk<C, R>(zero, zero);
   const int L = ta.lines;
+  if constexpr (FH) {
+    // slot/t are the mirror-paired sequence and butterfly c
+    const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+    const int s = slot, c = t;
+    const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+    const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
+    const long long b1 = b0 + ta.srcb;
 #pragma unroll
-  for (int i = 0; i < LPT; ++i) {
-    const int s = slot + SLOTS * i;
-    if (KIND == P_C2C) {
-      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
-      const bool ok = s < L;
-      const long long base = ta.src0 + (long long)s * ta.srcb + t;
+    for (int m = 0; m < 4; ++m) {
+      const int ba = c + T * m;
+      const int bb = c == 0 ? T / 2 + T * m : T * (m + 1) - c;
+      raw.xa[m] = ok0 ? in[b0 + ba] : z;
+      raw.xb[m] = ok0 ? in[b0 + bb] : z;
+      raw.ya[m] = ok1 ? in[b1 + ba] : z;
+      raw.yb[m] = ok1 ? in[b1 + bb] : z;
+    }
+    const R* __restrict__ inr = reinterpret_cast<const R*>(A.in);
+    raw.nx = (c == 0 && ok0) ? inr[2 * (b0 + N / 2)] : zero;
+    raw.ny = (c == 0 && ok1) ? inr[2 * (b1 + N / 2)] : zero;
+  } else {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[i][m] = ok ? in[base + T * m] : mk<C, R>(zero, zero);
-    } else if (KIND == P_R2C) {
-      const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
-      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
-      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb + t;
-      const long long b1 = b0 + ta.srcb;
+    for (int i = 0; i < LPT; ++i) {
+      const int s = slot + SLOTS * i;
+      if constexpr (KIND == P_C2C) {
+        const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+        const bool ok = s < L;
+        const long long base = ta.src0 + (long long)s * ta.srcb + t;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[i][m] = mk<C, R>(ok0 ? in[b0 + T * m] : zero, ok1 ? in[b1 + T * m] : zero);
-    } else {  // P_C2R: Hermitian extension of two half spectra
-      const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
-      const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
-      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
-      const long long b1 = b0 + ta.srcb;
-      const R w_in = R(A.pre_factor);
-      const bool weighted = A.pre_mode == W_HALF_INTERIOR;
+        for (int m = 0; m < 8; ++m) raw.a[i][m] = ok ? in[base + T * m] : z;
+      } else if constexpr (KIND == P_R2C) {
+        const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+        const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+        const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb + t;
+        const long long b1 = b0 + ta.srcb;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int q = t + T * m;
-        const bool mirror = q > N / 2;
-        const int hq = mirror ? N - q : q;
-        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
-        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
-        const bool edge = (hq == 0) || (hq == N / 2);
-        if (mirror) {
-          X.y = -X.y;
-          Y.y = -Y.y;
+        for (int m = 0; m < 8; ++m) raw.a[i][m] = mk<C, R>(ok0 ? in[b0 + T * m] : zero, ok1 ? in[b1 + T * m] : zero);
+      } else {  // P_C2R, line-major: Hermitian extension formed as the bins arrive
+        const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+        const bool ok0 = 2 * s < L, ok1 = 2 * s + 1 < L;
+        const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
+        const long long b1 = b0 + ta.srcb;
+        const R w_in = R(A.pre_factor);
+        const bool weighted = A.pre_mode == W_HALF_INTERIOR;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const int q = t + T * m;
+          const bool mirror = q > N / 2;
+          const int hq = mirror ? N - q : q;
+          C X = ok0 ? in[b0 + hq] : z;
+          C Y = ok1 ? in[b1 + hq] : z;
+          const bool edge = (hq == 0) || (hq == N / 2);
+          if (mirror) {
+            X.y = -X.y;
+            Y.y = -Y.y;
+          }
+          if (edge) {
+            X.y = zero;
+            Y.y = zero;
+          }
+          const R w = (weighted && !edge) ? w_in : R(1);
+          raw.a[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
         }
-        if (edge) {
-          X.y = zero;
-          Y.y = zero;
-        }
-        const R w = (weighted && !edge) ? w_in : R(1);
-        v[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
       }
     }
+  }
+}
+
+// First-stage inputs from the raw loads.  Mirror-paired C2R: butterfly c
+// takes bins a[m] (m < 4) and conj(b[7-m]) (m >= 4), butterfly T - c takes
+// b[m] and conj(a[7-m]); for c = 0, butterfly 0 takes bins 0, T, 2T, 3T, N/2
+// and the conjugates of 3T, 2T, T, butterfly T/2 takes b[m] and conj(b[7-m]).
+// The imaginary parts of bins 0 and N/2 are dropped, the other bins weighted
+// when the pass asks for it, and the two lines packed as X + iY.
+template <typename R, int N, int KIND, int LPT, bool FH>
+__device__ __forceinline__ void p2_finish(typename Cx<R>::T (&v)[LPT][8], const P2Raw<R, KIND, LPT, FH>& raw,
+                                          const PassArgs& A, int c) {
+  using C = typename Cx<R>::T;
+  if constexpr (FH) {
+    const R zero = R(0);
+    const bool c0 = c == 0;
+    const R wi = A.pre_mode == W_HALF_INTERIOR ? R(A.pre_factor) : R(1);
+    auto cj = [](C u) { u.y = -u.y; return u; };
+    auto pack = [&](C X, C Y, R w) { return mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w); };
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      C X0, Y0, X1, Y1;
+      if (m < 4) {
+        X0 = raw.xa[m];
+        Y0 = raw.ya[m];
+        X1 = raw.xb[m];
+        Y1 = raw.yb[m];
+      } else {
+        // c = 0: bins N/2 (m = 4) and T*(8-m) (m > 4) for butterfly 0
+        const C xa0 = m == 4 ? mk<C, R>(raw.nx, zero) : cj(raw.xa[(8 - m) & 3]);
+        const C ya0 = m == 4 ? mk<C, R>(raw.ny, zero) : cj(raw.ya[(8 - m) & 3]);
+        X0 = c0 ? xa0 : cj(raw.xb[7 - m]);
+        Y0 = c0 ? ya0 : cj(raw.yb[7 - m]);
+        X1 = c0 ? cj(raw.xb[7 - m]) : cj(raw.xa[7 - m]);
+        Y1 = c0 ? cj(raw.yb[7 - m]) : cj(raw.ya[7 - m]);
+      }
+      R w0 = wi;
+      if (m == 0 || m == 4) {  // bins 0 and N/2 of butterfly 0 are real and unweighted
+        if (c0) {
+          X0.y = zero;
+          Y0.y = zero;
+          w0 = R(1);
+        }
+      }
+      v[0][m] = pack(X0, Y0, w0);
+      v[1][m] = pack(X1, Y1, wi);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < LPT; ++i)
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[i][m] = raw.a[i][m];
+  }
+}
+
+// One radix-RAD Stockham step on the 8 register values of one sequence.
+template <typename C, int N, int ST, bool INV>
+__device__ __forceinline__ void p2_bfly8(C (&v)[8], const C (&tw)[7]) {
+  using S = Sched<N>;
+  constexpr int RAD = S::radix(ST);
+  constexpr int NS = S::ns(ST);
+  constexpr int U = 8 / RAD;
+  C out[8];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    C b[RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) b[r] = v[u + r * U];
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < RAD; ++r) b[r] = twmul<INV>(b[r], tw[r - 1]);
+    }
+    Bfly<C, RAD, INV>::run(b);
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) out[u * RAD + r] = b[r];
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) v[q] = out[q];
+}
+
+// Twiddles of butterfly T - c from those of butterfly c in the last stage
+// (NS = T): W^{(T-c) r} = W_8^r conj(W^{c r}); for c = 0 the partner is
+// butterfly T/2 with W^{(T/2) r} = W_16^r.
+template <typename C, typename R>
+__device__ __forceinline__ void p2_mirror_tw(C (&w1)[7], const C (&w0)[7], bool c0) {
+#pragma unroll
+  for (int r = 1; r < 8; ++r) {
+    const C e8 = mk<C, R>(R(kcos2pi(r, 8)), R(-ksin2pi(r, 8)));
+    const C e16 = mk<C, R>(R(kcos2pi(r, 16)), R(-ksin2pi(r, 16)));
+    C cw = w0[r - 1];
+    cw.y = -cw.y;
+    const C m = cmul(e8, cw);
+    w1[r - 1] = c0 ? e16 : m;
   }
 }
 
@@ -158,6 +288,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
   using S = Sched<N>;
   using G = P2Geom<R, N>;
+  using MD = P2Modes<R, N, KIND, DIRECT>;
   constexpr int T = G::T;
   constexpr int SLOTS = G::SLOTS;
   constexpr int LPT = G::LPT;
@@ -166,6 +297,10 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   constexpr int LMAX = (KIND == P_C2C) ? NSEQ : 2 * NSEQ;
   constexpr int H = N / 2 + 1;
   constexpr int NOUT = (KIND == P_R2C) ? H : N;
+  constexpr int NST = S::NST;
+  constexpr int LAST = MD::LAST;
+  constexpr bool FH = MD::FIRST_H;
+  constexpr bool SMEM_STORE = !(DIRECT && KIND != P_R2C) && LAST == P2_LAST_NAT;
   extern __shared__ __align__(16) unsigned char smem[];
   C* sm = reinterpret_cast<C*>(smem);
   long long* Atab = reinterpret_cast<long long*>(sm + NSEQ * SEQ);
@@ -177,8 +312,28 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   long long tile = blockIdx.x;
   if (tile >= A.ntiles) return;
   const int tid = threadIdx.x;
+  // middle stages (line-major)
   const int slot = tid / T;
   const int t = tid - slot * T;
+  // first stage
+  const int fs = FH ? tid / (T / 2) : slot;
+  const int fc = FH ? tid % (T / 2) : t;
+  // last stage
+  int lseq[LPT], lbf[LPT];
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    if (LAST == P2_LAST_X) {
+      lseq[i] = LPT * (tid % SLOTS) + i;
+      lbf[i] = tid / SLOTS;
+    } else if (LAST == P2_LAST_R) {
+      const int c = tid / NSEQ;
+      lseq[i] = tid % NSEQ;
+      lbf[i] = i == 0 ? c : (c == 0 ? T / 2 : T - c);
+    } else {
+      lseq[i] = slot + SLOTS * i;
+      lbf[i] = t;
+    }
+  }
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
   const int npieces = DIRECT ? 0 : A.npieces;
@@ -188,13 +343,13 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     for (int k = tid; k < NOUT; k += P2_THREADS) ktab[k] = A.ktab[k];
 
   // twiddles of this thread, fixed for the whole kernel: stage ST > 0 (radix 8)
-  // multiplies input r by W_N^{k*r*N/(NS*8)} with k = t mod NS
+  // multiplies input r by W_N^{k*r*N/(NS*8)} with k = butterfly mod NS
   const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
-  C tw[S::NST][7];
+  C tw[NST][7];
 #pragma unroll
-  for (int st = 1; st < S::NST; ++st) {
+  for (int st = 1; st < NST; ++st) {
     const int NS = S::ns(st);
-    const int k = t & (NS - 1);
+    const int k = (st == NST - 1 ? lbf[0] : t) & (NS - 1);
     const int step = N / (NS * 8);
 #pragma unroll
     for (int r = 1; r < 8; ++r) tw[st][r - 1] = Wg[(k * r * step) & (N - 1)];
@@ -208,7 +363,11 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   // ahead, so the prefetch of a tile never waits on the load of its address
   TileAddr ta = load_tile(tiles, tile);
   C v[LPT][8];
-  p2_load<R, N, KIND, LPT>(v, A, ta, slot, t);
+  {
+    P2Raw<R, KIND, LPT, FH> raw;
+    p2_fetch<R, N, KIND, LPT, FH>(raw, A, ta, fs, fc);
+    p2_finish<R, N, KIND, LPT, FH>(v, raw, A, fc);
+  }
   TileAddr t1 = ta;
   if (tile + G0 < A.ntiles) t1 = load_tile(tiles, tile + G0);
   PieceAddr my_piece{0, 0};
@@ -218,9 +377,9 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     const bool has_next = tile + G0 < A.ntiles;
     TileAddr t2 = t1;
     PieceAddr next_piece{0, 0};
-    C nv[LPT][8];
+    P2Raw<R, KIND, LPT, FH> nraw;
     if (has_next) {
-      p2_load<R, N, KIND, LPT>(nv, A, t1, slot, t);
+      p2_fetch<R, N, KIND, LPT, FH>(nraw, A, t1, fs, fc);
       if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
       if (tid < npieces) next_piece = pieces[(tile + G0) * npieces + tid];
     }
@@ -228,33 +387,43 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 
     // ---- Stockham stages
 #pragma unroll
-    for (int st = 0; st < S::NST; ++st) {
+    for (int st = 0; st < NST; ++st) {
+      const bool last = st == NST - 1;
       if (st > 0) {
 #pragma unroll
         for (int i = 0; i < LPT; ++i) {
-          const C* seq = sm + (slot + SLOTS * i) * SEQ;
+          const C* seq = sm + (last ? lseq[i] : slot + SLOTS * i) * SEQ;
+          const int bf = last ? lbf[i] : t;
 #pragma unroll
-          for (int m = 0; m < 8; ++m) v[i][m] = seq[G::pad(t + T * m)];
+          for (int m = 0; m < 8; ++m) v[i][m] = seq[G::pad(bf + T * m)];
         }
       }
-      switch (st) {
-        case 0: p2_stage<C, N, 0, INV, LPT>(v, tw); break;
-        case 1: p2_stage<C, N, (S::NST > 1 ? 1 : 0), INV, LPT>(v, tw); break;
-        case 2: p2_stage<C, N, (S::NST > 2 ? 2 : 0), INV, LPT>(v, tw); break;
-        default: p2_stage<C, N, (S::NST > 3 ? 3 : 0), INV, LPT>(v, tw); break;
+      C tw1[7];
+      if (LAST == P2_LAST_R && last) p2_mirror_tw<C, R>(tw1, tw[NST - 1], lbf[0] == 0);
+#pragma unroll
+      for (int i = 0; i < LPT; ++i) {
+        const C(&w)[7] = (LAST == P2_LAST_R && last && i == 1) ? tw1 : tw[st];
+        switch (st) {
+          case 0: p2_bfly8<C, N, 0, INV>(v[i], w); break;
+          case 1: p2_bfly8<C, N, (NST > 1 ? 1 : 0), INV>(v[i], w); break;
+          case 2: p2_bfly8<C, N, (NST > 2 ? 2 : 0), INV>(v[i], w); break;
+          default: p2_bfly8<C, N, (NST > 3 ? 3 : 0), INV>(v[i], w); break;
+        }
       }
-      if (st + 1 < S::NST) {
+      if (st + 1 < NST) {
         __syncthreads();  // every thread has read the buffer (previous stage or tile)
 #pragma unroll
         for (int i = 0; i < LPT; ++i) {
-          C* seq = sm + (slot + SLOTS * i) * SEQ;
+          const bool first = st == 0;
+          C* seq = sm + (first ? (FH ? fs : slot + SLOTS * i) : slot + SLOTS * i) * SEQ;
+          const int bf = first && FH ? (i == 0 ? fc : (fc == 0 ? T / 2 : T - fc)) : t;
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
             int o;
             switch (st) {
-              case 0: o = p2_out_index<N, 0>(t, q); break;
-              case 1: o = p2_out_index<N, (S::NST > 1 ? 1 : 0)>(t, q); break;
-              default: o = p2_out_index<N, (S::NST > 2 ? 2 : 0)>(t, q); break;
+              case 0: o = p2_out_index<N, 0>(bf, q); break;
+              case 1: o = p2_out_index<N, (NST > 1 ? 1 : 0)>(bf, q); break;
+              default: o = p2_out_index<N, (NST > 2 ? 2 : 0)>(bf, q); break;
             }
             seq[G::pad(o)] = v[i][q];
           }
@@ -271,9 +440,92 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
         }
       }
     }
-    // thread t now holds natural-order outputs t + T*r
+    // set i now holds outputs lbf[i] + T*r of sequence lseq[i]
+    // destination in 8-byte units: element o of an f32 complex buffer is
+    // 16-byte aligned when a8 + o is even (buffers are 8-byte aligned)
+    const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
 
-    if (DIRECT && KIND != P_R2C) {
+    // the row table is written after the first exchange; with two stages no
+    // barrier follows that before the register stores read it
+    if constexpr (LAST != P2_LAST_NAT && NST == 2) __syncthreads();
+    if constexpr (LAST == P2_LAST_X) {
+      // lines j0 .. j0+LPT-1 of rows k = b + T*r, straight from registers
+      C* __restrict__ out = reinterpret_cast<C*>(A.out);
+      const int j0 = lseq[0];
+      if (j0 < L) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const long long o = Atab[lbf[0] + T * r] + j0;
+          const C v0 = scl(v[0][r], sc);
+          if (LPT == 2 && j0 + 1 < L) {
+            const C v1 = scl(v[LPT - 1][r], sc);
+            if (sizeof(R) == 4 && ((a8 + o) & 1) == 0) {
+              float4 w;
+              w.x = (float)v0.x;
+              w.y = (float)v0.y;
+              w.z = (float)v1.x;
+              w.w = (float)v1.y;
+              *reinterpret_cast<float4*>(out + o) = w;
+            } else {
+              out[o] = v0;
+              out[o + 1] = v1;
+            }
+          } else {
+            out[o] = v0;
+          }
+        }
+      }
+    } else if constexpr (LAST == P2_LAST_R) {
+      // lines 2s, 2s+1 of rows k: X0[k] = (Z[k] + conj Z[N-k]) / 2,
+      // X1[k] = (Z[k] - conj Z[N-k]) / 2i.  Set 0 is butterfly c, set 1
+      // butterfly T - c (T/2 for c = 0); the thread outputs k = c + T*u and
+      // k = lbf[1] + T*u for u < 4, and k = N/2 when c = 0.
+      C* __restrict__ out = reinterpret_cast<C*>(A.out);
+      const bool weighted = A.post_mode == W_HALF_INTERIOR;
+      const int j = 2 * lseq[0];
+      const bool c0 = lbf[0] == 0;
+#pragma unroll
+      for (int u = 0; u < 9; ++u) {
+        int k;
+        C a, b;
+        if (u < 4) {
+          k = lbf[0] + T * u;
+          a = v[0][u];
+          b = c0 ? v[0][(8 - u) & 7] : v[1][7 - u];
+        } else if (u < 8) {
+          k = lbf[1] + T * (u - 4);
+          a = v[1][u - 4];
+          b = c0 ? v[1][11 - u] : v[0][11 - u];
+        } else {  // bin N/2, output by the c = 0 groups only
+          k = N / 2;
+          a = v[0][4];
+          b = v[0][4];
+        }
+        R f = sc * R(0.5);
+        if (weighted && k != 0 && k != N / 2) f *= pf;
+        const C x0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+        const C x1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
+        const long long o = Atab[k] + j;
+        if (j < L && (u < 8 || c0)) {
+          if (j + 1 < L) {
+            if (((a8 + o) & 1) == 0) {
+              float4 w;
+              w.x = (float)x0.x;
+              w.y = (float)x0.y;
+              w.z = (float)x1.x;
+              w.w = (float)x1.y;
+              *reinterpret_cast<float4*>(out + o) = w;
+            } else {
+              out[o] = x0;
+              out[o + 1] = x1;
+            }
+          } else {
+            out[o] = x0;
+          }
+        }
+      }
+    } else if constexpr (!SMEM_STORE) {
+      // direct C2C / C2R store from registers (line-major last stage)
 #pragma unroll
       for (int i = 0; i < LPT; ++i) {
         const int s = slot + SLOTS * i;
@@ -324,66 +576,24 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
           }
         }
       } else {
-        // transposed store: element (k, j) of the tile goes to Atab[k] + j;
-        // lanes take pairs (j, j+1) of one row k and store 16-byte vectors
-        // where the destination address allows it
+        // transposed store through shared memory: element (k, j) of the tile
+        // goes to Atab[k] + j; lanes take pairs (j, j+1) of one row k
         constexpr int PAIRS = LMAX >= 2 ? LMAX / 2 : 1;
         constexpr int TOTAL = PAIRS * NOUT;
-        // destination in 8-byte units: element o of an f32 complex buffer is
-        // 16-byte aligned when a8 + o is even (buffers are 8-byte aligned)
-        const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
-        if (KIND == P_C2C) {
-          // the pairs are aligned to 16 bytes in the destination: (2p, 2p+1)
-          // on an even row base, (2p-1, 2p) on an odd one, where lane p = 0
-          // stores the two unpaired ends 0 and 2*PAIRS-1 of the row
-          C* __restrict__ out = reinterpret_cast<C*>(A.out);
-          for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
-            const int p = idx & (PAIRS - 1);
-            const int k = idx / PAIRS;
-            const long long base = Atab[k];
-            const int j0 = 2 * p - (sizeof(R) == 4 ? (int)((a8 + base) & 1) : 0);
-            if (j0 >= 0) {
-              if (j0 >= L) continue;
-              const C v0 = scl(sm[j0 * SEQ + G::pad(k)], sc);
-              if (j0 + 1 < L) {  // row j0 + 1 exists only when the tile holds that line
-                const C v1 = scl(sm[(j0 + 1) * SEQ + G::pad(k)], sc);
-                if (sizeof(R) == 4) {
-                  float4 w;
-                  w.x = (float)v0.x;
-                  w.y = (float)v0.y;
-                  w.z = (float)v1.x;
-                  w.w = (float)v1.y;
-                  *reinterpret_cast<float4*>(out + base + j0) = w;
-                } else {
-                  out[base + j0] = v0;
-                  out[base + j0 + 1] = v1;
-                }
-              } else {
-                out[base + j0] = v0;
-              }
-            } else {
-              out[base] = scl(sm[G::pad(k)], sc);
-              constexpr int JE = 2 * PAIRS - 1;
-              if (JE < L) out[base + JE] = scl(sm[JE * SEQ + G::pad(k)], sc);
-            }
-          }
-        } else if (KIND == P_R2C) {
+        if (KIND == P_R2C) {
           C* __restrict__ out = reinterpret_cast<C*>(A.out);
           const bool weighted = A.post_mode == W_HALF_INTERIOR;
           for (int idx = tid; idx < TOTAL; idx += P2_THREADS) {
             const int j = 2 * (idx & (PAIRS - 1));
             const int k = idx / PAIRS;
             if (j >= L) continue;
-            C v0, v1;
-            {
-              const C* seq = sm + (j >> 1) * SEQ;
-              const C a = seq[G::pad(k)];
-              const C b = seq[G::pad((N - k) & (N - 1))];
-              R f = sc * R(0.5);
-              if (weighted && k != 0 && k != N / 2) f *= pf;
-              v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
-              v1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
-            }
+            const C* seq = sm + (j >> 1) * SEQ;
+            const C a = seq[G::pad(k)];
+            const C b = seq[G::pad((N - k) & (N - 1))];
+            R f = sc * R(0.5);
+            if (weighted && k != 0 && k != N / 2) f *= pf;
+            const C v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+            const C v1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
             const long long o = Atab[k] + j;
             if (j + 1 < L) {
               if (sizeof(R) == 4 && ((a8 + o) & 1) == 0) {
@@ -421,10 +631,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     ta = t1;
     t1 = t2;
     my_piece = next_piece;
-#pragma unroll
-    for (int i = 0; i < LPT; ++i)
-#pragma unroll
-      for (int m = 0; m < 8; ++m) v[i][m] = nv[i][m];
+    p2_finish<R, N, KIND, LPT, FH>(v, nraw, A, fc);
     // the next tile's first shared-memory write is preceded by a barrier
   }
 }
