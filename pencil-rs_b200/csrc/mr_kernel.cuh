@@ -348,6 +348,78 @@ __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const Til
   }
 }
 
+// Last stage with the transposed C2C store, from registers: item (g, jb) of
+// the stage transforms butterfly jb of the adjacent sequences 2g and 2g+1
+// (the same twiddles) and writes its outputs k = jb + r*NB of both lines as
+// one pair to Atab[k] + 2g, a 16-byte vector where aligned in f32.  The lanes
+// of a warp take consecutive g, so they cover whole runs of the destination
+// rows, and no natural-order round through shared memory is needed.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void mr_last_stage_xstore(const PassArgs& A, const TileAddr& ta,
+                                                     const typename Cx<R>::T* __restrict__ in,
+                                                     const typename Cx<R>::T* __restrict__ W, const long long* Atab) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int ST = G::NST - 1;
+  constexpr int RAD = G::RL.r[ST];
+  constexpr int NB = N / RAD;
+  constexpr int PAIRS = G::NSEQ / 2;
+  constexpr int TOT = PAIRS * NB;
+  constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
+  const int L = ta.lines;
+  const R sc = R(A.scale);
+  const C* __restrict__ tw = W + mr_tw_off(G::RL, ST);
+  C* __restrict__ out = reinterpret_cast<C*>(A.out);
+  const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
+#pragma unroll 1
+  for (int it = 0; it < ITER; ++it) {
+    const int item = threadIdx.x + it * MR_THREADS;
+    if (TOT % MR_THREADS != 0 && item >= TOT) break;
+    const int g = item % PAIRS;
+    const int jb = item / PAIRS;
+    C v0[RAD], v1[RAD];
+    const C* src0 = in + (2 * g) * G::SEQ;
+    const C* src1 = src0 + G::SEQ;
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) {
+      v0[r] = src0[G::pad(jb + r * NB)];
+      v1[r] = src1[G::pad(jb + r * NB)];
+    }
+#pragma unroll
+    for (int r = 1; r < RAD; ++r) {
+      const C w = tw[(r - 1) * NB + jb];  // k = jb, NS = NB
+      v0[r] = twmul<INV>(v0[r], w);
+      v1[r] = twmul<INV>(v1[r], w);
+    }
+    Bfly<C, RAD, INV>::run(v0);
+    Bfly<C, RAD, INV>::run(v1);
+    const int j = 2 * g;
+    if (j < L) {
+#pragma unroll
+      for (int r = 0; r < RAD; ++r) {
+        const long long o = Atab[jb + r * NB] + j;
+        const C x0 = scl(v0[r], sc);
+        if (j + 1 < L) {
+          const C x1 = scl(v1[r], sc);
+          if (sizeof(R) == 4 && ((a8 + o) & 1) == 0) {
+            float4 w4;
+            w4.x = (float)x0.x;
+            w4.y = (float)x0.y;
+            w4.z = (float)x1.x;
+            w4.w = (float)x1.y;
+            *reinterpret_cast<float4*>(out + o) = w4;
+          } else {
+            out[o] = x0;
+            out[o + 1] = x1;
+          }
+        } else {
+          out[o] = x0;
+        }
+      }
+    }
+  }
+}
+
 // Stores the natural-order results `res` of one tile (R2C direct, or any
 // transposed store; element (k, line j) of a transposed store goes to
 // Atab[k] + j, each thread writing the pair of lines (j, j+1), as one 16-byte
@@ -504,6 +576,14 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
     // stages 1 .. NST-2 in shared memory, the last one to HBM
     mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
     mr_last_stage_store<R, N, INV>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W);
+    return;
+  }
+  if (A.kind == P_C2C) {
+    // transposed C2C: the last stage stores from registers; with two stages no
+    // barrier follows the row-table writes above before it reads them
+    mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
+    if constexpr (G::NST == 2) __syncthreads();
+    mr_last_stage_xstore<R, N, INV>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab);
     return;
   }
   mr_stages_upto<R, N, INV, 1, G::NST>(b0, b1, W);
