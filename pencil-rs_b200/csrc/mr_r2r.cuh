@@ -36,18 +36,27 @@ struct R2rSource {
   }
 };
 
-// Stage-0 butterfly inputs of one tile (FFT input q of each pair).
-template <typename R, int N>
-__device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
-                                            const PassArgs& A, const TileAddr& ta) {
+// Line length n of kind SUB on an N-point FFT: N for the DHT and the type-II
+// and type-III kinds, N/2 + 1 for DCT-I, N/2 - 1 for DST-I.
+template <int N, int SUB>
+__host__ __device__ constexpr int r2r_len() {
+  return SUB == S_DCT1 ? N / 2 + 1 : (SUB == S_DST1 ? N / 2 - 1 : N);
+}
+
+// Stage-0 butterfly inputs of one tile (FFT input q of each pair), for the
+// kind SUB (a template parameter, so every index below is compile-time but
+// the butterfly index).
+template <typename R, int N, int SUB>
+__device__ __forceinline__ void mr_load_r2r_k(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                              const PassArgs& A, const TileAddr& ta) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int NB = G::NB0;
   constexpr int R0 = G::R0;
+  constexpr int n = r2r_len<N, SUB>();
+  constexpr int sub = SUB;
   const R zero = R(0);
   const int L = ta.lines;
-  const int n = A.n;
-  const int sub = A.sub;
   const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
 #pragma unroll
   for (int u = 0; u < G::U0; ++u) {
@@ -111,13 +120,33 @@ __device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>:
   }
 }
 
+template <typename R, int N>
+__device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                            const PassArgs& A, const TileAddr& ta) {
+  switch (A.sub) {
+    case S_DCT2: mr_load_r2r_k<R, N, S_DCT2>(v, A, ta); break;
+    case S_DST2: mr_load_r2r_k<R, N, S_DST2>(v, A, ta); break;
+    case S_DCT3: mr_load_r2r_k<R, N, S_DCT3>(v, A, ta); break;
+    case S_DST3: mr_load_r2r_k<R, N, S_DST3>(v, A, ta); break;
+    case S_DCT1:
+      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DCT1>(v, A, ta);
+      break;
+    case S_DST1:
+      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DST1>(v, A, ta);
+      break;
+    default: mr_load_r2r_k<R, N, S_DHT>(v, A, ta); break;
+  }
+}
+
 // Outputs k of both lines of a pair (x: first line / real part, y: second
 // line / imaginary part), from the natural-order FFT results `seq`.
-template <typename R, int N>
-__device__ __forceinline__ typename Cx<R>::T r2r_output(int sub, const typename Cx<R>::T* seq, int k, int n,
+template <typename R, int N, int SUB>
+__device__ __forceinline__ typename Cx<R>::T r2r_output(const typename Cx<R>::T* seq, int k,
                                                        const typename Cx<R>::T* __restrict__ aux0) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
+  constexpr int n = r2r_len<N, SUB>();
+  constexpr int sub = SUB;
   const R h = R(0.5);
   switch (sub) {
     case S_DCT2:
@@ -152,17 +181,16 @@ __device__ __forceinline__ typename Cx<R>::T r2r_output(int sub, const typename 
 
 // Post-processing and store of one tile: direct (transform axis contiguous
 // in the destination) or transposed through the row table.
-template <typename R, int N>
-__device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
-                                             const long long* Atab) {
+template <typename R, int N, int SUB>
+__device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
+                                               const long long* Atab) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int NSEQ = G::NSEQ;
   constexpr int SEQ = G::SEQ;
+  constexpr int n = r2r_len<N, SUB>();
   const int tid = threadIdx.x;
   const int L = ta.lines;
-  const int n = A.n_out;
-  const int sub = A.sub;
   const bool cplx = A.out_complex != 0;
   const R sc = R(A.scale);
   const R pf = R(A.post_factor);
@@ -179,7 +207,7 @@ __device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& 
       k = i / NSEQ;
     }
     if (cplx ? s >= L : 2 * s >= L) continue;
-    C v = r2r_output<R, N>(sub, res + s * SEQ, k, n, aux0);
+    C v = r2r_output<R, N, SUB>(res + s * SEQ, k, aux0);
     R f = sc;
     if (post_mode != W_NONE && weight_hit(post_mode, k, n)) f *= pf;
     v = scl(v, f);
@@ -198,6 +226,24 @@ __device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& 
         if (2 * s + 1 < L) out[o + 1] = v.y;
       }
     }
+  }
+}
+
+template <typename R, int N>
+__device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
+                                             const long long* Atab) {
+  switch (A.sub) {
+    case S_DCT2: mr_store_r2r_k<R, N, S_DCT2>(A, ta, res, Atab); break;
+    case S_DST2: mr_store_r2r_k<R, N, S_DST2>(A, ta, res, Atab); break;
+    case S_DCT3: mr_store_r2r_k<R, N, S_DCT3>(A, ta, res, Atab); break;
+    case S_DST3: mr_store_r2r_k<R, N, S_DST3>(A, ta, res, Atab); break;
+    case S_DCT1:
+      if constexpr (N % 2 == 0) mr_store_r2r_k<R, N, S_DCT1>(A, ta, res, Atab);
+      break;
+    case S_DST1:
+      if constexpr (N % 2 == 0) mr_store_r2r_k<R, N, S_DST1>(A, ta, res, Atab);
+      break;
+    default: mr_store_r2r_k<R, N, S_DHT>(A, ta, res, Atab); break;
   }
 }
 
