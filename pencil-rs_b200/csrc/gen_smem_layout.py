@@ -6,14 +6,18 @@ Element i of a sequence sits at s*SEQ + i + (i >> SH) (SH = 0: no padding).
 For every candidate (SH, SEQ) this script replays each shared-memory access of
 a tile -- the Stockham exchanges, the twiddle reads, the natural-order writes
 and the transposed or R2C-split reads of the store, for every pass kind and
-store mode -- warp by warp, and counts wavefronts with the bank model
+store mode (and the real-to-real kernel's), with the kernels' thread mappings
+-- warp by warp, and counts wavefronts with the bank model
 
-    wavefronts(access) = max(ceil(active lanes * E / 128),
-                             max over bank groups of distinct elements)
+    wavefronts(access) = sum over phases of max(1 if a lane is active,
+                                                max over bank groups of distinct elements)
 
-(E = 8 or 16 bytes per complex element: bank group = element mod 16 or mod 8;
-lanes reading the same element share it).  The layout with the fewest
-wavefronts summed over all kinds wins (the smaller SEQ on a tie).
+A phase is 128 bytes of lanes (16 lanes of 8-byte elements, 8 lanes of
+16-byte elements); bank group = element mod 16 or mod 8; lanes reading the
+same element share it.  This per-phase rule reproduces the shared-memory
+wavefronts ncu counts for the register kernel (1280 per 512-point tile, where
+balancing bank groups over the whole warp predicts 1024).  The layout with
+the fewest wavefronts summed over all kinds wins (the smaller SEQ on a tie).
 
 Run from this directory: ``python gen_smem_layout.py`` (a few minutes).
 The thread/sequence mappings replayed here are those of pow2_kernel.cu and
@@ -44,15 +48,17 @@ def wavefronts(idx: np.ndarray, E: int) -> int:
     """idx: (M, 32) element indices of M warp accesses, -1 for idle lanes."""
     M = idx.shape[0]
     G = 128 // E
-    s = np.sort(idx, axis=1)
+    P = 128 // E  # lanes per phase
+    sub = idx.reshape(M * (32 // P), P)
+    R = sub.shape[0]
+    s = np.sort(sub, axis=1)
     valid = s >= 0
     uniq = valid.copy()
     uniq[:, 1:] &= s[:, 1:] != s[:, :-1]
-    cnt = np.zeros((M, G), dtype=np.int64)
-    rows = np.broadcast_to(np.arange(M)[:, None], (M, 32))
+    cnt = np.zeros((R, G), dtype=np.int64)
+    rows = np.broadcast_to(np.arange(R)[:, None], (R, P))
     np.add.at(cnt, (rows[uniq], s[uniq] % G), 1)
-    minwf = -(-valid.sum(axis=1) * E // 128)
-    return int(np.maximum(cnt.max(axis=1), minwf).sum())
+    return int(np.maximum(cnt.max(axis=1), valid.any(axis=1)).sum())
 
 
 def loop_lanes(count: int) -> np.ndarray:
@@ -81,23 +87,42 @@ def p2_cost(N, rb, sh, SEQ, kind, direct):
     lead = 8 if log % 3 == 0 else (2 if log % 3 == 1 else 4)
     nst = log // 3 if log % 3 == 0 else log // 3 + 1
     tid = np.arange(THREADS).reshape(-1, 32)
-    slot, t = tid // T, tid % T
+    # thread mappings of pow2_kernel.cu: (sequence, butterfly) of each value set
+    last = "x" if (not direct and kind == "c2c") else ("r" if (not direct and kind == "r2c" and lpt == 2) else "m")
+    first_h = kind == "c2r" and lpt == 2
+
+    def mapping(which):
+        if which == "x":
+            g, b = tid % slots, tid // slots
+            return [(lpt * g + i, b) for i in range(lpt)]
+        if which in ("r", "h"):
+            if which == "r":
+                s, c = tid % nseq, tid // nseq
+            else:
+                s, c = tid // (T // 2), tid % (T // 2)
+            return [(s, c), (s, np.where(c == 0, T // 2, T - c))]
+        slot, t = tid // T, tid % T
+        return [(slot + slots * i, t) for i in range(lpt)]
+
     tot = 0
-    for st in range(nst - 1):
+    for st in range(nst - 1):  # exchange after stage st
         R = lead if st == 0 else 8
         NS = 1 if st == 0 else lead * 8 ** (st - 1)
-        for i in range(lpt):
-            base = (slot + slots * i) * SEQ
+        for sq, bf in mapping("h" if (st == 0 and first_h) else "m"):
             for q in range(8):
                 u, r = divmod(q, R)
-                jb = t + u * T
+                jb = bf + u * T
                 k = jb & (NS - 1)
-                tot += wavefronts(base + padded((jb - k) * R + k + r * NS, sh), E)
+                tot += wavefronts(sq * SEQ + padded((jb - k) * R + k + r * NS, sh), E)
+        for sq, bf in mapping(last if st + 1 == nst - 1 else "m"):
             for m in range(8):
-                tot += wavefronts(base + padded(t + T * m, sh), E)
+                tot += wavefronts(sq * SEQ + padded(bf + T * m, sh), E)
     H = N // 2 + 1
-    if direct and kind != "r2c":
+    # register stores (direct C2C/C2R, transposed C2C, transposed R2C at two
+    # sequences per thread) touch no shared memory after the last stage
+    if (direct and kind != "r2c") or last != "m":
         return tot
+    slot, t = tid // T, tid % T
     for i in range(lpt):
         base = (slot + slots * i) * SEQ
         for r in range(8):
@@ -120,14 +145,9 @@ def p2_cost(N, rb, sh, SEQ, kind, direct):
     Ia = np.where(act, I, 0)
     j = 2 * (Ia & (pairs - 1))
     k = Ia // pairs
-    if kind == "c2c":
-        tot += wavefronts(np.where(act, j * SEQ + padded(k, sh), -1), E)
-        tot += wavefronts(np.where(act, (j + 1) * SEQ + padded(k, sh), -1), E)
-    elif kind == "r2c":
-        tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded(k, sh), -1), E)
+    tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded(k, sh), -1), E)
+    if kind == "r2c":
         tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded((N - k) & (N - 1), sh), -1), E)
-    else:
-        tot += wavefronts(np.where(act, (j >> 1) * SEQ + padded(k, sh), -1), E)
     return tot
 
 
@@ -189,6 +209,8 @@ def mr_sched(N, nseq, rb):
 
 
 def mr_cost(N, rb, sh, SEQ, kind, direct):
+    if kind == "r2r":
+        return mr_r2r_cost(N, rb, sh, SEQ, direct)
     E = 2 * rb
     nseq = mr_nseq(N, rb)
     rad = mr_sched(N, nseq, rb)
@@ -198,9 +220,25 @@ def mr_cost(N, rb, sh, SEQ, kind, direct):
         NB = N // R
         B = loop_lanes(nseq * NB)
         act = B >= 0
-        s, jb = np.divmod(np.where(act, B, 0), NB)
-        k = jb % ns
         last_to_hbm = st == len(rad) - 1 and direct and kind != "r2c"
+        if st == 0 or last_to_hbm:  # butterfly-fastest (coalesced HBM side)
+            s, jb = np.divmod(np.where(act, B, 0), NB)
+        else:  # shared-memory stages: sequence-fastest
+            jb, s = np.divmod(np.where(act, B, 0), nseq)
+        k = jb % ns
+        if st == len(rad) - 1 and not direct and kind == "c2c":
+            # register store: item (g, jb) reads butterfly jb of sequences 2g, 2g+1
+            P = nseq // 2
+            I = loop_lanes(P * NB)
+            act = I >= 0
+            Ia = np.where(act, I, 0)
+            g, jb = Ia % P, Ia // P
+            for r in range(R):
+                for i in range(2):
+                    tot += wavefronts(np.where(act, (2 * g + i) * SEQ + padded(jb + r * NB, sh), -1), E)
+                if r > 0:
+                    tot += wavefronts(np.where(act, (r - 1) * ns + jb, -1), E)
+            return tot
         for r in range(R):
             if st > 0:
                 tot += wavefronts(np.where(act, s * SEQ + padded(jb + r * NB, sh), -1), E)
@@ -239,14 +277,54 @@ def mr_cost(N, rb, sh, SEQ, kind, direct):
     return tot
 
 
+def mr_r2r_cost(N, rb, sh, SEQ, direct):
+    """The real-to-real kernel on the same layout: every stage after stage 0 in
+    shared memory (sequence-fastest), then the store's reads, modelled on the
+    DHT's pair k, n - k (lanes over sequences for a transposed store, along k
+    for a direct one)."""
+    E = 2 * rb
+    nseq = mr_nseq(N, rb)
+    rad = mr_sched(N, nseq, rb)
+    tot = 0
+    ns = 1
+    for st, R in enumerate(rad):
+        NB = N // R
+        B = loop_lanes(nseq * NB)
+        act = B >= 0
+        if st == 0:
+            s, jb = np.divmod(np.where(act, B, 0), NB)
+        else:
+            jb, s = np.divmod(np.where(act, B, 0), nseq)
+        k = jb % ns
+        for r in range(R):
+            if st > 0:
+                tot += wavefronts(np.where(act, s * SEQ + padded(jb + r * NB, sh), -1), E)
+                if r > 0:
+                    tot += wavefronts(np.where(act, (r - 1) * ns + k, -1), E)
+            base = (jb - k) * R + k
+            tot += wavefronts(np.where(act, s * SEQ + padded(base + r * ns, sh), -1), E)
+        ns *= R
+    I = loop_lanes(nseq * N)
+    act = I >= 0
+    Ia = np.where(act, I, 0)
+    if direct:
+        p, k = Ia // N, Ia % N
+    else:
+        p, k = Ia % nseq, Ia // nseq
+    tot += wavefronts(np.where(act, p * SEQ + padded(k, sh), -1), E)
+    tot += wavefronts(np.where(act, p * SEQ + padded((N - k) % N, sh), -1), E)
+    return tot
+
+
 def best_layout(args):
     family, N, rb = args
     cost = p2_cost if family == "pow2" else mr_cost
+    kinds = KINDS if family == "pow2" else KINDS + [("r2r", False), ("r2r", True)]
     best = None
     for sh in SHIFTS:
         lo = padded(N - 1, sh) + 1
         for SEQ in range(lo, lo + 16):
-            c = sum(cost(N, rb, sh, SEQ, kind, direct) for kind, direct in KINDS)
+            c = sum(cost(N, rb, sh, SEQ, kind, direct) for kind, direct in kinds)
             key = (c, SEQ, sh)
             if best is None or key < best:
                 best = key

@@ -148,7 +148,9 @@ struct MRGeom {
 
 // Stockham stage ST >= 1 from shared buffer `in` to shared buffer `out`: for
 // butterfly jb of a sequence (k = jb mod NS), inputs jb + r*N/RAD times
-// W_N^{k*r*N/(NS*RAD)}, outputs (jb - k)*RAD + k + r*NS.
+// W_N^{k*r*N/(NS*RAD)}, outputs (jb - k)*RAD + k + r*NS.  Work item b is
+// butterfly b / NSEQ of sequence b % NSEQ: the lanes of a warp cover NSEQ
+// sequences at a few butterflies, so the twiddle reads are broadcasts.
 template <typename R, int N, int ST, bool INV>
 __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ in, typename Cx<R>::T* __restrict__ out,
                                          const typename Cx<R>::T* __restrict__ Wst) {
@@ -164,8 +166,8 @@ __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ i
   for (int it = 0; it < ITER; ++it) {
     const int b = threadIdx.x + it * MR_THREADS;
     if (TOT % MR_THREADS != 0 && b >= TOT) break;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = b % G::NSEQ;
+    const int jb = b / G::NSEQ;
     const int k = jb % NS;
     const C* src = in + s * G::SEQ;
     C* dst = out + s * G::SEQ;
