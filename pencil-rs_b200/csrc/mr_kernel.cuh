@@ -162,7 +162,7 @@ __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ i
   constexpr int TOT = G::NSEQ * NB;
   constexpr int ITER = (TOT + MR_THREADS - 1) / MR_THREADS;
   const C* __restrict__ tw = Wst + mr_tw_off(G::RL, ST);
-#pragma unroll 1
+#pragma unroll 2
   for (int it = 0; it < ITER; ++it) {
     const int b = threadIdx.x + it * MR_THREADS;
     if (TOT % MR_THREADS != 0 && b >= TOT) break;
@@ -317,7 +317,7 @@ __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const Til
   const int L = ta.lines;
   const R sc = R(A.scale);
   const C* __restrict__ tw = W + mr_tw_off(G::RL, ST);
-#pragma unroll 1
+#pragma unroll 2
   for (int it = 0; it < ITER; ++it) {
     const int b = threadIdx.x + it * MR_THREADS;
     if (TOT % MR_THREADS != 0 && b >= TOT) break;
@@ -373,7 +373,7 @@ __device__ __forceinline__ void mr_last_stage_xstore(const PassArgs& A, const Ti
   const C* __restrict__ tw = W + mr_tw_off(G::RL, ST);
   C* __restrict__ out = reinterpret_cast<C*>(A.out);
   const long long a8 = (long long)(reinterpret_cast<uintptr_t>(A.out) >> 3);
-#pragma unroll 1
+#pragma unroll 2
   for (int it = 0; it < ITER; ++it) {
     const int item = threadIdx.x + it * MR_THREADS;
     if (TOT % MR_THREADS != 0 && item >= TOT) break;
