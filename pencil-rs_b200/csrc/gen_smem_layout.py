@@ -185,6 +185,8 @@ def mr_nseq(N, rb):
     fit = (3072 if rb == 4 else 1536) // N
     if fit >= 64:
         return 64
+    if rb == 4 and N > 512:
+        return 4
     if fit < 2:
         return 2
     p = 1

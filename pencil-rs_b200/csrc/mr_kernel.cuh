@@ -126,7 +126,11 @@ template <typename R, int N>
 struct MRGeom {
   static constexpr int TILE_ELEMS = sizeof(R) == 4 ? 3072 : 1536;
   static constexpr int FIT = TILE_ELEMS / N;
-  static constexpr int NSEQ = FIT >= 64 ? 64 : (FIT < 2 ? 2 : mr_pow2floor(FIT));
+  // lengths above 512 (the 770-point DST-I FFT) would get 2 sequences, whose
+  // transposed store writes 16-byte runs per destination row: f32 takes 4
+  static constexpr int NSEQ = FIT >= 64 ? 64
+                              : (sizeof(R) == 4 && N > 512) ? 4
+                              : (FIT < 2 ? 2 : mr_pow2floor(FIT));
   // shared-memory layout (bank-conflict model of gen_smem_layout.py): element
   // i of sequence s at s*SEQ + pad(i)
   static constexpr SmemLayout LAY = mr_layout(N, (int)sizeof(R));

@@ -197,6 +197,10 @@ __device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr
   const int post_mode = A.post_mode;
   const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
   const bool direct = A.dst_k_contig != 0;
+  // destination in units of the real type: a pair at element o is aligned
+  // to its two-element vector when a4 + o is even (buffers are aligned to
+  // one element)
+  const long long a4 = (long long)(reinterpret_cast<uintptr_t>(A.out) / sizeof(R));
   for (int i = tid; i < NSEQ * n; i += MR_THREADS) {
     int s, k;
     if (direct) {
@@ -221,9 +225,15 @@ __device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr
         out[o] = v.x;
         if (2 * s + 1 < L) out[o + ta.dstb] = v.y;
       } else {
+        // the two lines of the pair are adjacent in the destination row: one
+        // vector store of both (the complex type) where aligned
         const long long o = Atab[k] + 2 * s;
-        out[o] = v.x;
-        if (2 * s + 1 < L) out[o + 1] = v.y;
+        if (2 * s + 1 < L && ((a4 + o) & 1) == 0) {
+          *reinterpret_cast<C*>(out + o) = v;
+        } else {
+          out[o] = v.x;
+          if (2 * s + 1 < L) out[o + 1] = v.y;
+        }
       }
     }
   }

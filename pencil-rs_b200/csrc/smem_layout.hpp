@@ -112,7 +112,7 @@ __host__ __device__ constexpr SmemLayout mr_layout(int N, int real_bytes) {
     case 500: return real_bytes == 4 ? SmemLayout{0, 500} : SmemLayout{2, 628};
     case 504: return real_bytes == 4 ? SmemLayout{3, 572} : SmemLayout{3, 572};
     case 512: return real_bytes == 4 ? SmemLayout{4, 548} : SmemLayout{3, 580};
-    case 770: return real_bytes == 4 ? SmemLayout{0, 776} : SmemLayout{0, 772};
+    case 770: return real_bytes == 4 ? SmemLayout{0, 780} : SmemLayout{0, 772};
     default: return SmemLayout{3, N + N / 8 + 1};
   }
 }
