@@ -1199,7 +1199,8 @@ static void row_pitch(Pencil& p, int elem_bytes) {
   if (p.split_of(inner) >= 0 || 32 % elem_bytes != 0) return;
   const long long per = 32 / elem_bytes;
   const long long n = p.shape[inner];
-  if (n % per != 0) p.pitch = (n + per - 1) / per * per;
+  // short rows are left alone: padding them would cost more than 1/8 of the layout
+  if (n % per != 0 && n >= 8 * per) p.pitch = (n + per - 1) / per * per;
 }
 
 static void build_program(pb_plan& P, int mode) {

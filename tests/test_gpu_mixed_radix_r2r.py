@@ -93,3 +93,28 @@ def test_r2r_vjp_adjoint_identity_f64_mixed_radix(kinds, cplx):
         lhs = _dot(to_host(ax), to_host(y))
         rhs = _dot(to_host(x), to_host(aty))
         assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (op, lhs, rhs)
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+def test_real_pairs_into_outputs_offset_by_one_element(rb):
+    """The transposed real-to-real store writes the two lines of a pair with one
+    vector store where the destination allows it; an output that starts one
+    element past that alignment must give the same bits (odd line counts
+    included: 7 rows per rank on the 2x3 grid)."""
+    torch.manual_seed(7)
+    dt = RDT[rb]
+    plan = pb.R2rPlan.from_shape(pb.MpiTopology((2, 3)), (14, 384, 21), (), ("DctII", "DstI", "Dht"), dtype=dt)
+    assert "mixed_radix" in plan.step_kernels(L.FORWARD)
+    x = torch.randn(plan.info.input_elems, dtype=dt, device="cuda")
+    ref = plan.allocate_output()
+    plan.forward(x, ref)
+    shifted = torch.zeros(plan.info.output_elems + 1, dtype=dt, device="cuda")[1:]
+    assert shifted.data_ptr() % (2 * shifted.element_size()) != 0
+    plan.forward(x, shifted)
+    back_ref = plan.allocate_input()
+    back = torch.zeros(plan.info.input_elems + 1, dtype=dt, device="cuda")[1:]
+    plan.inverse(ref, back_ref)
+    plan.inverse(ref, back)
+    torch.cuda.synchronize()
+    assert torch.equal(shifted, ref)
+    assert torch.equal(back, back_ref)
