@@ -109,6 +109,9 @@ cudaError_t launch_batch(const BatchArgs& B, int real_bytes, size_t smem, int gr
 int batch_occupancy(int real_bytes, size_t smem);
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int pow2_lines(int m, int kind, int real_bytes);
+bool pow2_half_supported(int m, int kind, int direct, int real_bytes);
+int pow2_half_lines(int m);
+int pow2_half_occupancy(int m, int kind);
 int pow2_occupancy(int m, int kind, int inv, int direct, int real_bytes);
 // real-to-real kinds on the mixed-radix kernel (mr_r2r.cuh), FFT lengths of
 // kMrR2rLengths

@@ -942,6 +942,9 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
           }
           g[A.a] = 0;
         }
+        // the half-length C2R kernel writes real lines as 8-byte pairs: their
+        // starts are even (N is even), checked here
+        if (A.half && ((ta_.dst0 | (long long)ta_.dstb) & 1)) fail(PB_EUNSUPPORTED);
         ++t;
       }
     }
@@ -964,6 +967,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int occ = A.fast == 3   ? mr_r2r_occupancy(A.m, P.real_bytes)
                     : A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
+                    : A.half      ? pow2_half_occupancy(A.m, A.kind)
                                   : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
     A.grid_ctas = sms * std::max(1, occ);
   }
@@ -1046,7 +1050,17 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
     if (direct || transposed) {
       A.fast = 1;
       A.dst_k_contig = direct ? 1 : 0;
-      L = pow2_lines(A.m, op.kind, P.real_bytes);
+      if (pow2_half_supported(A.m / 2, op.kind, direct ? 1 : 0, P.real_bytes)) {
+        // one real output line as an m/2-point complex sequence: 8-byte
+        // stores of the real lines, split twiddles W_N^c for c <= m/16
+        A.half = 1;
+        A.m /= 2;
+        A.twiddle = enc(roots_table(P, A.m));
+        A.aux0 = enc(phase_table(P, A.m / 16 + 1, -2, 0, 2.0L * A.m));
+        L = pow2_half_lines(A.m);
+      } else {
+        L = pow2_lines(A.m, op.kind, P.real_bytes);
+      }
       A.lines = L;
     }
   }

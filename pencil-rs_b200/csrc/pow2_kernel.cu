@@ -637,6 +637,220 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// Half-length C2R (f32, direct store).  One real output line x of N = 2M
+// points is the complex sequence z[n] = x[2n] + i x[2n+1] of M points, so it
+// stores as 8-byte pairs and every complex sequence of a tile is one line:
+//   Z'[k] = (X[k] + conj X[M-k]) + i W_N^-k (X[k] - conj X[M-k]),
+// with the imaginary parts of X[0] and X[M] dropped, is twice the DFT of z,
+// so the unnormalised inverse M-point FFT of Z' has the N-point scale and
+// gives x[2n] + i x[2n+1].  The first stage pairs butterflies c and T-c (0
+// and T/2 for c = 0, as P2_FIRST_H): both take the same 16 bins, c = 0 also
+// the real part of bin M.  Thread c's twiddles W_N^q are W_N^c W_16^m
+// (q = c + T m), W_16^{m+1} conj(W_N^c) (q = T - c + T m) and W_32 W_16^m
+// (q = T/2 + T m for c = 0); W_N^c comes from a table of T/2 + 1 entries
+// (aux0).  (The same split for R2C, with 8-byte stores of one line per
+// thread, was slower than the two-line pair store of pow2_kernel.)
+
+// W_16^u (negative exponent).
+__device__ __forceinline__ float2 p2h_w16(int u) {
+  return make_float2((float)kcos2pi(u, 16), (float)-ksin2pi(u, 16));
+}
+
+template <int M>
+__global__ void __launch_bounds__(P2_THREADS, 2) pow2_half_c2r_kernel(const PassArgs A) {
+  using R = float;
+  using C = float2;
+  using S = Sched<M>;
+  using G = P2Geom<R, M>;
+  constexpr int T = G::T;
+  constexpr int SLOTS = G::SLOTS;
+  constexpr int LPT = G::LPT;
+  constexpr int SEQ = G::SEQ;
+  constexpr int NST = S::NST;
+  static_assert(LPT == 2, "the half-length kernel pairs two butterflies per thread");
+  extern __shared__ __align__(16) unsigned char smem[];
+  C* sm = reinterpret_cast<C*>(smem);
+
+  if (A.gate != nullptr && *A.gate != 0) return;
+  const long long G0 = gridDim.x;
+  long long tile = blockIdx.x;
+  if (tile >= A.ntiles) return;
+  const int tid = threadIdx.x;
+  const int slot = tid / T;
+  const int t = tid - slot * T;
+  // first stage: line ps, butterflies pc and pb1
+  const int ps = tid / (T / 2);
+  const int pc = tid % (T / 2);
+  const bool c0 = pc == 0;
+  const int pb1 = c0 ? T / 2 : T - pc;
+  const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
+
+  const C* __restrict__ Wg = reinterpret_cast<const C*>(A.twiddle);
+  C tw[NST][7];
+#pragma unroll
+  for (int st = 1; st < NST; ++st) {
+    const int NS = S::ns(st);
+    const int k = t & (NS - 1);
+    const int step = M / (NS * 8);
+#pragma unroll
+    for (int r = 1; r < 8; ++r) tw[st][r - 1] = Wg[(k * r * step) & (M - 1)];
+  }
+#pragma unroll
+  for (int r = 0; r < 7; ++r) tw[0][r] = make_float2(1.f, 0.f);
+  const C wc = reinterpret_cast<const C*>(A.aux0)[pc];  // W_N^c
+  const C w32 = make_float2((float)kcos2pi(1, 32), (float)-ksin2pi(1, 32));
+
+  const R sc = R(A.scale);
+  const R wi = A.pre_mode == W_HALF_INTERIOR ? R(A.pre_factor) : R(1);
+  const bool vec_out = (reinterpret_cast<uintptr_t>(A.out) & 7) == 0;
+
+  // the 16 bins of the paired butterflies (a: c + T m, b: pb1 + T m) and,
+  // for c = 0, the real part of bin M, kept raw until the tile before is done
+  struct Raw {
+    C a[8], b[8];
+    R nm;
+  };
+  auto fetch = [&](Raw& raw, const TileAddr& ta) {
+    const C z = make_float2(0.f, 0.f);
+    const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+    const bool ok = ps < ta.lines;
+    const long long base = ta.src0 + (long long)ps * ta.srcb;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      raw.a[m] = ok ? in[base + pc + T * m] : z;
+      raw.b[m] = ok ? in[base + pb1 + T * m] : z;
+    }
+    raw.nm = (ok && c0) ? reinterpret_cast<const R*>(A.in)[2 * (base + M)] : 0.f;
+  };
+  auto finish = [&](C (&v)[2][8], const Raw& raw) {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      // bins q of set 0 (c + T m) and set 1 (pb1 + T m), and their mirrors M - q
+      C x0 = raw.a[m], x1 = raw.b[m];
+      C p0;
+      R w0 = wi, wp0 = wi;
+      if (m == 0) {
+        p0 = c0 ? make_float2(raw.nm, 0.f) : raw.b[7];
+        if (c0) {
+          x0.y = 0.f;  // bin 0
+          w0 = 1.f;
+          wp0 = 1.f;  // bin M
+        }
+      } else {
+        p0 = c0 ? raw.a[8 - m] : raw.b[7 - m];
+      }
+      C p1 = c0 ? raw.b[7 - m] : raw.a[7 - m];
+      x0 = scl(x0, w0);
+      p0 = scl(p0, wp0);
+      x1 = scl(x1, wi);
+      p1 = scl(p1, wi);
+      // W_N^-q
+      const C e = p2h_w16(m), e1 = p2h_w16(m + 1);
+      C wq0 = cmul(wc, e);
+      C wq1 = c0 ? cmul(w32, e) : cmul(e1, make_float2(wc.x, -wc.y));
+      wq0.y = -wq0.y;
+      wq1.y = -wq1.y;
+      auto comb = [](C x, C p, C w) {
+        const C E = make_float2(x.x + p.x, x.y - p.y);
+        const C O = cmul(w, make_float2(x.x - p.x, x.y + p.y));
+        return make_float2(E.x - O.y, E.y + O.x);
+      };
+      v[0][m] = comb(x0, p0, wq0);
+      v[1][m] = comb(x1, p1, wq1);
+    }
+  };
+
+  TileAddr ta = load_tile(tiles, tile);
+  C v[2][8];
+  {
+    Raw raw;
+    fetch(raw, ta);
+    finish(v, raw);
+  }
+  TileAddr t1 = ta;
+  if (tile + G0 < A.ntiles) t1 = load_tile(tiles, tile + G0);
+
+  for (;;) {
+    const bool has_next = tile + G0 < A.ntiles;
+    TileAddr t2 = t1;
+    Raw nraw;
+    if (has_next) {
+      fetch(nraw, t1);
+      if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
+    }
+    const int L = ta.lines;
+
+#pragma unroll
+    for (int st = 0; st < NST; ++st) {
+      if (st > 0) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const C* seq = sm + (slot + SLOTS * i) * SEQ;
+#pragma unroll
+          for (int m = 0; m < 8; ++m) v[i][m] = seq[G::pad(t + T * m)];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        switch (st) {
+          case 0: p2_bfly8<C, M, 0, true>(v[i], tw[0]); break;
+          case 1: p2_bfly8<C, M, (NST > 1 ? 1 : 0), true>(v[i], tw[st]); break;
+          case 2: p2_bfly8<C, M, (NST > 2 ? 2 : 0), true>(v[i], tw[st]); break;
+          default: p2_bfly8<C, M, (NST > 3 ? 3 : 0), true>(v[i], tw[st]); break;
+        }
+      }
+      if (st + 1 < NST) {
+        __syncthreads();  // every thread has read the buffer (previous stage or tile)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          C* seq = sm + (st == 0 ? ps : slot + SLOTS * i) * SEQ;
+          const int bf = st == 0 ? (i == 0 ? pc : pb1) : t;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            int o;
+            switch (st) {
+              case 0: o = p2_out_index<M, 0>(bf, q); break;
+              case 1: o = p2_out_index<M, (NST > 1 ? 1 : 0)>(bf, q); break;
+              default: o = p2_out_index<M, (NST > 2 ? 2 : 0)>(bf, q); break;
+            }
+            seq[G::pad(o)] = v[i][q];
+          }
+        }
+        __syncthreads();
+      }
+    }
+
+    // direct store: sequence slot + SLOTS i is line slot + SLOTS i; z[n]
+    // gives x[2n], x[2n+1]
+    R* __restrict__ out = reinterpret_cast<R*>(A.out);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int sq = slot + SLOTS * i;
+      if (sq < L) {
+        const long long b0 = ta.dst0 + (long long)sq * ta.dstb + 2 * t;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const long long o = b0 + 2 * T * r;
+          const C z = v[i][r];
+          if (vec_out) {
+            *reinterpret_cast<float2*>(out + o) = make_float2(z.x * sc, z.y * sc);
+          } else {
+            out[o] = z.x * sc;
+            out[o + 1] = z.y * sc;
+          }
+        }
+      }
+    }
+
+    if (!has_next) break;
+    tile += G0;
+    ta = t1;
+    t1 = t2;
+    finish(v, nraw);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host-side dispatch
 // ---------------------------------------------------------------------------
 template <typename R, int N>
@@ -750,9 +964,71 @@ int pow2_lines(int m, int kind, int real_bytes) {
   return real_bytes == 4 ? p2_lines_r<float>(m, kind) : p2_lines_r<double>(m, kind);
 }
 
+template <int M>
+static size_t p2h_smem() {
+  return (size_t)P2Geom<float, M>::NSEQ * P2Geom<float, M>::SEQ * sizeof(float2);
+}
+
+template <int M>
+static cudaError_t p2h_launch(const PassArgs& A, cudaStream_t stream) {
+  const size_t smem = p2h_smem<M>();
+  auto fn = pow2_half_c2r_kernel<M>;
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
+  if (grid > A.ntiles) grid = A.ntiles;
+  fn<<<dim3((unsigned)grid), P2_THREADS, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+template <int M>
+static int p2h_occ() {
+  int blocks = 0;
+  auto fn = pow2_half_c2r_kernel<M>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2h_smem<M>()) != cudaSuccess)
+    return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, P2_THREADS, p2h_smem<M>()) != cudaSuccess) return 1;
+  return blocks > 0 ? blocks : 1;
+}
+
+// The half-length C2R kernel: FFT length m = N/2 in 64..512, direct store, f32.
+bool pow2_half_supported(int m, int kind, int direct, int real_bytes) {
+  return real_bytes == 4 && m >= 64 && m <= 512 && (m & (m - 1)) == 0 && kind == P_C2R && direct;
+}
+
+int pow2_half_lines(int m) {
+  switch (m) {
+    case 64: return P2Geom<float, 64>::NSEQ;
+    case 128: return P2Geom<float, 128>::NSEQ;
+    case 256: return P2Geom<float, 256>::NSEQ;
+    default: return P2Geom<float, 512>::NSEQ;
+  }
+}
+
+int pow2_half_occupancy(int m, int kind) {
+  (void)kind;
+  switch (m) {
+    case 64: return p2h_occ<64>();
+    case 128: return p2h_occ<128>();
+    case 256: return p2h_occ<256>();
+    default: return p2h_occ<512>();
+  }
+}
+
+static cudaError_t p2h_dispatch(const PassArgs& A, cudaStream_t stream) {
+  switch (A.m) {
+    case 64: return p2h_launch<64>(A, stream);
+    case 128: return p2h_launch<128>(A, stream);
+    case 256: return p2h_launch<256>(A, stream);
+    case 512: return p2h_launch<512>(A, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_pow2(const PassArgs& A, int real_bytes, cudaStream_t stream) {
   if (A.ntiles <= 0) return cudaSuccess;
   if (A.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if (A.half) return (real_bytes == 4 && A.kind == P_C2R) ? p2h_dispatch(A, stream) : cudaErrorInvalidValue;
   return real_bytes == 4 ? p2_dispatch<float>(A, stream) : p2_dispatch<double>(A, stream);
 }
 

@@ -415,20 +415,22 @@ def test_pow2_register_kernel_c2c_and_r2c(rb, dims, shape, extra):
         check_transform(plan, route, spec, e, rb, True, d)
 
 
+@pytest.mark.parametrize("n", [64, 256])
 @pytest.mark.parametrize("rb", [4, 8])
 @pytest.mark.parametrize("family", ["r2c", "c2r", "c2c"])
-def test_pow2_vjp_adjoint_identity(family, rb):
-    """<A x, y> = <x, A^T y> through the register kernel, whose real-to-complex
-    and complex-to-real adjoints weight the interior bins.  f32: within
-    1e-5 * |A x| * |y|; f64: within 1e-10 * max(1, |<A x, y>|)."""
+def test_pow2_vjp_adjoint_identity(family, rb, n):
+    """<A x, y> = <x, A^T y> through the register kernels, whose real-to-complex
+    and complex-to-real adjoints weight the interior bins (n = 256 takes the
+    half-length real kernels in f32).  f32: within 1e-5 * |A x| * |y|; f64:
+    within 1e-10 * max(1, |<A x, y>|)."""
     rng = np.random.default_rng(11)
     topo = pb.MpiTopology((2, 2))
     if family == "r2c":
-        plan = pb.R2cPlan.from_shape(topo, (32, 64, 64), (), dtype=RDT[rb])
+        plan = pb.R2cPlan.from_shape(topo, (32, 64, n), (), dtype=RDT[rb])
     elif family == "c2r":
-        plan = pb.C2rPlan.from_shape(topo, (33, 64, 32), 64, (), dtype=RDT[rb])
+        plan = pb.C2rPlan.from_shape(topo, (n // 2 + 1, 64, 32), n, (), dtype=RDT[rb])
     else:
-        plan = pb.C2cPlan.from_shape(topo, (32, 64, 128), (), dtype=CDT[rb])
+        plan = pb.C2cPlan.from_shape(topo, (32, 64, 2 * n), (), dtype=CDT[rb])
 
     def rnd(n, dtype):
         if dtype.is_complex:
