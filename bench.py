@@ -313,7 +313,8 @@ def b200_arm(args):
     kinds_f = plan.step_kinds(L.FORWARD)
     kinds_i = plan.step_kinds(L.INVERSE)
     families = sorted(set(plan.step_kernels(L.FORWARD) + plan.step_kernels(L.INVERSE)) - {"check"})
-    kernel_names = ", ".join({"pow2": "pb::pow2_kernel<float, 512, kind, sign, store>",
+    kernel_names = ", ".join({"pow2": "pb::pow2_kernel<float, 512, kind, sign, store> (R2C, C2C), "
+                                      "pb::pow2_half_c2r_kernel<256> (C2R)",
                               "mixed_radix": "pb::mr_kernel<float, N>",
                               "generic": "pb::pass_kernel<float>"}[f] for f in families)
     fwd_t, inv_t = [], []
