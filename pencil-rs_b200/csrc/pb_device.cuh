@@ -57,7 +57,7 @@ __device__ __forceinline__ TileAddr load_tile(const TileAddr* tab, long long t) 
   a.srcb = (int)(r1.x & 0xffffffffLL);
   a.dstb = (int)(r1.x >> 32);
   a.lines = (int)(r1.y & 0xffffffffLL);
-  a.pad = 0;
+  a.srcq = (int)(r1.y >> 32);
   return a;
 }
 

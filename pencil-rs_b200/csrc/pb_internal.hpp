@@ -124,7 +124,7 @@ struct TileAddr {
   int srcb;        // line-to-line stride in the source
   int dstb;        // line-to-line stride in the destination (direct store)
   int lines;       // lines in this tile
-  int pad;
+  int srcq;        // stride of the transform axis in the source when the lines are strided (0: contiguous)
 };
 
 // Destination row of one piece (virtual rank) of the transform axis.

@@ -921,7 +921,11 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
         ta_.src0 = hs.offset(e, g, &r);
         ta_.srcb = (int)hs.stride[r][A.b];
         ta_.lines = c.y;
-        ta_.pad = 0;
+        ta_.srcq = 0;
+        if (!A.src_k_contig) {  // strided lines (the register kernel's transposed load)
+          if (hs.stride[r][A.a] > INT_MAX) fail(PB_EUNSUPPORTED);
+          ta_.srcq = (int)hs.stride[r][A.a];
+        }
         if (direct) {
           ta_.dst0 = hd.offset(e, g, &r);
           ta_.dstb = (int)hd.stride[r][A.b];
@@ -1042,11 +1046,16 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   // destination either with the same property (direct) or with the tile axis
   // innermost and unsplit (transposed store)
   const bool pow2 = !P.force_generic && A.m >= 32 && A.m <= 2048 && (A.m & (A.m - 1)) == 0;
-  if ((op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && pow2 && src.perm[N - 1] == a &&
-      src.split_of(a) < 0) {
+  // strided lines (permute_dims = false): the tile's lines are consecutive along
+  // the source's innermost axis, which the register kernel loads across lines
+  // (the tile axis may be split in either layout: the chunks are cut at both
+  // partitions of it, and the row tables are built per tile)
+  const bool src_strided = (op.kind == P_C2C || op.kind == P_R2C) && src.perm[N - 1] == b && b != a;
+  if ((op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && pow2 &&
+      (src.perm[N - 1] == a || src_strided) && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
-    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
     if (direct || transposed) {
       A.fast = 1;
       A.dst_k_contig = direct ? 1 : 0;

@@ -84,6 +84,10 @@ __device__ __forceinline__ int p2_out_index(int t, int q) {
 //    the last stage sits in butterfly k mod T, so the thread holds both Z[k]
 //    and Z[N-k] of every k it outputs and splits the two real lines in
 //    registers.
+//  * P2_FIRST_X (strided lines, C2C and R2C): g = tid % SLOTS, b = tid / SLOTS;
+//    sequences LPT*g + i, butterfly b.  The lines of a tile are consecutive
+//    along the source's innermost axis, so the lanes of a warp load runs of
+//    adjacent lines at each position of the (strided) transform axis.
 //  * P2_FIRST_H (C2R, LPT = 2): s = tid / (T/2), c = tid % (T/2); sequence s,
 //    butterflies c and T - c (0 and T/2 for c = 0).  Input q of the first
 //    stage sits in butterfly q mod T; the Hermitian extension reads bin q or
@@ -93,6 +97,7 @@ enum { P2_LAST_NAT = 0, P2_LAST_X = 1, P2_LAST_R = 2 };
 
 template <typename R, int N, int KIND, bool DIRECT>
 struct P2Modes {
+  // (P2_FIRST_X is the SX template flag of the kernel)
   static constexpr int LPT = P2Geom<R, N>::LPT;
   static constexpr int LAST = (!DIRECT && KIND == P_C2C) ? P2_LAST_X
                               : ((!DIRECT && KIND == P_R2C && LPT == 2) ? P2_LAST_R : P2_LAST_NAT);
@@ -114,7 +119,7 @@ struct P2Raw<R, KIND, LPT, true> {
   R nx, ny;
 };
 
-template <typename R, int N, int KIND, int LPT, bool FH>
+template <typename R, int N, int KIND, int LPT, bool FH, bool SX>
 __device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const PassArgs& A, const TileAddr& ta,
                                          int slot, int t) {
   using C = typename Cx<R>::T;
@@ -123,7 +128,27 @@ __device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const Pas
   const R zero = R(0);
   const C z = mk<C, R>(zero, zero);
   const int L = ta.lines;
-  if constexpr (FH) {
+  if constexpr (SX) {
+    // slot/t are g and b: sequences LPT*g + i, inputs b + T*m along the
+    // strided axis (stride srcq), adjacent lines srcb apart
+    const int g = slot, b = t;
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int sq = LPT * g + i;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const long long q = (long long)(b + T * m) * ta.srcq;
+        if constexpr (KIND == P_C2C) {
+          const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+          raw.a[i][m] = sq < L ? in[ta.src0 + (long long)sq * ta.srcb + q] : z;
+        } else {  // P_R2C: lines 2sq and 2sq + 1 packed as x + iy
+          const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+          const long long o = ta.src0 + (long long)(2 * sq) * ta.srcb + q;
+          raw.a[i][m] = mk<C, R>(2 * sq < L ? in[o] : zero, 2 * sq + 1 < L ? in[o + ta.srcb] : zero);
+        }
+      }
+    }
+  } else if constexpr (FH) {
     // slot/t are the mirror-paired sequence and butterfly c
     const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
     const int s = slot, c = t;
@@ -283,7 +308,7 @@ __device__ __forceinline__ void p2_mirror_tw(C (&w1)[7], const C (&w0)[7], bool 
   }
 }
 
-template <typename R, int N, int KIND, bool INV, bool DIRECT>
+template <typename R, int N, int KIND, bool INV, bool DIRECT, bool SX>
 __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
   using S = Sched<N>;
@@ -315,9 +340,10 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   // middle stages (line-major)
   const int slot = tid / T;
   const int t = tid - slot * T;
-  // first stage
-  const int fs = FH ? tid / (T / 2) : slot;
-  const int fc = FH ? tid % (T / 2) : t;
+  // first stage (SX: g = tid % SLOTS, b = tid / SLOTS)
+  static_assert(!(SX && FH), "strided C2R lines take the generic kernel");
+  const int fs = FH ? tid / (T / 2) : (SX ? tid % SLOTS : slot);
+  const int fc = FH ? tid % (T / 2) : (SX ? tid / SLOTS : t);
   // last stage
   int lseq[LPT], lbf[LPT];
 #pragma unroll
@@ -365,7 +391,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   C v[LPT][8];
   {
     P2Raw<R, KIND, LPT, FH> raw;
-    p2_fetch<R, N, KIND, LPT, FH>(raw, A, ta, fs, fc);
+    p2_fetch<R, N, KIND, LPT, FH, SX>(raw, A, ta, fs, fc);
     p2_finish<R, N, KIND, LPT, FH>(v, raw, A, fc);
   }
   TileAddr t1 = ta;
@@ -379,7 +405,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
     PieceAddr next_piece{0, 0};
     P2Raw<R, KIND, LPT, FH> nraw;
     if (has_next) {
-      p2_fetch<R, N, KIND, LPT, FH>(nraw, A, t1, fs, fc);
+      p2_fetch<R, N, KIND, LPT, FH, SX>(nraw, A, t1, fs, fc);
       if (tile + 2 * G0 < A.ntiles) t2 = load_tile(tiles, tile + 2 * G0);
       if (tid < npieces) next_piece = pieces[(tile + G0) * npieces + tid];
     }
@@ -415,8 +441,8 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 #pragma unroll
         for (int i = 0; i < LPT; ++i) {
           const bool first = st == 0;
-          C* seq = sm + (first ? (FH ? fs : slot + SLOTS * i) : slot + SLOTS * i) * SEQ;
-          const int bf = first && FH ? (i == 0 ? fc : (fc == 0 ? T / 2 : T - fc)) : t;
+          C* seq = sm + (first ? (FH ? fs : (SX ? LPT * fs + i : slot + SLOTS * i)) : slot + SLOTS * i) * SEQ;
+          const int bf = first && FH ? (i == 0 ? fc : (fc == 0 ? T / 2 : T - fc)) : ((first && SX) ? fc : t);
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
             int o;
@@ -869,7 +895,10 @@ static size_t p2_smem(int kind) {
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
 static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
   const size_t smem = p2_smem<R, N>(KIND);
-  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT>;
+  // strided source lines: C2C and R2C only (C2R lines are planned contiguous)
+  constexpr bool SXOK = KIND != P_C2R;
+  auto fn = (SXOK && A.src_k_contig == 0) ? pow2_kernel<R, N, KIND, INV, DIRECT, SXOK>
+                                          : pow2_kernel<R, N, KIND, INV, DIRECT, false>;
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
@@ -925,7 +954,7 @@ static int p2_lines_r(int m, int kind) {
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
 static int p2_occ() {
   int blocks = 0;
-  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT>;
+  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT, false>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2_smem<R, N>(KIND)) != cudaSuccess)
     return 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, P2_THREADS, p2_smem<R, N>(KIND)) != cudaSuccess)

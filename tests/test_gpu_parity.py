@@ -415,6 +415,38 @@ def test_pow2_register_kernel_c2c_and_r2c(rb, dims, shape, extra):
         check_transform(plan, route, spec, e, rb, True, d)
 
 
+STRIDED_CASES = [((2, 2), (64, 128, 32), (2,)), ((2, 4), (128, 64, 256), ()), ((3, 2), (32, 512, 64), ()),
+                 ((2, 3), (33, 64, 96), ())]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape,extra", STRIDED_CASES)
+def test_pow2_strided_lines_match_oracle(rb, dims, shape, extra):
+    """permute_dims = false keeps every stage's memory order, so most lines are
+    strided; power-of-two passes load them across the tile's adjacent lines.
+    The grids split the innermost axis, so tiles meet rank edges on both
+    sides."""
+    from pencil_b200 import _lib as L
+    rng = np.random.default_rng(12)
+    topo = pb.MpiTopology(dims)
+    e = int(np.prod(extra)) if extra else 1
+    lay = pb.DistributedLayout(False)
+    plan = pb.C2cPlan.from_shape(topo, shape, extra, layout=lay, dtype=CDT[rb])
+    assert "pow2" in plan.step_kernels(L.FORWARD)
+    route = po.c2c_route(po.Topology(dims), shape, None, False)
+    x = rand_field(rng, shape, extra, True, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, e, rb, True, d)
+    plan = pb.R2cPlan.from_shape(topo, shape, extra, layout=lay, dtype=RDT[rb])
+    route = po.r2c_route(po.Topology(dims), shape, None, False)
+    x = rand_field(rng, shape, extra, False, rb)
+    check_transform(plan, route, x, e, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), (e,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, e, rb, True, d)
+
+
 @pytest.mark.parametrize("n", [64, 256])
 @pytest.mark.parametrize("rb", [4, 8])
 @pytest.mark.parametrize("family", ["r2c", "c2r", "c2c"])
