@@ -84,7 +84,7 @@ struct PassArgs {
   double post_factor;
   double scale;
   int src_k_contig;  // transform axis has unit stride in the source
-  int dst_k_contig;  // transform axis has unit stride in the destination
+  int dst_k_contig;  // transform axis has unit stride in the destination (register kernel: 2 = and is split across ranks)
   int fast;          // 1: power-of-two kernel (pow2_kernel.cu), 2: mixed-radix (mr_kernel.cuh), 3: its R2R kinds (mr_r2r.cuh)
   int half;          // fast == 1, C2R: one real line as an m-point complex sequence (m = N/2; aux0 = W_N^c, c <= m/16)
   int nstages;

@@ -896,7 +896,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
                               const std::vector<int2>& chunks) {
   HostLayout hs(src, P.extra), hd(dst, P.extra);
   const int N = src.N;
-  const bool direct = A.dst_k_contig != 0;
+  const bool direct = A.dst_k_contig == 1;  // 2: direct store split into pieces
   const int ta = dst.split_of(A.a);
   const int npieces = direct ? 1 : (ta >= 0 ? dst.grid[ta] : 1);
   const long long nout = dst.shape[A.a];
@@ -942,7 +942,8 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
             }
             g[A.a] = st;
             pa.rowbase = hd.offset(e, g, &r);
-            pa.stride = hd.stride[r][A.a];
+            // transposed store: stride of k; split direct store: stride between lines
+            pa.stride = A.dst_k_contig == 2 ? hd.stride[r][A.b] : hd.stride[r][A.a];
           }
           g[A.a] = 0;
         }
@@ -972,7 +973,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
     const int occ = A.fast == 3   ? mr_r2r_occupancy(A.m, P.real_bytes)
                     : A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
                     : A.half      ? pow2_half_occupancy(A.m, A.kind)
-                                  : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig, P.real_bytes);
+                                  : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig == 1, P.real_bytes);
     A.grid_ctas = sms * std::max(1, occ);
   }
 }
@@ -1056,9 +1057,13 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
     const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
-    if (direct || transposed) {
+    // the transform axis contiguous in the destination but split across its
+    // ranks: a direct store whose row base and line stride follow the piece
+    const bool dsplit = !direct && dst.perm[N - 1] == a && ta >= 0 && dst.grid[ta] <= 64 &&
+                        (op.kind == P_C2C || op.kind == P_R2C);
+    if (direct || transposed || dsplit) {
       A.fast = 1;
-      A.dst_k_contig = direct ? 1 : 0;
+      A.dst_k_contig = direct ? 1 : (dsplit ? 2 : 0);
       if (pow2_half_supported(A.m / 2, op.kind, direct ? 1 : 0, P.real_bytes)) {
         // one real output line as an m/2-point complex sequence: 8-byte
         // stores of the real lines, split twiddles W_N^c for c <= m/16

@@ -308,12 +308,15 @@ __device__ __forceinline__ void p2_mirror_tw(C (&w1)[7], const C (&w0)[7], bool 
   }
 }
 
-template <typename R, int N, int KIND, bool INV, bool DIRECT, bool SX>
+// DSPLIT: the transform axis is contiguous in the destination but split
+// across its ranks: a direct store whose row base (per k) and line stride come
+// from the piece that k falls in (Atab, Jtab).
+template <typename R, int N, int KIND, bool INV, bool DIRECT, bool SX, bool DSPLIT>
 __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   using C = typename Cx<R>::T;
   using S = Sched<N>;
   using G = P2Geom<R, N>;
-  using MD = P2Modes<R, N, KIND, DIRECT>;
+  using MD = P2Modes<R, N, KIND, DIRECT || DSPLIT>;
   constexpr int T = G::T;
   constexpr int SLOTS = G::SLOTS;
   constexpr int LPT = G::LPT;
@@ -325,12 +328,15 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   constexpr int NST = S::NST;
   constexpr int LAST = MD::LAST;
   constexpr bool FH = MD::FIRST_H;
-  constexpr bool SMEM_STORE = !(DIRECT && KIND != P_R2C) && LAST == P2_LAST_NAT;
+  constexpr bool DLIKE = DIRECT || DSPLIT;  // line-major outputs, coalesced along k
+  constexpr bool SMEM_STORE = !(DLIKE && KIND != P_R2C) && LAST == P2_LAST_NAT;
+  static_assert(!DSPLIT || (!DIRECT && KIND != P_C2R), "split direct stores: C2C and R2C");
   extern __shared__ __align__(16) unsigned char smem[];
   C* sm = reinterpret_cast<C*>(smem);
   long long* Atab = reinterpret_cast<long long*>(sm + NSEQ * SEQ);
   int2* ktab = reinterpret_cast<int2*>(Atab + NOUT);
   PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + NOUT);
+  long long* Jtab = reinterpret_cast<long long*>(prow + P2_MAX_PIECES);
 
   if (A.gate != nullptr && *A.gate != 0) return;
   const long long G0 = gridDim.x;
@@ -461,7 +467,12 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
           for (int k = tid; k < NOUT; k += P2_THREADS) {
             const int2 kp = ktab[k];
             const PieceAddr pa = prow[kp.x];
-            Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+            if (DSPLIT) {
+              Atab[k] = pa.rowbase + kp.y;
+              Jtab[k] = pa.stride;
+            } else {
+              Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+            }
           }
         }
       }
@@ -473,7 +484,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 
     // the row table is written after the first exchange; with two stages no
     // barrier follows that before the register stores read it
-    if constexpr (LAST != P2_LAST_NAT && NST == 2) __syncthreads();
+    if constexpr ((LAST != P2_LAST_NAT || DSPLIT) && NST == 2) __syncthreads();
     if constexpr (LAST == P2_LAST_X) {
       // lines j0 .. j0+LPT-1 of rows k = b + T*r, straight from registers
       C* __restrict__ out = reinterpret_cast<C*>(A.out);
@@ -555,7 +566,16 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
 #pragma unroll
       for (int i = 0; i < LPT; ++i) {
         const int s = slot + SLOTS * i;
-        if (KIND == P_C2C) {
+        if (DSPLIT) {  // C2C
+          if (s < L) {
+            C* __restrict__ out = reinterpret_cast<C*>(A.out);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+              const int k = t + T * r;
+              out[Atab[k] + (long long)s * Jtab[k]] = scl(v[i][r], sc);
+            }
+          }
+        } else if (KIND == P_C2C) {
           if (s < L) {
             C* __restrict__ out = reinterpret_cast<C*>(A.out);
             const long long base = ta.dst0 + (long long)s * ta.dstb + t;
@@ -585,7 +605,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
         for (int r = 0; r < 8; ++r) seq[G::pad(t + T * r)] = v[i][r];
       }
       __syncthreads();
-      if (KIND == P_R2C && DIRECT) {
+      if (KIND == P_R2C && DLIKE) {
         C* __restrict__ out = reinterpret_cast<C*>(A.out);
 #pragma unroll
         for (int i = 0; i < LPT; ++i) {
@@ -596,9 +616,11 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
             const C b = seq[G::pad((N - k) & (N - 1))];
             R f = sc * R(0.5);
             if (A.post_mode == W_HALF_INTERIOR && k != 0 && k != N / 2) f *= pf;
-            if (2 * s < L) out[ta.dst0 + (long long)(2 * s) * ta.dstb + k] = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
-            if (2 * s + 1 < L)
-              out[ta.dst0 + (long long)(2 * s + 1) * ta.dstb + k] = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
+            const long long o0 = DSPLIT ? Atab[k] + (long long)(2 * s) * Jtab[k]
+                                        : ta.dst0 + (long long)(2 * s) * ta.dstb + k;
+            const long long ls = DSPLIT ? Jtab[k] : (long long)ta.dstb;
+            if (2 * s < L) out[o0] = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+            if (2 * s + 1 < L) out[o0 + ls] = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
           }
         }
       } else {
@@ -888,17 +910,17 @@ static int p2_lines(int kind) {
 template <typename R, int N>
 static size_t p2_smem(int kind) {
   const int nout = (kind == P_R2C) ? N / 2 + 1 : N;
-  return (size_t)P2Geom<R, N>::NSEQ * P2Geom<R, N>::SEQ * sizeof(typename Cx<R>::T) + (size_t)nout * 16 +
+  return (size_t)P2Geom<R, N>::NSEQ * P2Geom<R, N>::SEQ * sizeof(typename Cx<R>::T) + (size_t)nout * 24 +
          (size_t)P2_MAX_PIECES * sizeof(PieceAddr);
 }
 
-template <typename R, int N, int KIND, bool INV, bool DIRECT>
+template <typename R, int N, int KIND, bool INV, bool DIRECT, bool DSPLIT = false>
 static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
   const size_t smem = p2_smem<R, N>(KIND);
   // strided source lines: C2C and R2C only (C2R lines are planned contiguous)
   constexpr bool SXOK = KIND != P_C2R;
-  auto fn = (SXOK && A.src_k_contig == 0) ? pow2_kernel<R, N, KIND, INV, DIRECT, SXOK>
-                                          : pow2_kernel<R, N, KIND, INV, DIRECT, false>;
+  auto fn = (SXOK && A.src_k_contig == 0) ? pow2_kernel<R, N, KIND, INV, DIRECT, SXOK, DSPLIT>
+                                          : pow2_kernel<R, N, KIND, INV, DIRECT, false, DSPLIT>;
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
@@ -909,13 +931,18 @@ static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
 
 template <typename R, int N>
 static cudaError_t p2_dispatch_n(const PassArgs& A, cudaStream_t stream) {
-  const bool direct = A.dst_k_contig != 0;
+  const bool direct = A.dst_k_contig == 1;
+  const bool dsplit = A.dst_k_contig == 2;
   switch (A.kind) {
     case P_C2C:
+      if (dsplit)
+        return A.inv ? p2_launch<R, N, P_C2C, true, false, true>(A, stream)
+                     : p2_launch<R, N, P_C2C, false, false, true>(A, stream);
       if (A.inv)
         return direct ? p2_launch<R, N, P_C2C, true, true>(A, stream) : p2_launch<R, N, P_C2C, true, false>(A, stream);
       return direct ? p2_launch<R, N, P_C2C, false, true>(A, stream) : p2_launch<R, N, P_C2C, false, false>(A, stream);
     case P_R2C:
+      if (dsplit) return p2_launch<R, N, P_R2C, false, false, true>(A, stream);
       return direct ? p2_launch<R, N, P_R2C, false, true>(A, stream) : p2_launch<R, N, P_R2C, false, false>(A, stream);
     case P_C2R:
       return direct ? p2_launch<R, N, P_C2R, true, true>(A, stream) : p2_launch<R, N, P_C2R, true, false>(A, stream);
@@ -954,7 +981,7 @@ static int p2_lines_r(int m, int kind) {
 template <typename R, int N, int KIND, bool INV, bool DIRECT>
 static int p2_occ() {
   int blocks = 0;
-  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT, false>;
+  auto fn = pow2_kernel<R, N, KIND, INV, DIRECT, false, false>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2_smem<R, N>(KIND)) != cudaSuccess)
     return 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, P2_THREADS, p2_smem<R, N>(KIND)) != cudaSuccess)
