@@ -221,7 +221,9 @@ __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const t
 
 // Loads the stage-0 butterfly inputs of one tile into registers: butterfly b
 // (sequence b / NB0, index jb) takes elements jb + r*NB0 of its sequence.
-template <typename R, int N>
+// SX, strided lines (C2C, R2C): item b is butterfly b / NSEQ of sequence
+// b % NSEQ, so the lanes read adjacent lines at each position of the axis.
+template <typename R, int N, bool SX = false>
 __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0], const PassArgs& A,
                                         const TileAddr& ta) {
   using C = typename Cx<R>::T;
@@ -233,23 +235,38 @@ __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0]
 #pragma unroll
   for (int u = 0; u < G::U0; ++u) {
     const int b = threadIdx.x + u * MR_THREADS;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = SX ? b % G::NSEQ : b / NB;
+    const int jb = SX ? b / G::NSEQ : b - s * NB;
     const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
     if (A.kind == P_C2C) {
       const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
       const bool ok = live && s < L;
-      const long long base = ta.src0 + (long long)s * ta.srcb + jb;
+      const long long base = ta.src0 + (long long)s * ta.srcb;
+      if constexpr (SX) {
+        const C* __restrict__ p = in + base + (long long)jb * ta.srcq;
 #pragma unroll
-      for (int r = 0; r < R0; ++r) v[u][r] = ok ? in[base + r * NB] : mk<C, R>(zero, zero);
+        for (int r = 0; r < R0; ++r) v[u][r] = ok ? p[(long long)r * NB * ta.srcq] : mk<C, R>(zero, zero);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[u][r] = ok ? in[base + jb + r * NB] : mk<C, R>(zero, zero);
+      }
     } else if (A.kind == P_R2C) {
       const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
       const bool ok0 = live && 2 * s < L, ok1 = live && 2 * s + 1 < L;
-      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb + jb;
+      const long long b0 = ta.src0 + (long long)(2 * s) * ta.srcb;
       const long long b1 = b0 + ta.srcb;
+      if constexpr (SX) {
+        const long long o = (long long)jb * ta.srcq;
 #pragma unroll
-      for (int r = 0; r < R0; ++r)
-        v[u][r] = mk<C, R>(ok0 ? in[b0 + r * NB] : zero, ok1 ? in[b1 + r * NB] : zero);
+        for (int r = 0; r < R0; ++r) {
+          const long long q = o + (long long)r * NB * ta.srcq;
+          v[u][r] = mk<C, R>(ok0 ? in[b0 + q] : zero, ok1 ? in[b1 + q] : zero);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R0; ++r)
+          v[u][r] = mk<C, R>(ok0 ? in[b0 + jb + r * NB] : zero, ok1 ? in[b1 + jb + r * NB] : zero);
+      }
     } else {  // C2R: Hermitian extension of two half spectra
       const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
       const bool ok0 = live && 2 * s < L, ok1 = live && 2 * s + 1 < L;
@@ -281,7 +298,7 @@ __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0]
 }
 
 // Stage 0 (no twiddles) on the registers; outputs jb*R0 + r go to `out`.
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, bool SX = false>
 __device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                           typename Cx<R>::T* out) {
   using C = typename Cx<R>::T;
@@ -292,8 +309,8 @@ __device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U
   for (int u = 0; u < G::U0; ++u) {
     const int b = threadIdx.x + u * MR_THREADS;
     if (G::B0 % MR_THREADS != 0 && b >= G::B0) break;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = SX ? b % G::NSEQ : b / NB;  // the mapping of mr_load
+    const int jb = SX ? b / G::NSEQ : b - s * NB;
     C t[R0];
 #pragma unroll
     for (int r = 0; r < R0; ++r) t[r] = v[u][r];
@@ -307,10 +324,11 @@ __device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U
 // Last stage with the direct C2C or C2R store: in the last Stockham stage
 // (NS = N/RAD) butterfly jb writes outputs jb + r*NB, so each output goes
 // straight to HBM, coalesced across the threads of a sequence.
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, bool DS>
 __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const TileAddr& ta,
                                                     const typename Cx<R>::T* __restrict__ in,
-                                                    const typename Cx<R>::T* __restrict__ W) {
+                                                    const typename Cx<R>::T* __restrict__ W, const long long* Atab,
+                                                    const int2* ktab, const PieceAddr* prow) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int ST = G::NST - 1;
@@ -336,9 +354,18 @@ __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const Til
     Bfly<C, RAD, INV>::run(v);
     if (A.kind == P_C2C) {
       if (s < L) {
-        C* __restrict__ out = reinterpret_cast<C*>(A.out) + ta.dst0 + (long long)s * ta.dstb + jb;
+        if (DS && A.dst_k_contig == 2) {  // split across the destination's ranks
+          C* __restrict__ out = reinterpret_cast<C*>(A.out);
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) out[r * NB] = scl(v[r], sc);
+          for (int r = 0; r < RAD; ++r) {
+            const int k = jb + r * NB;
+            out[Atab[k] + (long long)s * prow[ktab[k].x].stride] = scl(v[r], sc);
+          }
+        } else {
+          C* __restrict__ out = reinterpret_cast<C*>(A.out) + ta.dst0 + (long long)s * ta.dstb + jb;
+#pragma unroll
+          for (int r = 0; r < RAD; ++r) out[r * NB] = scl(v[r], sc);
+        }
       }
     } else {
       R* __restrict__ out = reinterpret_cast<R*>(A.out) + ta.dst0 + (long long)(2 * s) * ta.dstb + jb;
@@ -430,9 +457,9 @@ __device__ __forceinline__ void mr_last_stage_xstore(const PassArgs& A, const Ti
 // transposed store; element (k, line j) of a transposed store goes to
 // Atab[k] + j, each thread writing the pair of lines (j, j+1), as one 16-byte
 // vector where aligned in f32).
-template <typename R, int N>
+template <typename R, int N, bool DS>
 __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
-                                         const long long* Atab) {
+                                         const long long* Atab, const int2* ktab, const PieceAddr* prow) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int NSEQ = G::NSEQ;
@@ -455,8 +482,9 @@ __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, 
       const C b = seq[G::pad(k == 0 ? 0 : N - k)];
       R f = sc * R(0.5);
       if (post_weighted && k != 0 && 2 * k != N) f *= pf;
-      out[ta.dst0 + (long long)l * ta.dstb + k] = (l & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f)
-                                                         : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
+      const long long o = (DS && A.dst_k_contig == 2) ? Atab[k] + (long long)l * prow[ktab[k].x].stride  // split
+                                                      : ta.dst0 + (long long)l * ta.dstb + k;
+      out[o] = (l & 1) ? mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f) : mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
     }
     return;
   }
@@ -556,7 +584,7 @@ __host__ __device__ constexpr size_t mr_smem_bytes() {
          (size_t)MR_MAX_PIECES * 16;
 }
 
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, bool SX, bool DS>
 __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
                                         typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                         typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
@@ -565,23 +593,27 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   const int tid = threadIdx.x;
-  const bool direct = A.dst_k_contig != 0;
+  const bool direct = A.dst_k_contig != 0;  // 2: split across the destination's ranks
+  const bool dsplit = DS && A.dst_k_contig == 2;
   const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
-  mr_stage0<R, N, INV>(v, b0);
+  mr_stage0<R, N, INV, SX>(v, b0);
   if (tid < npieces) prow[tid] = my_piece;
   __syncthreads();
-  if (!direct) {
-    // destination row of each k of this tile (read after later barriers)
+  if (!direct || dsplit) {
+    // destination row of each k of this tile (read after later barriers);
+    // split direct store: the offset of k in line 0, the line stride is the
+    // piece's
     for (int k = tid; k < nout; k += MR_THREADS) {
       const int2 kp = ktab[k];
       const PieceAddr pa = prow[kp.x];
-      Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+      Atab[k] = pa.rowbase + (dsplit ? (long long)kp.y : (long long)kp.y * pa.stride);
     }
   }
   if (direct && A.kind != P_R2C) {
     // stages 1 .. NST-2 in shared memory, the last one to HBM
     mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
-    mr_last_stage_store<R, N, INV>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W);
+    if (G::NST == 2 && dsplit) __syncthreads();  // the row tables above are read next
+    mr_last_stage_store<R, N, INV, DS>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab, ktab, prow);
     return;
   }
   if (A.kind == P_C2C) {
@@ -593,7 +625,7 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
     return;
   }
   mr_stages_upto<R, N, INV, 1, G::NST>(b0, b1, W);
-  mr_store<R, N>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab);
+  mr_store<R, N, DS>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab, ktab, prow);
 }
 
 // Tiles first, first + step, ... (< end) of one pass: the persistent loop of
@@ -613,7 +645,7 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
                                             const typename Cx<R>::T* W, long long* Atab, const int2* ktab,
                                             PieceAddr* prow, const PieceAddr& my_piece, int npieces);
 
-template <typename R, int N, bool R2R = false>
+template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false>
 __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
                                        unsigned char* smem, bool setup) {
   using C = typename Cx<R>::T;
@@ -629,7 +661,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   long long tile = first;
   if (tile >= end) return;
   const int tid = threadIdx.x;
-  const bool direct = A.dst_k_contig != 0;
+  const bool direct = A.dst_k_contig == 1;  // 2 (split direct store) reads the row tables
   const int nout = R2R ? A.n_out : ((A.kind == P_R2C) ? N / 2 + 1 : N);
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
@@ -644,7 +676,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   if constexpr (R2R)
     mr_load_r2r<R, N>(v, A, ta);
   else
-    mr_load<R, N>(v, A, ta);
+    mr_load<R, N, SX>(v, A, ta);
   TileAddr t1 = ta;
   if (tile + step < end) t1 = load_tile(tiles, tile + step);
   PieceAddr my_piece{0, 0};
@@ -660,7 +692,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
       if constexpr (R2R)
         mr_load_r2r<R, N>(nv, A, t1);
       else
-        mr_load<R, N>(nv, A, t1);
+        mr_load<R, N, SX>(nv, A, t1);
       if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
       if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
@@ -671,9 +703,9 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
         mr_tile_r2r<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     } else {
       if (A.inv)
-        mr_tile<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile<R, N, true, SX, DS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
       else
-        mr_tile<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile<R, N, false, SX, DS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     }
     if (!has_next) break;
     tile += step;
@@ -688,34 +720,45 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   }
 }
 
-template <typename R, int N>
+// Variants V: 0 lines contiguous in the source, direct or transposed store;
+// 1 strided lines (the source's innermost axis is the tile axis), any store;
+// 2 contiguous lines, split direct store.  Kernels of their own, so that the
+// common one keeps its register allocation.
+template <typename R, int N, int V>
 __global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
-  mr_run<R, N>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
+  mr_run<R, N, false, V == 1, V != 0>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
 }
+
+inline int mr_variant(const PassArgs& A) { return A.src_k_contig == 0 ? 1 : (A.dst_k_contig == 2 ? 2 : 0); }
 
 // Host entry points of one length (instantiated by mr_kernels.cu).
 template <typename R, int N>
 cudaError_t mr_launch(const PassArgs& A, cudaStream_t stream) {
   constexpr size_t smem = mr_smem_bytes<R, N>();
-  cudaError_t err = cudaFuncSetAttribute(mr_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int var = mr_variant(A);
+  const auto kern = var == 1 ? mr_kernel<R, N, 1> : var == 2 ? mr_kernel<R, N, 2> : mr_kernel<R, N, 0>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
   if (grid > A.ntiles) grid = A.ntiles;
-  mr_kernel<R, N><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
+  kern<<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
   return cudaGetLastError();
 }
 
+// resident CTAs per SM, the smallest of the variants' figures
 template <typename R, int N>
 int mr_occupancy() {
   constexpr size_t smem = mr_smem_bytes<R, N>();
-  int blocks = 0;
-  if (cudaFuncSetAttribute(mr_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_kernel<R, N>, MR_THREADS, smem) != cudaSuccess)
-    return 1;
-  return blocks > 0 ? blocks : 1;
+  int best = 0;
+  for (const auto kern : {mr_kernel<R, N, 0>, mr_kernel<R, N, 1>, mr_kernel<R, N, 2>}) {
+    int blocks = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, MR_THREADS, smem) != cudaSuccess) return 1;
+    best = best == 0 ? blocks : std::min(best, blocks);
+  }
+  return best > 0 ? best : 1;
 }
 
 }  // namespace pb

@@ -1078,15 +1078,18 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.lines = L;
     }
   }
-  // register-fed mixed-radix kernel: the same layouts, 7-smooth lengths
+  // register-fed mixed-radix kernel: the same layouts (strided lines and the
+  // split direct store included), 7-smooth lengths
   if (!A.fast && !P.force_generic && (op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) &&
-      mr_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+      mr_supported(A.m, P.real_bytes) && (src.perm[N - 1] == a || src_strided) && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
-    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
-    if (direct || transposed) {
+    const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
+    const bool dsplit = !direct && dst.perm[N - 1] == a && ta >= 0 && dst.grid[ta] <= 64 &&
+                        (op.kind == P_C2C || op.kind == P_R2C);
+    if (direct || transposed || dsplit) {
       A.fast = 2;
-      A.dst_k_contig = direct ? 1 : 0;
+      A.dst_k_contig = direct ? 1 : (dsplit ? 2 : 0);
       L = mr_lines(A.m, op.kind, P.real_bytes);
       A.lines = L;
     }

@@ -447,6 +447,40 @@ def test_pow2_strided_lines_match_oracle(rb, dims, shape, extra):
         check_transform(plan, route, spec, e, rb, True, d)
 
 
+MR_STRIDED_CASES = [((2, 2), (48, 96, 40), (2,)), ((2, 3), (60, 36, 90), ()), ((3, 2), (45, 120, 72), ()),
+                    ((2, 4), (36, 50, 80), ())]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape,extra", MR_STRIDED_CASES)
+def test_mixed_radix_strided_lines_match_oracle(rb, dims, shape, extra):
+    """permute_dims = false with 7-smooth lengths: every pass on the
+    mixed-radix kernel, strided lines loaded across the tile's adjacent lines
+    and stores split across the destination's ranks where the transform axis
+    stays innermost.  Grids with 3 ranks cut the axes unevenly."""
+    from pencil_b200 import _lib as L
+    rng = np.random.default_rng(13)
+    topo = pb.MpiTopology(dims)
+    e = int(np.prod(extra)) if extra else 1
+    lay = pb.DistributedLayout(False)
+    plan = pb.C2cPlan.from_shape(topo, shape, extra, layout=lay, dtype=CDT[rb])
+    for op in (L.FORWARD, L.INVERSE):
+        assert set(plan.step_kernels(op)) <= {"mixed_radix", "check"}
+    route = po.c2c_route(po.Topology(dims), shape, None, False)
+    x = rand_field(rng, shape, extra, True, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, e, rb, True, d)
+    plan = pb.R2cPlan.from_shape(topo, shape, extra, layout=lay, dtype=RDT[rb])
+    assert "generic" not in plan.step_kernels(L.FORWARD)
+    route = po.r2c_route(po.Topology(dims), shape, None, False)
+    x = rand_field(rng, shape, extra, False, rb)
+    check_transform(plan, route, x, e, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), (e,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, e, rb, True, d)
+
+
 @pytest.mark.parametrize("n", [64, 256])
 @pytest.mark.parametrize("rb", [4, 8])
 @pytest.mark.parametrize("family", ["r2c", "c2r", "c2c"])
