@@ -315,7 +315,7 @@ def b200_arm(args):
     families = sorted(set(plan.step_kernels(L.FORWARD) + plan.step_kernels(L.INVERSE)) - {"check"})
     kernel_names = ", ".join({"pow2": "pb::pow2_kernel<float, 512, kind, sign, store> (R2C, C2C), "
                                       "pb::pow2_half_c2r_kernel<256> (C2R)",
-                              "mixed_radix": "pb::mr_kernel<float, N>",
+                              "mixed_radix": "pb::mr_kernel<float, N, variant>",
                               "generic": "pb::pass_kernel<float>"}[f] for f in families)
     fwd_t, inv_t = [], []
     for _ in range(max(3, min(args.steps, 10))):
