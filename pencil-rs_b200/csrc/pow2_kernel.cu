@@ -132,6 +132,37 @@ __device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const Pas
     // slot/t are g and b: sequences LPT*g + i, inputs b + T*m along the
     // strided axis (stride srcq), adjacent lines srcb apart
     const int g = slot, b = t;
+    if constexpr (LPT == 2 && sizeof(R) == 4) {
+      // f32, two sequences per thread: its adjacent lines (C2C 2g, 2g+1; R2C
+      // 4g .. 4g+3) are 16 contiguous bytes at each position, one vector load
+      // where aligned
+      constexpr int NL = KIND == P_C2C ? 2 : 4;
+      const bool full = ta.srcb == 1 && NL * g + NL - 1 < L;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const long long q = (long long)(b + T * m) * ta.srcq;
+        const long long o = ta.src0 + (long long)(NL * g) * ta.srcb + q;
+        const R* __restrict__ p = reinterpret_cast<const R*>(A.in) + (KIND == P_C2C ? 2 * o : o);
+        if (full && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+          const float4 w = *reinterpret_cast<const float4*>(p);
+          raw.a[0][m] = mk<C, R>(w.x, w.y);
+          raw.a[1][m] = mk<C, R>(w.z, w.w);
+        } else if constexpr (KIND == P_C2C) {
+          const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+          raw.a[0][m] = 2 * g < L ? in[o] : z;
+          raw.a[1][m] = 2 * g + 1 < L ? in[o + ta.srcb] : z;
+        } else {
+          const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int l = 4 * g + 2 * i;
+            const long long oi = o + (long long)(2 * i) * ta.srcb;
+            raw.a[i][m] = mk<C, R>(l < L ? in[oi] : zero, l + 1 < L ? in[oi + ta.srcb] : zero);
+          }
+        }
+      }
+      return;
+    }
 #pragma unroll
     for (int i = 0; i < LPT; ++i) {
       const int sq = LPT * g + i;
