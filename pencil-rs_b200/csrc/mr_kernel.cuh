@@ -21,7 +21,9 @@
 // destination) or transposed through shared memory so that the lines of a
 // tile form runs of the destination's innermost axis (the fused pencil
 // transpose), with host-precomputed tile, piece and k tables as in the
-// power-of-two kernel.
+// power-of-two kernel.  Strided lines (permute_dims = false: the source's
+// innermost axis is the tile axis) and the direct store split across the
+// destination's ranks take kernel variants of their own (mr_kernel's V).
 #pragma once
 
 #include <cuda_runtime.h>
