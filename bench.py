@@ -484,6 +484,54 @@ def b200_arm(args):
     return 0 if ok else 3
 
 
+LAYOUT_CASES = (((512, 512, 512), "c2c"), ((384, 384, 384), "c2c"), ((512, 512, 512), "r2c"),
+                ((384, 384, 384), "r2c"))
+
+
+def layouts_arm(args):
+    """Forward + inverse per-launch device times (median over the timed
+    repetitions) of 512^3 and 384^3 C2C and R2C f32 on the 4x8 virtual grid,
+    with permuted (permute_dims = true) and strided (permute_dims = false)
+    layouts: one JSON line per case.  Not the headline; 1 GPU."""
+    import statistics
+
+    import torch
+    import pencil_b200 as pb
+    from pencil_b200 import _lib as L
+
+    torch.manual_seed(0)
+    reps = max(5, min(args.steps, 20))
+    for shape, kind in LAYOUT_CASES:
+        for permute in (True, False):
+            topo = pb.MpiTopology(GRID)
+            lay = pb.DistributedLayout(permute)
+            if kind == "c2c":
+                plan = pb.C2cPlan.from_shape(topo, shape, (), layout=lay, dtype=torch.complex64)
+                x = torch.randn(plan.info.input_elems, dtype=torch.complex64, device="cuda")
+            else:
+                plan = pb.R2cPlan.from_shape(topo, shape, (), layout=lay, dtype=torch.float32)
+                x = torch.randn(plan.info.input_elems, dtype=torch.float32, device="cuda")
+            y, z, ws = plan.allocate_output(), plan.allocate_input(), plan.allocate_workspace()
+            for _ in range(args.warmup):
+                plan.forward(x, y, ws)
+                plan.inverse(y, z, ws)
+            torch.cuda.synchronize()
+            tf = [plan.execute_timed(L.FORWARD, x, y, ws) for _ in range(reps)]
+            ti = [plan.execute_timed(L.INVERSE, y, z, ws) for _ in range(reps)]
+            fm = [statistics.median(c) for c in zip(*tf)]
+            im = [statistics.median(c) for c in zip(*ti)]
+            rt = float(torch.linalg.vector_norm(z - x) / torch.linalg.vector_norm(x))
+            print(json.dumps({"layouts": {"shape": list(shape), "kind": kind + " f32", "grid": list(GRID),
+                                          "layout": "permuted" if permute else "strided",
+                                          "kernels": plan.step_kernels(L.FORWARD),
+                                          "forward_ms": [round(v, 4) for v in fm],
+                                          "inverse_ms": [round(v, 4) for v in im],
+                                          "total_ms": round(sum(fm) + sum(im), 4), "repetitions": reps,
+                                          "roundtrip_rel_l2": rt}}), flush=True)
+            plan.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -495,9 +543,13 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-grid ragged-batch comparison")
     ap.add_argument("--batch-grids", type=int, default=64,
                     help="grids of the ragged batch (the first K of the 64-grid workload; profiling runs)")
+    ap.add_argument("--layouts", action="store_true",
+                    help="instead of the headline: permuted against strided layouts, per-launch times (1 GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.layouts:
+        return layouts_arm(args)
     if args.impl == "reference":
         return reference_arm(args)
     return b200_arm(args)
