@@ -164,13 +164,10 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids
     of 2, forward + inverse.  One graph-replayed persistent launch for the whole
     batch against per-grid launches of the plain kernels (pb_execute per grid
     and direction), at the same accuracy bound."""
-    import numpy as np
-    smooth = sorted({2 ** a * 3 ** b * 5 ** c * 7 ** d for a in range(9) for b in range(6) for c in range(4)
-                     for d in range(3) if 32 <= 2 ** a * 3 ** b * 5 ** c * 7 ** d <= 256})
-    rng = np.random.default_rng(4)
-    shapes = [tuple(int(v) for v in rng.choice(smooth, 3)) for _ in range(64)]
-    with_extra = set(int(i) for i in rng.choice(64, 16, replace=False))
-    shapes = shapes[:ngrids]
+    from pencil_b200 import workloads
+    work = workloads.ragged_batch(4)
+    shapes = [s for s, _ in work][:ngrids]
+    with_extra = set(i for i, (_, e) in enumerate(work) if e)
     from pencil_b200 import distributed as pbd
     mine = list(pbd.shard(len(shapes), rank, world))  # grids are independent: no exchange across GPUs
     gen = torch.Generator(device=dev).manual_seed(4 + rank)
@@ -238,6 +235,175 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids
             "launches_per_grid": int(pbd.sum_over_ranks(sum(p.info.passes_forward + p.info.passes_inverse for p in plans))),
             "roundtrip_rel_l2_batch": rt_b, "roundtrip_rel_l2_per_grid": rt_p, "batch_vs_per_grid_rel_l2": diff,
             "bound": worst_bound, "shapes_seed": 4}
+
+
+def _event_ms(torch, stream, fn, steps, warmup):
+    """Mean device time of fn() over `steps` calls after `warmup`, CUDA events on `stream`."""
+    for _ in range(warmup):
+        fn()
+    stream.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    stream.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def cufft_section(torch, xa, bytes_step, steps, warmup):
+    """cuFFT on the same GPU and field (torch.fft.rfftn / irfftn, f32, the
+    global row-major field: no pencil layout), timed like the headline: a
+    comparison point, not part of the product."""
+    shape = tuple(xa.shape)
+    stream = torch.cuda.current_stream()
+    spec = torch.empty(shape[:-1] + (shape[-1] // 2 + 1,), dtype=torch.complex64, device=xa.device)
+    back = torch.empty_like(xa)
+
+    def step():
+        torch.fft.rfftn(xa, out=spec)
+        torch.fft.irfftn(spec, s=shape, out=back)
+
+    ms = _event_ms(torch, stream, step, steps, warmup)
+    torch.fft.rfftn(xa, out=spec)
+    ref = torch.fft.rfftn(xa.double())
+    err = float(torch.linalg.vector_norm(spec.to(torch.complex128) - ref) / torch.linalg.vector_norm(ref))
+    del ref
+    torch.fft.irfftn(spec, s=shape, out=back)
+    rt = float(torch.linalg.vector_norm((back - xa).double()) / torch.linalg.vector_norm(xa.double()))
+    return {"ms_per_step": ms, "gbs_at_pass_model_bytes": bytes_step / (ms * 1e-3) / 1e9,
+            "forward_rel_l2_vs_float64": err, "roundtrip_rel_l2": rt,
+            "what": "torch.fft.rfftn + irfftn (cuFFT) f32 on the global [512,512,512] field, same GPU"}
+
+
+def unfused_section(pb, L, torch, dev, shape, x, fused_spec, steps, warmup):
+    """The reference's unfused route on the same field and 4x8 virtual grid:
+    every stage is a line transform with a direct store in its own pencil
+    layout (a one-axis plan over the ranks' concatenated lines), and every
+    distributed edge is a separate transpose, either one transpose pass
+    (pb_transpose_execute) or the staged pack -> exchange -> unpack of the
+    segment layout (transpose.rs:1126-1281, alltoallv_transpose.rs:324-367)."""
+    topo = pb.MpiTopology(GRID)
+    cshape = tuple(shape[:-1]) + (shape[-1] // 2 + 1,)
+    pens, _ = pb.route_pencils(topo, cshape)
+    n = list(reversed(shape))  # stage k transforms axis N-1-k
+    flat = pb.DistributedLayout(False)
+    one = pb.MpiTopology((1,))
+    lines = []
+    for k, p in enumerate(pens):
+        count = p.total() // cshape[2 - k] if k == 0 else p.total() // n[k]
+        if k == 0:
+            lines.append(pb.R2cPlan.from_shape(one, (count, n[0]), (), selection=[1], layout=flat, dtype=torch.float32))
+        else:
+            lines.append(pb.C2cPlan.from_shape(one, (count, n[k]), (), selection=[1], layout=flat,
+                                               dtype=torch.complex64))
+    fwd_t = [pb.AllToAllvTransposePlan(pens[k], pens[k + 1], 1, torch.complex64) for k in range(2)]
+    inv_t = [pb.AllToAllvTransposePlan(pens[k + 1], pens[k], 1, torch.complex64) for k in range(2)]
+    kernels = [pl.step_kernels(L.FORWARD) for pl in lines]
+    wss = [pl.allocate_workspace(dev) for pl in lines]
+    bufs = [torch.empty(p.total(), dtype=torch.complex64, device=dev) for p in pens for _ in range(2)]
+    sendn = max(max(t.workspace_requirements()) for t in fwd_t + inv_t)
+    send = torch.empty(sendn, dtype=torch.complex64, device=dev)
+    recv = torch.empty(sendn, dtype=torch.complex64, device=dev)
+    back = torch.empty_like(x)
+    lib = L.load()
+    stream = torch.cuda.current_stream(dev)
+    sp = pb.plans._stream_ptr(stream)
+    P = pb.plans._ptr
+
+    def run(pl, op, a, b, w):
+        L.check(lib.pb_execute(pl._h, op, P(a), P(b), P(w), sp), "unfused pass")
+
+    def move(t, a, b, staged):
+        if staged:
+            t.pack(a, send, stream)
+            t.exchange(send, recv, stream)
+            t.unpack(recv, b, stream)
+        else:
+            t.execute(a, b, stream)
+
+    def step(staged):
+        # forward: stage k writes bufs[2k], the edge moves it to bufs[2k+1] (stage k+1's input)
+        run(lines[0], L.FORWARD, x, bufs[0], wss[0])
+        move(fwd_t[0], bufs[0], bufs[1], staged)
+        run(lines[1], L.FORWARD, bufs[1], bufs[2], wss[1])
+        move(fwd_t[1], bufs[2], bufs[3], staged)
+        run(lines[2], L.FORWARD, bufs[3], bufs[4], wss[2])
+        # normalised inverse back to the real field
+        run(lines[2], L.INVERSE, bufs[4], bufs[5], wss[2])
+        move(inv_t[1], bufs[5], bufs[2], staged)
+        run(lines[1], L.INVERSE, bufs[2], bufs[1], wss[1])
+        move(inv_t[0], bufs[1], bufs[0], staged)
+        run(lines[0], L.INVERSE, bufs[0], back, wss[0])
+
+    out = {}
+    for staged in (False, True):
+        ms = _event_ms(torch, stream, lambda: step(staged), steps, warmup)
+        L.check(lib.pb_execute_status(lines[0]._h, P(wss[0]), sp), "unfused spectrum")
+        key = "pack_exchange_unpack" if staged else "transpose_pass"
+        out[key] = {"ms_per_step": ms, "launches_per_step": 6 + (12 if staged else 4)}
+    err = float(torch.linalg.vector_norm(bufs[4] - fused_spec) / torch.linalg.vector_norm(fused_spec))
+    rt = float(torch.linalg.vector_norm((back - x).double()) / torch.linalg.vector_norm(x.double()))
+    out.update(kernels=kernels, unfused_vs_fused_spectrum_rel_l2=err, roundtrip_rel_l2=rt)
+    for pl in lines:
+        pl.close()
+    return out
+
+
+def configs_section(pb, L, torch, dev, steps, warmup):
+    """Device time of one forward + normalised inverse at the other benchmark
+    configurations (CUDA events, mean over `steps`; inputs resident):
+    64^3 C2C f64 on 2x2; [3,256,384,320] DCT-II/DST-I/DHT on 2x3 (real f32
+    through R2rPlan, complex f32 and f64 through MixedC2cPlan); 384^3 R2C f32
+    on 4x8 and its adjoint (VJP of forward then of inverse)."""
+    stream = torch.cuda.current_stream(dev)
+    lib = L.load()
+    sp = pb.plans._stream_ptr(stream)
+    P = pb.plans._ptr
+    cases = [
+        ("c2c_f64_64cube_2x2", lambda: pb.C2cPlan.from_shape(pb.MpiTopology((2, 2)), (64, 64, 64), (),
+                                                             dtype=torch.complex128), (L.FORWARD, L.INVERSE)),
+        ("mixed_real_f32_3x256x384x320_2x3",
+         lambda: pb.R2rPlan.from_shape(pb.MpiTopology((2, 3)), (256, 384, 320), (3,), ("DctII", "DstI", "Dht"),
+                                       dtype=torch.float32), (L.FORWARD, L.INVERSE)),
+        ("mixed_complex_f32_3x256x384x320_2x3",
+         lambda: pb.MixedC2cPlan.from_shape(pb.MpiTopology((2, 3)), (256, 384, 320), (3,), ("DctII", "DstI", "Dht"),
+                                            dtype=torch.complex64), (L.FORWARD, L.INVERSE)),
+        ("mixed_complex_f64_3x256x384x320_2x3",
+         lambda: pb.MixedC2cPlan.from_shape(pb.MpiTopology((2, 3)), (256, 384, 320), (3,), ("DctII", "DstI", "Dht"),
+                                            dtype=torch.complex128), (L.FORWARD, L.INVERSE)),
+        ("r2c_f32_384cube_4x8", lambda: pb.R2cPlan.from_shape(pb.MpiTopology((4, 8)), (384, 384, 384), (),
+                                                             dtype=torch.float32), (L.FORWARD, L.INVERSE)),
+        ("r2c_f32_384cube_4x8_vjp", lambda: pb.R2cPlan.from_shape(pb.MpiTopology((4, 8)), (384, 384, 384), (),
+                                                                 dtype=torch.float32),
+         (L.VJP_INVERSE, L.VJP_FORWARD)),
+    ]
+    out = {}
+    for name, make, ops in cases:
+        plan = make()
+        a = plan.allocate_input(dev)
+        if a.is_complex():
+            a.copy_(torch.randn(a.numel(), dtype=a.dtype, device=dev))
+        else:
+            a.normal_()
+        b = plan.allocate_output(dev)
+        c = plan.allocate_input(dev)
+        ws = plan.allocate_workspace(dev)
+        if ops[0] == L.FORWARD:
+            def step():
+                L.check(lib.pb_execute(plan._h, ops[0], P(a), P(b), P(ws), sp), name)
+                L.check(lib.pb_execute(plan._h, ops[1], P(b), P(c), P(ws), sp), name)
+        else:  # adjoint chain: cotangent of the inverse's output -> spectrum -> input
+            def step():
+                L.check(lib.pb_execute(plan._h, ops[0], P(a), P(b), P(ws), sp), name)
+                L.check(lib.pb_execute(plan._h, ops[1], P(b), P(c), P(ws), sp), name)
+        ms = _event_ms(torch, stream, step, steps, warmup)
+        err = float(torch.linalg.vector_norm(c - a) / torch.linalg.vector_norm(a)) if ops[0] == L.FORWARD else None
+        out[name] = {"ms_fwd_inv": ms, "kernels": plan.step_kernels(L.FORWARD), "roundtrip_rel_l2": err}
+        plan.close()
+        del a, b, c, ws
+    return out
 
 
 def b200_arm(args):
@@ -439,9 +605,25 @@ def b200_arm(args):
     if not args.no_batch:
         batch = batch_section(pb, L, torch, dev, rank=rank, world=world, ngrids=args.batch_grids)
 
+    cufft = unfused = others = None
+    if not args.no_compare:
+        reps = max(3, min(args.steps, 10))
+        cufft = cufft_section(torch, torch.from_numpy(xa_host).to(dev), bytes_step, reps, args.warmup)
+        plan.forward(x, spec, ws)
+        unfused = unfused_section(pb, L, torch, dev, shape, x, spec, reps, args.warmup)
+        others = configs_section(pb, L, torch, dev, reps, args.warmup)
+    # every rank takes the same collective steps: max over ranks of the comparison times
+    for sec in (cufft, (unfused or {}).get("transpose_pass"), (unfused or {}).get("pack_exchange_unpack")):
+        if sec is not None:
+            sec["ms_per_step"] = max_over_ranks(sec["ms_per_step"])
+    if unfused is not None:
+        for sec in ("transpose_pass", "pack_exchange_unpack"):
+            unfused[sec]["gbs_at_pass_model_bytes"] = bytes_step / (unfused[sec]["ms_per_step"] * 1e-3) / 1e9
+            unfused[sec]["fused_speedup"] = unfused[sec]["ms_per_step"] / ms
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline()
+        base = cpu_baseline(steps=5, warmup=1)
 
     if rank == 0:
         traffic = None
@@ -460,10 +642,16 @@ def b200_arm(args):
                        "l2": "no flush: every pass streams >= 512 MiB, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (each GPU runs the full field)"},
             "gflops": flops(shape) / (ms * 1e-3) / 1e9 * world,
+            "gflops_real_halved": flops(shape) / 2 / (ms * 1e-3) / 1e9 * world,
+            "gflops_note": "5 N log2 N per direction (the north-star convention); the halved figure counts a "
+                           "real transform as half a complex one",
             "accuracy": {"roundtrip_rel_l2": rt, "field_b_rel_l2": kb, "bound": 1e-6 * lg,
                          "e2e_roundtrip_rel_l2": e2e_err},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch of the "
+                                           "dominant kernel from one committed ncu capture of this workload "
+                                           "(profiles/traffic_pow2_kernel_512cube.json), not measured in this run",
                          "kernel": kernel_names, "bytes_per_launch": per_pass,
                          "launch_ms_avg": pass_ms / launches, "spectrum_check_ms": check_ms,
                          "launch_ms": {"forward": dict(zip([f"{i}:{k}" for i, k in enumerate(kinds_f)],
@@ -472,10 +660,15 @@ def b200_arm(args):
                                                            per_pass_ms[len(kinds_f):]))}},
             "e2e": {"value": bytes_step / (e2e_ms * 1e-3) / 1e9 * world, "unit": "GB/s", "ms_per_step": e2e_ms,
                     "wall_ms_per_step": e2e_wall_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps * (plan.info.passes_forward + plan.info.passes_inverse + 2),
+            # the library's own kernels in the timed region: every pass plus the C2R spectrum
+            # check (passes_inverse counts it); the check words' cudaMemsetAsync is not a kernel here
+            "gpu_launches": args.steps * (plan.info.passes_forward + plan.info.passes_inverse),
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "cpu_baseline": base,
             "ragged_batch": batch,
+            "cufft": cufft,
+            "unfused": unfused,
+            "other_configs": others,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -541,6 +734,8 @@ def main():
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-grid ragged-batch comparison")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the cuFFT and unfused-route comparisons and the other configurations")
     ap.add_argument("--batch-grids", type=int, default=64,
                     help="grids of the ragged batch (the first K of the 64-grid workload; profiling runs)")
     ap.add_argument("--layouts", action="store_true",

@@ -218,7 +218,8 @@ int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int3
  * this library holds until exit; the call allocates nothing.  A plan whose
  * pb_plan_info.workspace_bytes exceeds that size is rejected with
  * PB_ENO_ALLOC_LIMIT before any device work.  The first call on a device looks
- * up the array's device address (once per device, with that device current):
+ * up the array's device address (once per device, with that device current,
+ * and again when the device's context changes, e.g. after cudaDeviceReset):
  * make that first call before any stream capture.  All calls share the one
  * array: calls that overlap on the GPU (other streams, other threads) race
  * and must be serialised by the caller.  The spectrum-check words are cleared
@@ -256,6 +257,14 @@ int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, voi
 /* Waits for `stream`; PB_ETIMEOUT if a bounded dependency wait in the last
  * execution gave up (its tiles were skipped), else PB_OK. */
 int pb_batch_status(pb_batch* batch, void* workspace, void* stream);
+/* Bound of each dependency wait inside the batch kernel, in steps of about
+ * 100 ns (default 2^24, about 1.7 s).  A wait that runs out sets the batch's
+ * error word, the items behind it are skipped (nothing is written for them)
+ * and pb_batch_status returns PB_ETIMEOUT; the next execution starts from
+ * cleared control words.  No counterpart in the reference (its collection
+ * loop has no device waits); a short limit lets a caller or a test make the
+ * wait give up without stalling the GPU. */
+int pb_batch_set_wait_limit(pb_batch* batch, int64_t spins);
 int pb_batch_destroy(pb_batch* batch);
 
 /* ---- transposes ------------------------------------------------------- */

@@ -2566,6 +2566,7 @@ struct pb_batch {
   std::vector<const void*> bound;   // buffers + workspace the device descriptors were resolved with
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
+  long long spin_limit = 1LL << 24;  // __nanosleep(100) steps of a dependency wait (about 1.7 s)
   ~pb_batch() {
     if (graph) cudaGraphExecDestroy(graph);
     if (d_descs) cudaFree(d_descs);
@@ -2884,7 +2885,7 @@ static int batch_execute(pb_batch* B, void* const* buffers, void* ws, cudaStream
   A.head = reinterpret_cast<unsigned long long*>(ctrl);
   A.error = reinterpret_cast<int*>(ctrl + 8);
   A.done = reinterpret_cast<unsigned*>(ctrl + 16);
-  A.spin_limit = 1LL << 24;
+  A.spin_limit = B->spin_limit;
   const size_t ctrl_bytes = 16 + B->descs.size() * sizeof(unsigned);
   if (s == nullptr) {  // the legacy stream cannot be captured: launch directly
     cuda_ok(cudaMemsetAsync(ctrl, 0, ctrl_bytes, s));
@@ -2944,6 +2945,19 @@ int pb_batch_status(pb_batch* batch, void* workspace, void* stream) {
     cuda_ok(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
     return err ? (int)PB_ETIMEOUT : (int)PB_OK;
   });
+}
+
+int pb_batch_set_wait_limit(pb_batch* batch, int64_t spins) {
+  if (!batch) return PB_ENULL;
+  if (spins < 0) return PB_EINVALID_ARGUMENT;
+  if (spins != batch->spin_limit) {
+    batch->spin_limit = spins;
+    if (batch->graph) {  // the captured launch holds the old limit
+      cudaGraphExecDestroy(batch->graph);
+      batch->graph = nullptr;
+    }
+  }
+  return PB_OK;
 }
 
 int pb_batch_destroy(pb_batch* batch) {

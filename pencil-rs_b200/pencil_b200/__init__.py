@@ -21,10 +21,11 @@ from .plans import (  # noqa: F401
     R2cPlan,
     R2rPlan,
     SpatialRemapPlan,
+    route_pencils,
 )
 
 __all__ = [
     "AllToAllvTransposePlan", "C2cPlan", "C2rPlan", "DhtPlan", "DistributedLayout", "InvalidSpectrum",
     "LocalTransposePlan", "MixedC2cPlan", "MixedR2cPlan", "MpiTopology", "Pencil", "PencilError", "PlanBatch", "R2cPlan",
-    "R2rPlan", "SpatialRemapPlan", "load",
+    "R2rPlan", "SpatialRemapPlan", "load", "route_pencils",
 ]

@@ -160,6 +160,23 @@ def _geom(topology: MpiTopology, shape, extra_shape, layout: DistributedLayout) 
     return g
 
 
+def route_pencils(topology: MpiTopology, global_shape, layout: DistributedLayout = DistributedLayout()):
+    """Stage pencils of the canonical route (``build_route``,
+    distributed.rs:2306-2382), stage k transforming axis N-1-k, and for each
+    edge k -> k+1 whether it is a distributed transition."""
+    g = _geom(topology, global_shape, (), layout)
+    lib = L.load()
+    pencils, edges = [], []
+    for k in range(len(global_shape)):
+        d = L.PbPencilDesc()
+        dist = C.c_int32()
+        L.check(lib.pb_route_stage(C.byref(g), k, C.byref(d), C.byref(dist)), "route stage")
+        pencils.append(Pencil._from_desc(d))
+        if k + 1 < len(global_shape):
+            edges.append(bool(dist.value))
+    return pencils, edges
+
+
 def _mask(n: int, selection) -> Optional[C.Array]:
     if selection is None:
         return None
@@ -225,13 +242,25 @@ class _Plan:
                                                                                        self.info.input_elems)
         self._check_buf(src, in_dt, in_n, "source")
         self._check_buf(dst, out_dt, out_n, "destination")
-        if workspace is None:
-            workspace = self.allocate_workspace(src.device)
+        temp = workspace is None
+        if temp:
+            workspace = self._stream_workspace(src.device, stream)
         lib = L.load()
         sp = _stream_ptr(stream)
         L.check(lib.pb_execute(self._h, op, _ptr(src), _ptr(dst), _ptr(workspace), sp), "execute")
+        if temp and stream is not None:
+            # the caching allocator must not hand this block to other work
+            # before the kernels enqueued on `stream` are done with it
+            workspace.record_stream(stream)
         if check_spectrum:
             L.check(lib.pb_execute_status(self._h, _ptr(workspace), sp), "spectrum")
+
+    def _stream_workspace(self, device, stream) -> torch.Tensor:
+        """A temporary workspace allocated on the stream that will use it."""
+        if stream is None:
+            return self.allocate_workspace(device)
+        with torch.cuda.stream(stream):
+            return self.allocate_workspace(device)
 
     def forward(self, src, dst, workspace=None, stream=None):
         self.execute(L.FORWARD, src, dst, workspace, stream, check_spectrum=self._forward_checks)
@@ -254,13 +283,16 @@ class _Plan:
 
     def execute_timed(self, op, src, dst, workspace=None, stream=None):
         """``*_with_timing`` analogue: device milliseconds of every launch."""
-        if workspace is None:
-            workspace = self.allocate_workspace(src.device)
+        temp = workspace is None
+        if temp:
+            workspace = self._stream_workspace(src.device, stream)
         cap = 64
         ms = (C.c_float * cap)()
         cnt = C.c_int32()
         L.check(L.load().pb_execute_timed(self._h, op, _ptr(src), _ptr(dst), _ptr(workspace), _stream_ptr(stream),
                                           ms, cap, C.byref(cnt)), "execute_timed")
+        if temp and stream is not None:
+            workspace.record_stream(stream)
         return [ms[i] for i in range(cnt.value)]
 
     def spectral_multiply(self, mode: int, scale: float, src, dst, stream=None):
@@ -556,6 +588,11 @@ class PlanBatch:
 
     def status(self, workspace, stream=None):
         L.check(L.load().pb_batch_status(self._h, _ptr(workspace), _stream_ptr(stream)), "batch status")
+
+    def set_wait_limit(self, spins: int) -> None:
+        """Bound of each in-kernel dependency wait (steps of about 100 ns);
+        a wait that runs out makes ``status`` raise ``Timeout``."""
+        L.check(L.load().pb_batch_set_wait_limit(self._h, int(spins)), "batch wait limit")
 
     def close(self):
         if getattr(self, "_h", None):

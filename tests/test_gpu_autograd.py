@@ -2,9 +2,9 @@
 
 * f64 central finite differences (h = 1e-6, 32 random directions) of
   L(u) = sum |k|^2 |R2C(u)|^2 and of a spectral Poisson solve followed by C2R;
-* the VJP against the reference's raw ``backward`` (C2C: the adjoint is the
-  raw opposite-sign transform; R2C: raw C2R of the cotangent with interior
-  bins halved);
+* the VJP against the oracle's restatement of the reference's raw
+  ``backward`` (C2C: the adjoint is the raw opposite-sign transform; R2C: raw
+  C2R of the cotangent with interior bins halved);
 * at full size, R2C f32 [384,384,384] on a 4x8 grid, the gradient of the loss
   and the Poisson solve against torch's float64 FFT autograd (checker only).
 """
@@ -59,16 +59,28 @@ def test_vjp_matches_f64_central_differences(shape, dims):
 
 
 def test_vjp_matches_the_reference_backward():
+    """The VJP kernels against the oracle's restatement of the reference's raw
+    ``backward`` (execute_inverse with backward locals and no normalisation,
+    distributed.rs:1448-1500, distributed/r2c.rs:3410-3511): for C2C the
+    adjoint of forward is the raw opposite-sign transform; for R2C it is the
+    raw C2R of the cotangent with the interior bins of the reduced axis
+    halved."""
+    import pencil_oracle as po
+    from pb_testutil import oracle_pencil
+
     torch.manual_seed(4)
-    topo = pb.MpiTopology((2, 2))
-    c2c = pb.C2cPlan.from_shape(topo, (12, 10, 8), (), dtype=torch.complex128)
+    dims, shape = (2, 2), (12, 10, 8)
+    topo = pb.MpiTopology(dims)
+    c2c = pb.C2cPlan.from_shape(topo, shape, (), dtype=torch.complex128)
     g = torch.randn(c2c.info.output_elems, dtype=torch.complex128, device="cuda")
-    a, b = c2c.allocate_input(), c2c.allocate_input()
+    a = c2c.allocate_input()
     c2c.vjp_forward(g, a)
-    c2c.backward(g, b)
+    route = po.c2c_route(po.Topology(dims), shape)
+    locs = po.split_flat(oracle_pencil(c2c.output_pencil), g.cpu().numpy(), 1)
+    exp = torch.from_numpy(po.flat_concat(po.execute_reverse(route, locs, False))).cuda()
     torch.cuda.synchronize()
-    assert torch.allclose(a, b, rtol=0, atol=1e-12 * float(b.abs().max()))
-    r2c = pb.R2cPlan.from_shape(topo, (12, 10, 8), (), dtype=torch.float64)
+    assert torch.allclose(a, exp, rtol=0, atol=1e-12 * float(exp.abs().max()))
+    r2c = pb.R2cPlan.from_shape(topo, shape, (), dtype=torch.float64)
     # a cotangent the raw backward accepts: the spectrum of a real field, whose
     # DC and Nyquist planes are Hermitian in the transverse axes
     spec = r2c.allocate_output()
@@ -76,11 +88,14 @@ def test_vjp_matches_the_reference_backward():
     gs = r2c.output_pencil.gather(spec)
     half = gs.clone()
     half[..., 1:4] *= 0.5  # interior bins of the reduced axis (n = 8)
-    x1, x2 = r2c.allocate_input(), r2c.allocate_input()
+    x1 = r2c.allocate_input()
     r2c.vjp_forward(r2c.output_pencil.scatter(gs).contiguous(), x1)
-    r2c.backward(r2c.output_pencil.scatter(half).contiguous(), x2)
+    route = po.r2c_route(po.Topology(dims), shape)
+    hflat = r2c.output_pencil.scatter(half).contiguous().cpu().numpy()
+    locs = po.split_flat(oracle_pencil(r2c.output_pencil), hflat, 1)
+    exp = torch.from_numpy(po.flat_concat(po.execute_reverse(route, locs, False)).real.copy()).cuda()
     torch.cuda.synchronize()
-    assert torch.allclose(x1, x2, rtol=0, atol=1e-12 * float(x2.abs().max()))
+    assert torch.allclose(x1, exp, rtol=0, atol=1e-12 * float(exp.abs().max()))
 
 
 def test_full_size_384_gradient_and_poisson_against_float64():
