@@ -60,7 +60,10 @@ typedef enum pb_status {
   PB_ECUDA = 16,                     /* CUDA runtime error */
   PB_EINVALID_ARGUMENT = 17,
   PB_EWRONG_PLAN = 18,               /* workspace/batch does not belong to this plan */
-  PB_ENO_ALLOC_LIMIT = 19            /* plan workspace exceeds PB_NO_ALLOC_SCRATCH_BYTES */
+  PB_ENO_ALLOC_LIMIT = 19,           /* plan workspace exceeds PB_NO_ALLOC_SCRATCH_BYTES */
+  PB_EINTEGER_OVERFLOW = 20,         /* CollectiveError::IntegerOverflow (checked integer sum) */
+  PB_EPOISONED = 21,                 /* ArrayError::Poisoned (an in-place execution did not complete) */
+  PB_EIO = 22                        /* IoError: file access or an invalid / incomplete file */
 } pb_status;
 
 typedef enum pb_precision { PB_F32 = 0, PB_F64 = 1 } pb_precision;
@@ -228,6 +231,31 @@ int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int3
 #define PB_NO_ALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int pb_execute_no_alloc(pb_plan* plan, int32_t op, const void* in, void* out, void* stream);
 
+/* ---- in-place single-allocation arrays -------------------------------- */
+/* C2cInPlaceArray / R2cInPlaceArray and their completion states
+ * (crates/pencil-fft/src/distributed.rs:327-336, 845-862, 2106-2257;
+ * distributed/r2c.rs:3513-3810).  The caller owns one device buffer of
+ * *buffer_bytes (the larger of the input and output layouts) and a workspace
+ * of *workspace_bytes; an array handle tracks which layout the buffer holds.
+ * FORWARD (and VJP_INVERSE / VJP_BACKWARD) needs state INPUT and leaves
+ * OUTPUT; INVERSE, BACKWARD and VJP_FORWARD need OUTPUT and leave INPUT (a
+ * C2rPlan's FORWARD starts from its spectrum, state INPUT).  A state or
+ * argument mismatch is a preflight error (PB_EINPUT_LAYOUT_MISMATCH,
+ * PB_EPOISONED, ...) that changes nothing; a failure after the start
+ * (including a rejected C2R spectrum, PB_EINVALID_SPECTRUM, which leaves the
+ * buffer's data as it was) leaves the array POISONED, as
+ * run_in_place_transaction (distributed.rs:3776-3794) does.  Operations with
+ * the C2R spectrum check synchronise `stream`. */
+#define PB_STATE_INPUT 0
+#define PB_STATE_OUTPUT 1
+#define PB_STATE_POISONED 2
+typedef struct pb_inplace pb_inplace;
+int pb_inplace_sizes(const pb_plan* plan, int64_t* buffer_bytes, int64_t* workspace_bytes);
+int pb_inplace_create(pb_plan* plan, void* buffer, int32_t state, pb_inplace** array);
+int pb_inplace_state(const pb_inplace* array, int32_t* state);
+int pb_inplace_execute(pb_inplace* array, int32_t op, void* workspace, void* stream);
+int pb_inplace_destroy(pb_inplace* array);
+
 /* ---- spectral multipliers ---------------------------------------------- */
 /* out = m(k) * scale * in on the plan's FORWARD output layout (complex), k the
  * integer wavevector of each element (FFT order; the R2C-reduced axis holds
@@ -237,6 +265,58 @@ int pb_execute_no_alloc(pb_plan* plan, int32_t op, const void* in, void* out, vo
 #define PB_MULT_K2 0
 #define PB_MULT_POISSON 1
 int pb_spectral_multiply(const pb_plan* plan, int32_t mode, double scale, const void* in, void* out, void* stream);
+
+/* ---- global reductions and pointwise maps ----------------------------- */
+/* Scalar element types: the reference's fixed scalar set (SupportedScalar,
+ * crates/pencil-array/src/collectives.rs:100-107) with pencil-io's stable type
+ * codes (ScalarType::code, crates/pencil-io/src/catalog.rs:24-66). */
+#define PB_SCALAR_I8 1
+#define PB_SCALAR_U8 2
+#define PB_SCALAR_I16 3
+#define PB_SCALAR_U16 4
+#define PB_SCALAR_I32 5
+#define PB_SCALAR_U32 6
+#define PB_SCALAR_I64 7
+#define PB_SCALAR_U64 8
+#define PB_SCALAR_F32 9
+#define PB_SCALAR_F64 10
+#define PB_SCALAR_C64 11
+#define PB_SCALAR_C128 12
+
+/* global_sum / global_min / global_max / l2_norm / any / all
+ * (crates/pencil-array/src/collectives.rs:519-590) over an array in `pencil`'s
+ * layout with extra_count extra elements per spatial point (all virtual
+ * ranks, concatenated).  Synchronous on `stream`.  *result receives: SUM the
+ * element type (integer sums are checked in each rank's storage order and
+ * then in rank order: PB_EINTEGER_OVERFLOW on any intermediate overflow);
+ * MIN/MAX the element type, *has_value = 0 for an empty array (complex types:
+ * PB_EINVALID_ARGUMENT); L2_NORM a float for F32/C64, else a double (NaN if
+ * any NaN, +inf if any infinity); ANY/ALL an int32_t (empty: any 0, all 1). */
+#define PB_REDUCE_SUM 0
+#define PB_REDUCE_MIN 1
+#define PB_REDUCE_MAX 2
+#define PB_REDUCE_L2_NORM 3
+#define PB_REDUCE_ANY 4
+#define PB_REDUCE_ALL 5
+int pb_reduce(int32_t op, int32_t scalar, const pb_pencil_desc* pencil, int64_t extra_count, const void* data,
+              void* result, int32_t* has_value, void* stream);
+
+/* pointwise2 / pointwise3 (crates/pencil-array/src/pointwise.rs:40-110,
+ * 492-600) with a fixed operation set, on arrays of one spatial layout
+ * (`pencil`) and extra shapes of equal rank: an operand's extra extent equals
+ * the output's or is 1 (broadcast), else PB_ESHAPE_MISMATCH
+ * (PointwiseError::ExtraExtentMismatch).  Scalars F32/F64/C64/C128; alpha and
+ * beta are (re, im) pairs or NULL (1 and 1); real types take real factors.
+ * `out` may be `a` (the in-place forms).  Asynchronous on `stream`. */
+#define PB_PW_AXPBY 0     /* out = alpha*a + beta*b (b may be NULL: out = alpha*a) */
+#define PB_PW_MUL 1       /* out = alpha*a*b */
+#define PB_PW_CONJ_MUL 2  /* out = alpha*conj(a)*b */
+#define PB_PW_DIV 3       /* out = alpha*a/b */
+#define PB_PW_FMA 4       /* out = a*b + c */
+#define PB_PW_ABS2 5      /* out = |a|^2 */
+int pb_pointwise(int32_t op, int32_t scalar, const pb_pencil_desc* pencil, int32_t extra_ndim, const int64_t* extra_out,
+                 void* out, const int64_t* extra_a, const void* a, const int64_t* extra_b, const void* b,
+                 const int64_t* extra_c, const void* c, const double* alpha, const double* beta, void* stream);
 
 /* ---- ragged batches ---------------------------------------------------- */
 /* The collections API (crates/pencil-fft/src/distributed/collections.rs:1-17)
@@ -281,10 +361,36 @@ int pb_transpose_execute(pb_transpose* plan, const void* src, void* dst, void* s
 /* The unfused steps with the reference's segment layout: pack_source
  * (transpose.rs:1126-1176), the MPI_Alltoallv of every sub-communicator
  * (alltoallv_transpose.rs:324-367), unpack_destination (transpose.rs:1233-1281). */
+/* execute_in_place (crates/pencil-array/src/alltoallv_transpose.rs:259-310):
+ * `buffer` (*buffer_bytes, the larger layout) holds the source layout before
+ * and the destination layout after the call; `workspace` holds
+ * *workspace_bytes. */
+int pb_transpose_in_place_sizes(const pb_transpose* plan, int64_t* buffer_bytes, int64_t* workspace_bytes);
+int pb_transpose_execute_in_place(pb_transpose* plan, void* buffer, void* workspace, void* stream);
 int pb_transpose_pack(pb_transpose* plan, const void* src, void* send, void* stream);
 int pb_transpose_exchange(pb_transpose* plan, const void* send, void* receive, void* stream);
 int pb_transpose_unpack(pb_transpose* plan, const void* receive, void* dst, void* stream);
 int pb_transpose_destroy(pb_transpose* plan);
+
+/* ---- field persistence ------------------------------------------------- */
+/* write_mpi / read_mpi of pencil-io in its native MPI-IO file format, version
+ * 1 (crates/pencil-io/src/mpi_io.rs:20-25, 1492-1606, 1760-1830): a 96-byte
+ * header prefix ("PENCILIO", version, lengths, commit marker, type code and
+ * width as PB_SCALAR_*, ranks), the global shape, extra shape, writer process
+ * grid and writer permutation, then the global array in canonical row-major
+ * little-endian [extra..., spatial...] order.  `data` is a device buffer in
+ * `pencil`'s layout (all virtual ranks concatenated).  Writes create the file
+ * exclusively (an existing path is PB_EIO) and set the commit marker only
+ * after the payload is flushed.  Reads accept committed files whose type and
+ * global and extra shapes equal the request (else PB_ESHAPE_MISMATCH / PB_EIO)
+ * and stage and check the whole payload before writing `data`, so a failed
+ * read leaves `data` unchanged; the writer's grid and permutation need not
+ * match the reader's.  Synchronous on `stream`; the layout change runs on
+ * the GPU for 4/8/16-byte elements. */
+int pb_field_write(const char* path, const pb_pencil_desc* pencil, int32_t extra_ndim, const int64_t* extra,
+                   int32_t scalar, const void* data, void* stream);
+int pb_field_read(const char* path, const pb_pencil_desc* pencil, int32_t extra_ndim, const int64_t* extra,
+                  int32_t scalar, void* data, void* stream);
 
 /* ---- affine remap ----------------------------------------------------- */
 /* SpatialRemapPlan::prepare (spatial_remap.rs:221-338); offsets are i64 (the

@@ -912,3 +912,159 @@ def remap_source_offsets(src: Pencil, dst: Pencil, signs, offsets):
             res[lin] = (q, off)
         out.append(res)
     return out
+
+
+# ---------------------------------------------------------------------------
+# global reductions and pointwise maps: crates/pencil-array/src/collectives.rs,
+# crates/pencil-array/src/pointwise.rs
+# ---------------------------------------------------------------------------
+
+
+class IntegerOverflow(OracleError):
+    """CollectiveError::IntegerOverflow."""
+
+
+_INT_RANGE = {np.dtype(t): (int(np.iinfo(t).min), int(np.iinfo(t).max))
+              for t in (np.int8, np.uint8, np.int16, np.uint16, np.int32, np.uint32, np.int64, np.uint64)}
+
+
+def _checked_fold(values, lo, hi):
+    """Storage-order fold with every addition checked (local_sum,
+    collectives.rs:207-212): overflow of any prefix is an error."""
+    s = 0
+    for v in values:
+        s += int(v)
+        if s < lo or s > hi:
+            raise IntegerOverflow()
+    return s
+
+
+def global_sum(locals_):
+    """global_sum (collectives.rs:519-527) over the ranks' local arrays.
+
+    Integers: each rank's checked storage-order fold, then the checked
+    rank-order fold of the partials (integer_collective_sum_prepared,
+    collectives.rs:2575-2600).  Floats and complex: the sum with the input's
+    non-finite flags deciding each component (sum_component_*,
+    collectives.rs:2501-2523); the finite values are summed in float64."""
+    dt = np.asarray(locals_[0]).dtype
+    if dt in _INT_RANGE:
+        lo, hi = _INT_RANGE[dt]
+        partials = [_checked_fold(np.asarray(a).ravel().tolist(), lo, hi) for a in locals_]
+        return _checked_fold(partials, lo, hi)
+    flat = np.concatenate([np.asarray(a).ravel() for a in locals_]) if locals_ else np.zeros(0, dt)
+
+    def component(v):
+        v = v.astype(np.float64)
+        nan, pinf, ninf = np.isnan(v).any(), np.isposinf(v).any(), np.isneginf(v).any()
+        if nan or (pinf and ninf):
+            return math.nan
+        if pinf:
+            return math.inf
+        if ninf:
+            return -math.inf
+        return float(np.sum(v))
+
+    if np.iscomplexobj(flat):
+        return complex(component(flat.real), component(flat.imag))
+    return component(flat)
+
+
+def global_extreme(locals_, minimum: bool):
+    """global_min / global_max (collectives.rs:530-550, mapped_extreme_layout
+    2066-2096): None when globally empty, NaN when any value is NaN."""
+    flat = np.concatenate([np.asarray(a).ravel() for a in locals_])
+    if flat.size == 0:
+        return None
+    if np.iscomplexobj(flat):
+        raise OracleError("complex values are not ordered")
+    if flat.dtype.kind == "f" and np.isnan(flat).any():
+        return math.nan
+    v = flat.min() if minimum else flat.max()
+    return int(v) if flat.dtype.kind in "iu" else float(v)
+
+
+def l2_norm(locals_):
+    """l2_norm (collectives.rs:557-565, norm_values 2215-2250): NaN if any
+    NaN, +inf if any infinity or the largest |v| is infinite, 0 when empty or
+    all zero, else max|v| * sqrt(sum((|v| / max|v|)^2)) in float64."""
+    flat = np.concatenate([np.asarray(a).ravel() for a in locals_])
+    if np.iscomplexobj(flat):
+        re, im = flat.real.astype(np.float64), flat.imag.astype(np.float64)
+        if np.isnan(re).any() or np.isnan(im).any():
+            return math.nan
+        if np.isinf(re).any() or np.isinf(im).any():
+            return math.inf
+        a = np.hypot(re, im)
+    else:
+        a = np.abs(flat.astype(np.float64))
+        if np.isnan(a).any():
+            return math.nan
+        if np.isinf(a).any():
+            return math.inf
+    if a.size == 0:
+        return 0.0
+    mx = float(a.max())
+    if math.isinf(mx):
+        return math.inf
+    if mx == 0.0:
+        return 0.0
+    return mx * math.sqrt(float(np.sum((a / mx) ** 2)))
+
+
+def global_truth(locals_, any_: bool):
+    """any / all (collectives.rs:567-585): the truth of a value is value != 0
+    (complex: either component); empty arrays give any = False, all = True."""
+    flat = np.concatenate([np.asarray(a).ravel() for a in locals_])
+    t = flat != 0
+    return bool(t.any()) if any_ else bool(t.all())
+
+
+def pointwise(op, out_extra, a, b=None, c=None, alpha=1.0, beta=1.0):
+    """pointwise2 / pointwise3 (pointwise.rs:40-110, 492-600) on global arrays
+    [extra..., spatial...]: operands broadcast from extra extent one."""
+    if op == "axpby":
+        r = alpha * a + (beta * b if b is not None else 0)
+    elif op == "mul":
+        r = alpha * a * b
+    elif op == "conj_mul":
+        r = alpha * np.conj(a) * b
+    elif op == "div":
+        r = alpha * a / b
+    elif op == "fma":
+        r = a * b + c
+    elif op == "abs2":
+        r = (a * np.conj(a)).real.astype(a.dtype) if np.iscomplexobj(a) else a * a
+    else:
+        raise OracleError(op)
+    return np.broadcast_to(r, tuple(out_extra) + r.shape[len(out_extra):])
+
+
+# ---------------------------------------------------------------------------
+# field files: pencil-io native MPI-IO format v1 (crates/pencil-io/src/mpi_io.rs)
+# ---------------------------------------------------------------------------
+
+IO_COMMIT = 0x434F_4D4D_4954_5445
+IO_INCOMPLETE = 0x494E_434F_4D50_4C45
+IO_CODES = {np.dtype(np.int8): (1, 1), np.dtype(np.uint8): (2, 1), np.dtype(np.int16): (3, 2),
+            np.dtype(np.uint16): (4, 2), np.dtype(np.int32): (5, 4), np.dtype(np.uint32): (6, 4),
+            np.dtype(np.int64): (7, 8), np.dtype(np.uint64): (8, 8), np.dtype(np.float32): (9, 4),
+            np.dtype(np.float64): (10, 8), np.dtype(np.complex64): (11, 8), np.dtype(np.complex128): (12, 16)}
+
+
+def field_file_bytes(glob: np.ndarray, extra_shape, writer_grid, writer_permutation, committed=True) -> bytes:
+    """The bytes write_mpi produces (Header::for_write / encode_into,
+    mpi_io.rs:1492-1606): 96-byte prefix, global / extra / grid / permutation
+    arrays as little-endian u64, then the canonical row-major payload of the
+    global array [extra..., spatial...]."""
+    extra_shape = tuple(int(e) for e in extra_shape)
+    spatial = glob.shape[len(extra_shape):]
+    code, width = IO_CODES[glob.dtype]
+    n, er, gr = len(spatial), len(extra_shape), len(writer_grid)
+    hlen = 96 + (n + er + gr + n) * 8
+    words = [1, hlen, IO_COMMIT if committed else IO_INCOMPLETE, n, code, width, er, hlen,
+             int(glob.size) * width, gr, 0]
+    head = b"PENCILIO" + b"".join(int(w).to_bytes(8, "little") for w in words)
+    arrays = list(spatial) + list(extra_shape) + list(writer_grid) + list(writer_permutation)
+    head += b"".join(int(v).to_bytes(8, "little") for v in arrays)
+    return head + np.ascontiguousarray(glob).astype(glob.dtype.newbyteorder("<")).tobytes()

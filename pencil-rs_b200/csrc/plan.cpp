@@ -15,6 +15,9 @@
 // the layout of the next transforming stage; identity stages cost nothing
 // beyond the composed layout change.
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <array>
@@ -1704,6 +1707,9 @@ const char* pb_status_string(int status) {
     case PB_EINVALID_ARGUMENT: return "invalid argument";
     case PB_EWRONG_PLAN: return "workspace or batch belongs to another plan";
     case PB_ENO_ALLOC_LIMIT: return "plan workspace exceeds the fixed no-allocation scratch (PB_NO_ALLOC_SCRATCH_BYTES)";
+    case PB_EINTEGER_OVERFLOW: return "checked integer sum overflowed (CollectiveError::IntegerOverflow)";
+    case PB_EPOISONED: return "in-place array poisoned by an execution that did not complete (ArrayError::Poisoned)";
+    case PB_EIO: return "field file could not be written or read, or is invalid or incomplete (IoError)";
     default: return "unknown status";
   }
 }
@@ -1976,6 +1982,124 @@ int pb_execute_status_async(pb_plan* plan, void* workspace, int32_t* status, voi
                             cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
     return (int)PB_OK;
   });
+}
+
+// ---- in-place single-allocation arrays ------------------------------------
+// C2cInPlaceArray / R2cInPlaceArray and the completion-state machine
+// (crates/pencil-fft/src/distributed.rs:327-336, 845-862, 2106-2257,
+// run_in_place_transaction 3776-3794; distributed/r2c.rs:3513-3810): one
+// caller-owned buffer holds the input before a forward and the output after
+// it.  An operation of two or more passes reads the buffer in its first pass
+// and writes it in its last, the intermediate layouts ping-pong through the
+// workspace, so it runs in place unchanged; a single-pass operation writes a
+// staging area after the plan workspace and is copied back.
+
+}  // extern "C"
+
+struct pb_inplace {
+  pb_plan* plan = nullptr;
+  void* buffer = nullptr;
+  int state = PB_STATE_INPUT;
+};
+
+namespace pb {
+
+static size_t layout_bytes(const pb_plan& P, bool out_side) {
+  const Pencil& p = out_side ? P.fout : P.fin;
+  const bool cplx = out_side ? P.fout_complex : P.fin_complex;
+  return (size_t)p.total(P.extra) * (size_t)P.real_bytes * (cplx ? 2 : 1);
+}
+
+static int pass_count(const pb_plan& P, int mode) {
+  int n = 0;
+  for (const Step& st : P.prog[mode].steps) n += st.type == 0;
+  return n;
+}
+
+static size_t inplace_staging(const pb_plan& P) {
+  for (int op = PB_FORWARD; op <= PB_VJP_BACKWARD; ++op)
+    if (pass_count(P, user_mode(P, op)) == 1) return (std::max(layout_bytes(P, false), layout_bytes(P, true)) + 255) & ~size_t(255);
+  return 0;
+}
+
+static int inplace_execute(pb_inplace* A, int op, void* ws, cudaStream_t s) {
+  pb_plan& P = *A->plan;
+  const int mode = user_mode(P, op);
+  const bool fwd_like = (mode == M_F || mode == M_FS || mode == M_AB || mode == M_AI);
+  // the user-facing input of FORWARD is the plan's input layout, except for
+  // a C2rPlan, whose FORWARD starts from the spectrum
+  const bool from_input = P.c2r_family ? !fwd_like : fwd_like;
+  if (A->state == PB_STATE_POISONED) return PB_EPOISONED;
+  if (A->state != (from_input ? PB_STATE_INPUT : PB_STATE_OUTPUT)) return PB_EINPUT_LAYOUT_MISMATCH;
+  const Program& prog = P.prog[mode];
+  const int npass = pass_count(P, mode);
+  if (!ws && (prog.steps.size() > 1 || prog.has_stats || npass == 1)) return PB_ENULL;
+  if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) return PB_EINVALID_ARGUMENT;
+  // preflight done: from here a failure leaves the array poisoned
+  A->state = PB_STATE_POISONED;
+  auto spectrum_ok = [&] {
+    int st[2] = {0, 0};
+    cuda_ok(cudaMemcpyAsync(st, static_cast<unsigned char*>(ws) + P.status_off, sizeof(st), cudaMemcpyDeviceToHost, s));
+    cuda_ok(cudaStreamSynchronize(s));
+    return st[0] == 0 && st[1] == 0;
+  };
+  if (npass != 1) {
+    run(&P, op, A->buffer, A->buffer, ws, s, nullptr, 0, nullptr);
+    if (prog.has_stats && !spectrum_ok()) return PB_EINVALID_SPECTRUM;
+  } else {
+    void* stage = static_cast<unsigned char*>(ws) + ((P.ws_bytes + 255) & ~size_t(255));
+    run(&P, op, A->buffer, stage, ws, s, nullptr, 0, nullptr);
+    // a rejected spectrum leaves the buffer as it was: nothing is copied back
+    if (prog.has_stats && !spectrum_ok()) return PB_EINVALID_SPECTRUM;
+    cuda_ok(cudaMemcpyAsync(A->buffer, stage, layout_bytes(P, fwd_like), cudaMemcpyDeviceToDevice, s));
+  }
+  A->state = from_input ? PB_STATE_OUTPUT : PB_STATE_INPUT;
+  return PB_OK;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_inplace_sizes(const pb_plan* plan, int64_t* buffer_bytes, int64_t* workspace_bytes) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    const size_t buf = std::max(layout_bytes(*plan, false), layout_bytes(*plan, true));
+    const size_t stage = inplace_staging(*plan);
+    if (buffer_bytes) *buffer_bytes = (int64_t)buf;
+    if (workspace_bytes) *workspace_bytes = (int64_t)(stage ? ((plan->ws_bytes + 255) & ~size_t(255)) + stage : plan->ws_bytes);
+    return (int)PB_OK;
+  });
+}
+
+int pb_inplace_create(pb_plan* plan, void* buffer, int32_t state, pb_inplace** array) {
+  if (!plan || !buffer || !array) return PB_ENULL;
+  if (state != PB_STATE_INPUT && state != PB_STATE_OUTPUT) return PB_EINVALID_ARGUMENT;
+  if (reinterpret_cast<uintptr_t>(buffer) % 16 != 0) return PB_EINVALID_ARGUMENT;
+  pb_inplace* a = new (std::nothrow) pb_inplace();
+  if (!a) return PB_EUNSUPPORTED;
+  a->plan = plan;
+  a->buffer = buffer;
+  a->state = state;
+  *array = a;
+  return PB_OK;
+}
+
+int pb_inplace_state(const pb_inplace* array, int32_t* state) {
+  if (!array || !state) return PB_ENULL;
+  *state = array->state;
+  return PB_OK;
+}
+
+int pb_inplace_execute(pb_inplace* array, int32_t op, void* workspace, void* stream) {
+  if (!array) return PB_ENULL;
+  const int rc = guard([&] { return inplace_execute(array, op, workspace, static_cast<cudaStream_t>(stream)); });
+  return rc;
+}
+
+int pb_inplace_destroy(pb_inplace* array) {
+  delete array;
+  return PB_OK;
 }
 
 int pb_execute_status(pb_plan* plan, void* workspace, void* stream) {
@@ -2368,6 +2492,318 @@ int pb_transpose_execute(pb_transpose* plan, const void* src, void* dst, void* s
       G.out = dst;
       cuda_ok(launch_remap(G, s));
     }
+    return (int)PB_OK;
+  });
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// field persistence: pencil-io's native MPI-IO format, version 1
+// (crates/pencil-io/src/mpi_io.rs:20-25, Header::for_write / encode_into
+// 1492-1606, V1Fields 1760-1830; README.md "Native collective I/O"): a 96-byte
+// prefix of little-endian u64 words (magic "PENCILIO", version, header
+// length, commit marker, spatial rank, type code, type width, extra rank,
+// payload offset, payload bytes, writer grid rank, reserved 0), then the
+// global shape, extra shape, writer process grid and writer permutation
+// (u64 each), then the payload: the global array in canonical row-major
+// [extra..., spatial...] order, little endian.  The file is created
+// exclusively with the incomplete marker, and the commit marker is written
+// only after the payload is flushed.  Readers accept committed files only and
+// stage and validate the whole payload before they touch the destination.
+// The layout change between the rank-concatenated device buffer and the
+// canonical order runs on the GPU for 4/8/16-byte elements (tiled permute
+// copies) and on the host otherwise.
+// ===========================================================================
+namespace pb {
+
+constexpr uint64_t kIoVersion = 1;
+constexpr uint64_t kCommit = 0x434f4d4d49545445ULL;
+constexpr uint64_t kIncomplete = 0x494e434f4d504c45ULL;
+constexpr size_t kPrefix = 96;
+
+static int scalar_width(int code) {
+  static const int w[13] = {0, 1, 1, 2, 2, 4, 4, 8, 8, 4, 8, 8, 16};
+  return (code >= 1 && code <= 12) ? w[code] : 0;
+}
+
+static void put_u64(std::vector<unsigned char>& b, size_t off, uint64_t v) {
+  for (int i = 0; i < 8; ++i) b[off + i] = (unsigned char)(v >> (8 * i));
+}
+static uint64_t get_u64(const unsigned char* b, size_t off) {
+  uint64_t v = 0;
+  for (int i = 7; i >= 0; --i) v = (v << 8) | b[off + i];
+  return v;
+}
+
+// the copy between a pencil layout and the canonical global order: per rank,
+// the box of its global ranges with both addresses affine
+static std::vector<XTile> canonical_tiles(const Pencil& P, long long extra, bool to_canonical, int* row) {
+  HostLayout h(P, extra);
+  long long glob = 1, zero[MAXN] = {}, shape[MAXN];
+  for (int a = 0; a < P.N; ++a) {
+    shape[a] = P.shape[a];
+    glob *= P.shape[a];
+  }
+  const AffineMap canon = segment_map(P.N, 0, glob, zero, shape);
+  std::vector<XTile> tiles;
+  for (int r = 0; r < P.nranks(); ++r) {
+    long long lo[MAXN], ext[MAXN];
+    P.local(r, lo, ext);
+    if (to_canonical)
+      box_xtiles(P.N, lo, ext, extra, rank_map(h, r), canon, P.perm[P.N - 1], P.N - 1, tiles);
+    else
+      box_xtiles(P.N, lo, ext, extra, canon, rank_map(h, r), P.N - 1, P.perm[P.N - 1], tiles);
+  }
+  *row = P.perm[P.N - 1] == P.N - 1;
+  return tiles;
+}
+
+// host form of the same copy for 1- and 2-byte elements
+static void canonical_host(const Pencil& P, long long extra, int width, const unsigned char* src, unsigned char* dst,
+                           bool to_canonical) {
+  HostLayout h(P, extra);
+  const int N = P.N;
+  for (int r = 0; r < P.nranks(); ++r) {
+    long long lo[MAXN], ext[MAXN];
+    P.local(r, lo, ext);
+    long long cnt = 1;
+    for (int a = 0; a < N; ++a) cnt *= ext[a];
+    for (long long e = 0; e < extra; ++e)
+      for (long long i = 0; i < cnt; ++i) {
+        long long g[MAXN], rem = i, coff = 0, rs = 1;
+        for (int a = N - 1; a >= 0; --a) {
+          g[a] = lo[a] + rem % ext[a];
+          rem /= ext[a];
+        }
+        for (int a = N - 1; a >= 0; --a) {
+          coff += g[a] * rs;
+          rs *= P.shape[a];
+        }
+        coff += e * rs;
+        const long long poff = h.offset(e, g, nullptr);
+        if (to_canonical)
+          std::memcpy(dst + coff * width, src + poff * width, width);
+        else
+          std::memcpy(dst + poff * width, src + coff * width, width);
+      }
+  }
+}
+
+// device buffer <-> canonical host payload
+static void canonical_copy(const Pencil& P, long long extra, int width, void* dev, unsigned char* host, bool to_host,
+                           cudaStream_t s) {
+  const size_t bytes = (size_t)P.total(extra) * (size_t)width;
+  if (bytes == 0) return;
+  if (width == 4 || width == 8 || width == 16) {
+    int row = 0;
+    const std::vector<XTile> tiles = canonical_tiles(P, extra, to_host, &row);
+    void* stage = nullptr;
+    void* dtiles = nullptr;
+    cuda_ok(cudaMalloc(&stage, bytes));
+    if (cudaMalloc(&dtiles, std::max<size_t>(tiles.size(), 1) * sizeof(XTile)) != cudaSuccess) {
+      cudaFree(stage);
+      fail(PB_ECUDA);
+    }
+    cudaError_t e = cudaMemcpyAsync(dtiles, tiles.data(), tiles.size() * sizeof(XTile), cudaMemcpyHostToDevice, s);
+    XposeArgs X{};
+    X.tiles = static_cast<const XTile*>(dtiles);
+    X.ntiles = (long long)tiles.size();
+    X.elem_bytes = width;
+    X.row = row;
+    if (to_host) {
+      X.in = dev;
+      X.out = stage;
+      if (e == cudaSuccess) e = launch_xpose(X, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, s);
+    } else {
+      if (e == cudaSuccess) e = cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, s);
+      X.in = stage;
+      X.out = dev;
+      if (e == cudaSuccess) e = launch_xpose(X, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(stage);
+    cudaFree(dtiles);
+    cuda_ok(e);
+    return;
+  }
+  std::vector<unsigned char> tmp(bytes);
+  if (to_host) {
+    cuda_ok(cudaMemcpyAsync(tmp.data(), dev, bytes, cudaMemcpyDeviceToHost, s));
+    cuda_ok(cudaStreamSynchronize(s));
+    canonical_host(P, extra, width, tmp.data(), host, true);
+  } else {
+    canonical_host(P, extra, width, host, tmp.data(), false);
+    cuda_ok(cudaMemcpyAsync(dev, tmp.data(), bytes, cudaMemcpyHostToDevice, s));
+    cuda_ok(cudaStreamSynchronize(s));
+  }
+}
+
+static bool write_all(int fd, const unsigned char* p, size_t n, off_t off) {
+  while (n > 0) {
+    const ssize_t w = pwrite(fd, p, n, off);
+    if (w <= 0) return false;
+    p += w;
+    n -= (size_t)w;
+    off += w;
+  }
+  return true;
+}
+
+static bool read_all(int fd, unsigned char* p, size_t n, off_t off) {
+  while (n > 0) {
+    const ssize_t r = pread(fd, p, n, off);
+    if (r <= 0) return false;
+    p += r;
+    n -= (size_t)r;
+    off += r;
+  }
+  return true;
+}
+
+static Pencil io_pencil(const pb_pencil_desc* pd, int extra_ndim, const int64_t* extra, long long* extra_count) {
+  if (!pd) fail(PB_ENULL);
+  if (extra_ndim < 0 || extra_ndim > PB_MAX_DIMS || (extra_ndim > 0 && !extra)) fail(PB_EINVALID_ARGUMENT);
+  Pencil P = pencil_from_desc(pd);
+  long long e = 1;
+  for (int i = 0; i < extra_ndim; ++i) {
+    if (extra[i] < 0) fail(PB_EINVALID_ARGUMENT);
+    e *= extra[i];
+  }
+  *extra_count = e;
+  return P;
+}
+
+static int field_write(const char* path, const pb_pencil_desc* pd, int extra_ndim, const int64_t* extra, int scalar,
+                       const void* data, cudaStream_t s) {
+  if (!path) return PB_ENULL;
+  const int width = scalar_width(scalar);
+  if (width == 0) return PB_EINVALID_ARGUMENT;
+  long long ec = 0;
+  const Pencil P = io_pencil(pd, extra_ndim, extra, &ec);
+  const long long count = P.total(ec);
+  if (count > 0 && !data) return PB_ENULL;
+  // header: prefix + global, extra, writer grid, writer permutation
+  const size_t hlen = kPrefix + (size_t)(P.N + extra_ndim + P.M + P.N) * 8;
+  const uint64_t payload = (uint64_t)count * (uint64_t)width;
+  std::vector<unsigned char> h(hlen, 0);
+  std::memcpy(h.data(), "PENCILIO", 8);
+  put_u64(h, 8, kIoVersion);
+  put_u64(h, 16, hlen);
+  put_u64(h, 24, kIncomplete);
+  put_u64(h, 32, (uint64_t)P.N);
+  put_u64(h, 40, (uint64_t)scalar);
+  put_u64(h, 48, (uint64_t)width);
+  put_u64(h, 56, (uint64_t)extra_ndim);
+  put_u64(h, 64, hlen);
+  put_u64(h, 72, payload);
+  put_u64(h, 80, (uint64_t)P.M);
+  put_u64(h, 88, 0);
+  size_t o = kPrefix;
+  for (int a = 0; a < P.N; ++a, o += 8) put_u64(h, o, (uint64_t)P.shape[a]);
+  for (int i = 0; i < extra_ndim; ++i, o += 8) put_u64(h, o, (uint64_t)extra[i]);
+  for (int t = 0; t < P.M; ++t, o += 8) put_u64(h, o, (uint64_t)P.grid[t]);
+  for (int q = 0; q < P.N; ++q, o += 8) put_u64(h, o, (uint64_t)P.perm[q]);
+  // stage the canonical payload before the file exists
+  std::vector<unsigned char> body((size_t)payload);
+  canonical_copy(P, ec, width, const_cast<void*>(data), body.data(), true, s);
+  const int fd = open(path, O_WRONLY | O_CREAT | O_EXCL, 0644);  // exclusive: never overwrite
+  if (fd < 0) return PB_EIO;
+  bool ok = write_all(fd, h.data(), h.size(), 0) && write_all(fd, body.data(), body.size(), (off_t)hlen) &&
+            fsync(fd) == 0;
+  if (ok) {
+    unsigned char m[8];
+    for (int i = 0; i < 8; ++i) m[i] = (unsigned char)(kCommit >> (8 * i));
+    ok = write_all(fd, m, 8, 24) && fsync(fd) == 0;
+  }
+  ok = (close(fd) == 0) && ok;
+  return ok ? PB_OK : PB_EIO;
+}
+
+static int field_read(const char* path, const pb_pencil_desc* pd, int extra_ndim, const int64_t* extra, int scalar,
+                      void* data, cudaStream_t s) {
+  if (!path) return PB_ENULL;
+  const int width = scalar_width(scalar);
+  if (width == 0) return PB_EINVALID_ARGUMENT;
+  long long ec = 0;
+  const Pencil P = io_pencil(pd, extra_ndim, extra, &ec);
+  const long long count = P.total(ec);
+  if (count > 0 && !data) return PB_ENULL;
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) return PB_EIO;
+  struct FdGuard {
+    int fd;
+    ~FdGuard() { close(fd); }
+  } guard_fd{fd};
+  struct stat st {};
+  if (fstat(fd, &st) != 0 || (size_t)st.st_size < kPrefix) return PB_EIO;
+  unsigned char pre[kPrefix];
+  if (!read_all(fd, pre, kPrefix, 0)) return PB_EIO;
+  // identity, commit marker (an incomplete file is refused), reserved word
+  if (std::memcmp(pre, "PENCILIO", 8) != 0 || get_u64(pre, 8) != kIoVersion) return PB_EIO;
+  if (get_u64(pre, 24) != kCommit || get_u64(pre, 88) != 0) return PB_EIO;
+  const uint64_t n = get_u64(pre, 32), er = get_u64(pre, 56), gr = get_u64(pre, 80), hlen = get_u64(pre, 16);
+  if (n > 1024 || er > 1024 || gr > n) return PB_EIO;
+  if (hlen != kPrefix + (n + er + gr + n) * 8 || get_u64(pre, 64) != hlen) return PB_EIO;
+  // the file must hold exactly the requested type and logical shapes
+  if (get_u64(pre, 40) != (uint64_t)scalar || get_u64(pre, 48) != (uint64_t)width) return PB_ESHAPE_MISMATCH;
+  if (n != (uint64_t)P.N || er != (uint64_t)extra_ndim) return PB_ESHAPE_MISMATCH;
+  std::vector<unsigned char> arr((size_t)(hlen - kPrefix));
+  if (!read_all(fd, arr.data(), arr.size(), (off_t)kPrefix)) return PB_EIO;
+  for (uint64_t a = 0; a < n; ++a)
+    if (get_u64(arr.data(), a * 8) != (uint64_t)P.shape[a]) return PB_ESHAPE_MISMATCH;
+  for (uint64_t i = 0; i < er; ++i)
+    if (get_u64(arr.data(), (n + i) * 8) != (uint64_t)extra[i]) return PB_ESHAPE_MISMATCH;
+  std::vector<int> seen(n, 0);  // the writer permutation is provenance, but must be a permutation
+  for (uint64_t q = 0; q < n; ++q) {
+    const uint64_t v = get_u64(arr.data(), (n + er + gr + q) * 8);
+    if (v >= n || seen[v]++) return PB_EIO;
+  }
+  const uint64_t payload = (uint64_t)count * (uint64_t)width;
+  if (get_u64(pre, 72) != payload || (uint64_t)st.st_size < hlen + payload) return PB_EIO;
+  std::vector<unsigned char> body((size_t)payload);
+  if (!read_all(fd, body.data(), body.size(), (off_t)hlen)) return PB_EIO;
+  canonical_copy(P, ec, width, data, body.data(), false, s);
+  return PB_OK;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_field_write(const char* path, const pb_pencil_desc* pencil, int32_t extra_ndim, const int64_t* extra,
+                   int32_t scalar, const void* data, void* stream) {
+  return guard([&] { return field_write(path, pencil, extra_ndim, extra, scalar, data, static_cast<cudaStream_t>(stream)); });
+}
+
+int pb_field_read(const char* path, const pb_pencil_desc* pencil, int32_t extra_ndim, const int64_t* extra,
+                  int32_t scalar, void* data, void* stream) {
+  return guard([&] { return field_read(path, pencil, extra_ndim, extra, scalar, data, static_cast<cudaStream_t>(stream)); });
+}
+
+// execute_in_place (alltoallv_transpose.rs:259-310; LocalTransposePlan's in
+// ManyPencilArray): one buffer holds the source layout before the call and
+// the destination layout after it.  The fused transpose pass writes the
+// workspace, which is copied back.
+int pb_transpose_in_place_sizes(const pb_transpose* plan, int64_t* buffer_bytes, int64_t* workspace_bytes) {
+  if (!plan) return PB_ENULL;
+  const long long s = plan->src.total(plan->extra) * plan->elem_bytes;
+  const long long d = plan->dst.total(plan->extra) * plan->elem_bytes;
+  if (buffer_bytes) *buffer_bytes = std::max(s, d);
+  if (workspace_bytes) *workspace_bytes = d;
+  return PB_OK;
+}
+
+int pb_transpose_execute_in_place(pb_transpose* plan, void* buffer, void* workspace, void* stream) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (plan->extra == 0) return (int)PB_OK;
+    if (!buffer || !workspace) return (int)PB_ENULL;
+    const int rc = pb_transpose_execute(plan, buffer, workspace, stream);
+    if (rc != PB_OK) return rc;
+    const size_t d = (size_t)plan->dst.total(plan->extra) * (size_t)plan->elem_bytes;
+    cuda_ok(cudaMemcpyAsync(buffer, workspace, d, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
     return (int)PB_OK;
   });
 }

@@ -12,6 +12,7 @@ from .plans import (  # noqa: F401
     C2rPlan,
     DhtPlan,
     DistributedLayout,
+    InPlaceArray,
     LocalTransposePlan,
     MixedC2cPlan,
     MixedR2cPlan,
@@ -25,7 +26,7 @@ from .plans import (  # noqa: F401
 )
 
 __all__ = [
-    "AllToAllvTransposePlan", "C2cPlan", "C2rPlan", "DhtPlan", "DistributedLayout", "InvalidSpectrum",
+    "AllToAllvTransposePlan", "C2cPlan", "C2rPlan", "DhtPlan", "DistributedLayout", "InPlaceArray", "InvalidSpectrum",
     "LocalTransposePlan", "MixedC2cPlan", "MixedR2cPlan", "MpiTopology", "Pencil", "PencilError", "PlanBatch", "R2cPlan",
     "R2rPlan", "SpatialRemapPlan", "load", "route_pencils",
 ]

@@ -22,7 +22,8 @@ STATUS_NAMES = {
     4: "InvalidPermutation", 5: "InvalidLength", 6: "InvalidGraph", 7: "InputLayoutMismatch",
     8: "UnsupportedDecompositionChange", 9: "CountOverflow", 10: "ShapeMismatch", 11: "InvalidSign",
     12: "InvalidSpectrum", 13: "Timeout", 14: "Null", 15: "Unsupported", 16: "Cuda",
-    17: "InvalidArgument", 18: "WrongPlan", 19: "NoAllocLimit",
+    17: "InvalidArgument", 18: "WrongPlan", 19: "NoAllocLimit", 20: "IntegerOverflow", 21: "Poisoned",
+    22: "Io",
 }
 
 # pb_op
@@ -80,6 +81,12 @@ SIGNATURES = {
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),
     "pb_spectral_multiply": ([_P, C.c_int32, C.c_double, _P, _P, _P], C.c_int),
+    "pb_reduce": ([C.c_int32, C.c_int32, C.POINTER(PbPencilDesc), C.c_int64, _P, _P, C.POINTER(C.c_int32), _P],
+                  C.c_int),
+    "pb_pointwise": ([C.c_int32, C.c_int32, C.POINTER(PbPencilDesc), C.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                      _P, _P], C.c_int),
+    "pb_field_write": ([C.c_char_p, C.POINTER(PbPencilDesc), C.c_int32, _P, C.c_int32, _P, _P], C.c_int),
+    "pb_field_read": ([C.c_char_p, C.POINTER(PbPencilDesc), C.c_int32, _P, C.c_int32, _P, _P], C.c_int),
     "pb_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_P)],
                         C.c_int),
     "pb_batch_workspace_bytes": ([_P, C.POINTER(C.c_int64)], C.c_int),
@@ -93,6 +100,13 @@ SIGNATURES = {
                                    C.POINTER(_P)], C.c_int),
     "pb_transpose_workspace": ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "pb_transpose_execute": ([_P, _P, _P, _P], C.c_int),
+    "pb_transpose_in_place_sizes": ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+    "pb_transpose_execute_in_place": ([_P, _P, _P, _P], C.c_int),
+    "pb_inplace_sizes": ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+    "pb_inplace_create": ([_P, _P, C.c_int32, C.POINTER(_P)], C.c_int),
+    "pb_inplace_state": ([_P, C.POINTER(C.c_int32)], C.c_int),
+    "pb_inplace_execute": ([_P, C.c_int32, _P, _P], C.c_int),
+    "pb_inplace_destroy": ([_P], C.c_int),
     "pb_transpose_pack": ([_P, _P, _P, _P], C.c_int),
     "pb_transpose_exchange": ([_P, _P, _P, _P], C.c_int),
     "pb_transpose_unpack": ([_P, _P, _P, _P], C.c_int),

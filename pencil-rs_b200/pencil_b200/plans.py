@@ -324,6 +324,38 @@ class _Plan:
         names = ("generic", "check", "pow2", "mixed_radix")
         return [names[ks[i]] for i in range(cnt.value)]
 
+    # in-place single-allocation arrays (C2cInPlaceArray / R2cInPlaceArray)
+    def in_place_sizes(self):
+        b, w = C.c_int64(), C.c_int64()
+        L.check(L.load().pb_inplace_sizes(self._h, C.byref(b), C.byref(w)), "in-place sizes")
+        return b.value, w.value
+
+    def allocate_in_place(self, device="cuda") -> "InPlaceArray":
+        """``allocate_in_place``: one buffer for the input and output layouts,
+        zero-filled, in state Input."""
+        nbytes, _ = self.in_place_sizes()
+        return InPlaceArray(self, torch.zeros(max(nbytes, 16), dtype=torch.uint8, device=device))
+
+    def allocate_in_place_workspace(self, device="cuda") -> torch.Tensor:
+        _, w = self.in_place_sizes()
+        return torch.empty(max(w, 16), dtype=torch.uint8, device=device)
+
+    def _in_place(self, op, array, workspace, stream):
+        if array.plan is not self:
+            raise L.PencilError(10, "in-place array of another plan (ArrayError::IncompatiblePencils)")
+        if workspace is None:
+            workspace = self.allocate_in_place_workspace(array.buffer.device)
+        L.check(L.load().pb_inplace_execute(array._h, op, _ptr(workspace), _stream_ptr(stream)), "in-place")
+
+    def forward_in_place(self, array, workspace=None, stream=None):
+        self._in_place(L.FORWARD, array, workspace, stream)
+
+    def inverse_in_place(self, array, workspace=None, stream=None):
+        self._in_place(L.INVERSE, array, workspace, stream)
+
+    def backward_in_place(self, array, workspace=None, stream=None):
+        self._in_place(L.BACKWARD, array, workspace, stream)
+
     _forward_checks = False
     _reverse_checks = False
 
@@ -461,6 +493,51 @@ class MixedR2cPlan(_Plan):
         return cls(h, dtype, extra_shape)
 
 
+class InPlaceArray:
+    """``C2cInPlaceArray`` / ``R2cInPlaceArray``: one device buffer whose
+    active layout is the plan's input (state "Input") or output ("Output");
+    an execution that fails after it started leaves it "Poisoned"."""
+
+    STATES = ("Input", "Output", "Poisoned")
+
+    def __init__(self, plan, buffer: torch.Tensor, state: str = "Input"):
+        self.plan, self.buffer = plan, buffer
+        h = C.c_void_p()
+        L.check(L.load().pb_inplace_create(plan._h, _ptr(buffer), self.STATES.index(state), C.byref(h)),
+                "in-place array")
+        self._h = h
+
+    @property
+    def state(self) -> str:
+        st = C.c_int32()
+        L.check(L.load().pb_inplace_state(self._h, C.byref(st)), "in-place state")
+        return self.STATES[st.value]
+
+    def view(self) -> torch.Tensor:
+        """The active layout as a typed flat tensor over the buffer (the
+        reference's ``view`` / ``view_mut``; an error when poisoned)."""
+        st = self.state
+        if st == "Poisoned":
+            raise L.PencilError(21, "in-place view")
+        p = self.plan
+        user_input = st == "Input"
+        dt = p.input_dtype if user_input else p.output_dtype
+        n = p.info.input_elems if user_input else p.info.output_elems
+        esz = torch.empty((), dtype=dt).element_size()
+        return self.buffer[:n * esz].view(dt)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().pb_inplace_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class _Transpose:
     _create_fn = ""
 
@@ -479,6 +556,19 @@ class _Transpose:
 
     def execute_views(self, src, dst, stream=None):
         L.check(L.load().pb_transpose_execute(self._h, _ptr(src), _ptr(dst), _stream_ptr(stream)), "transpose")
+
+    def in_place_sizes(self):
+        b, w = C.c_int64(), C.c_int64()
+        L.check(L.load().pb_transpose_in_place_sizes(self._h, C.byref(b), C.byref(w)), "in-place sizes")
+        return b.value, w.value
+
+    def execute_in_place(self, buffer, workspace=None, stream=None):
+        """``execute_in_place``: `buffer` holds the source layout before and
+        the destination layout after the call."""
+        if workspace is None:
+            workspace = torch.empty(max(self.in_place_sizes()[1], 16), dtype=torch.uint8, device=buffer.device)
+        L.check(L.load().pb_transpose_execute_in_place(self._h, _ptr(buffer), _ptr(workspace), _stream_ptr(stream)),
+                "transpose in place")
 
     execute = execute_views
 
