@@ -677,6 +677,96 @@ def b200_arm(args):
     return 0 if ok else 3
 
 
+def split_arm(args):
+    """Strong scaling: ONE 512^3 R2C field whose 4x8 virtual ranks are split
+    over the N GPUs by whole grid rows (pencil_b200.split.SplitPlan).  The
+    transition over the last grid axis stays fused inside each GPU; the one
+    over the first grid axis crosses GPUs as segment-layout blocks moved by
+    NCCL grouped send/recv, and the C2R spectrum check combines its plane
+    statistics with all-reduces.  value = the field's algorithmic bytes per
+    forward + inverse / max-over-ranks device time."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import pencil_b200 as pb
+    from pencil_b200 import split as sp
+    from pencil_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    shape = tuple(args.shape)
+    plan = pb.R2cPlan.from_shape(pb.MpiTopology(GRID), shape, (), dtype=torch.float32)
+    split = sp.SplitPlan(plan)
+    lo, hi = split.ranges[split.me]
+    xa = torch.from_numpy(np.random.default_rng(1).uniform(-1.0, 1.0, shape).astype(np.float32)).to(dev)
+    full = plan.input_pencil.scatter(xa).contiguous()
+    a = plan.input_pencil.local(lo)["offset"]
+    b = plan.info.input_elems if hi >= plan.info.nranks else plan.input_pencil.local(hi)["offset"]
+    x = full[a:b].contiguous()
+    del full, xa
+    y, back, ws = split.allocate_output(dev), split.allocate_input(dev), split.allocate_workspace(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        split.forward(x, y, ws, stream)
+        split.inverse(y, back, ws, stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    rt = float(torch.linalg.vector_norm((back - x).double()) / torch.linalg.vector_norm(x.double()))
+    if world > 1:
+        t = torch.tensor([ms, rt], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, rt = float(t[0]), float(t[1])
+    bytes_step, _ = algorithmic_bytes(shape)
+    lg = math.log2(shape[0] * shape[1] * shape[2])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": bytes_step / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: field A uniform(-1,1) numpy default_rng(1)",
+            "config": {"workload": "R2C f32 [512,512,512] -> [512,512,257], 4x8 virtual pencil grid split over the "
+                                   "GPUs by grid rows, forward + normalised inverse",
+                       "grid": list(GRID), "shape": list(shape), "ranges": split.ranges,
+                       "l2": "no flush: every pass streams >= 512 MiB / N, larger than the 126 MB L2 for N <= 4",
+                       "parallelism": f"split x{world} (one field, NCCL exchanges across GPUs)"},
+            "phases": {"forward": split.phases(L.FORWARD), "inverse": split.phases(L.INVERSE)},
+            "accuracy": {"roundtrip_rel_l2": rt, "bound": 1e-6 * lg},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        }
+        print(json.dumps(line), flush=True)
+    split.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0 if rt <= 1e-6 * lg else 3
+
+
 LAYOUT_CASES = (((512, 512, 512), "c2c"), ((384, 384, 384), "c2c"), ((512, 512, 512), "r2c"),
                 ((384, 384, 384), "r2c"))
 
@@ -738,6 +828,8 @@ def main():
                     help="skip the cuFFT and unfused-route comparisons and the other configurations")
     ap.add_argument("--batch-grids", type=int, default=64,
                     help="grids of the ragged batch (the first K of the 64-grid workload; profiling runs)")
+    ap.add_argument("--split", action="store_true",
+                    help="strong scaling: one field's virtual ranks split over the GPUs (NCCL exchanges)")
     ap.add_argument("--layouts", action="store_true",
                     help="instead of the headline: permuted against strided layouts, per-launch times (1 GPU)")
     args = ap.parse_args()
@@ -745,6 +837,8 @@ def main():
         args.warmup = 3
     if args.layouts:
         return layouts_arm(args)
+    if args.split and args.impl != "reference":
+        return split_arm(args)
     if args.impl == "reference":
         return reference_arm(args)
     return b200_arm(args)

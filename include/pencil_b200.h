@@ -256,6 +256,71 @@ int pb_inplace_state(const pb_inplace* array, int32_t* state);
 int pb_inplace_execute(pb_inplace* array, int32_t op, void* workspace, void* stream);
 int pb_inplace_destroy(pb_inplace* array);
 
+/* ---- slices: one process's virtual ranks of a plan split over GPUs ----- */
+/* The reference runs one MPI rank per process; each distributed transition is
+ * one MPI_Alltoallv per sub-communicator of the changed grid axis
+ * (crates/pencil-array/src/alltoallv_transpose.rs:324-367, transpose.rs
+ * 1126-1281).  A slice is a plan restricted to the contiguous virtual ranks
+ * [rank_lo, rank_hi) that one process (one GPU) holds; its buffers are the
+ * concatenation of those ranks' local arrays.  Transitions whose data stay in
+ * the slice remain fused into the passes.  The others, and the C2R spectrum
+ * check's statistics, end a phase at a "boundary" that the host completes:
+ *   EXCHANGE: the workspace's send block (at send_offset, in the reference's
+ *     segment layout) holds one segment per (local rank, peer) transfer; the
+ *     host moves each segment to the receive block (recv_offset) of the
+ *     process that owns the peer (NCCL grouped send/recv; device copies when
+ *     the peer is local), using pb_slice_transfers for counts and offsets;
+ *   REDUCE_*: the host combines the acc_groups x [max, max, sum, sum] doubles
+ *     at acc_offset across processes (maxima by max, sums by sum, both for
+ *     MAX_SUM) and the int32 word at status_offset + 4 by max.
+ * Phase k (0 <= k < phases) runs with pb_slice_execute_phase; boundary k
+ * follows phase k.  in/out are the slice's FORWARD input/output arrays. */
+#define PB_BOUNDARY_EXCHANGE 1
+#define PB_BOUNDARY_REDUCE_MAX_SUM 2
+#define PB_BOUNDARY_REDUCE_MAX 3
+#define PB_BOUNDARY_REDUCE_SUM 4
+typedef struct pb_slice pb_slice;
+typedef struct pb_slice_info {
+  int32_t rank_lo, rank_hi;
+  int64_t input_elems;     /* the slice's FORWARD input (its ranks, extra included) */
+  int64_t output_elems;
+  int64_t workspace_bytes; /* 256-byte aligned workspace of one concurrent execution */
+} pb_slice_info;
+typedef struct pb_slice_boundary_info {
+  int32_t kind;            /* PB_BOUNDARY_* */
+  int32_t elem_bytes;      /* EXCHANGE: element size of the segments */
+  int32_t ntransfers;
+  int32_t acc_groups;
+  int64_t send_offset, recv_offset;  /* byte offsets in the workspace */
+  int64_t send_elems, recv_elems;
+  int64_t acc_offset, status_offset;
+} pb_slice_boundary_info;
+typedef struct pb_slice_transfer {
+  int32_t receive;         /* 0: a segment of the send block, 1: of the receive block */
+  int32_t rank;            /* the local virtual rank */
+  int32_t peer;            /* the virtual rank it goes to (send) or comes from (receive) */
+  int32_t reserved;
+  int64_t offset;          /* elements from the start of the block */
+  int64_t count;           /* elements */
+} pb_slice_transfer;
+int pb_slice_create(const pb_plan* plan, int32_t rank_lo, int32_t rank_hi, pb_slice** slice);
+int pb_slice_get_info(const pb_slice* slice, pb_slice_info* info);
+int pb_slice_phases(const pb_slice* slice, int32_t op, int32_t* count);
+int pb_slice_boundary(const pb_slice* slice, int32_t op, int32_t boundary, pb_slice_boundary_info* out);
+int pb_slice_transfers(const pb_slice* slice, int32_t op, int32_t boundary, pb_slice_transfer* transfers,
+                       int32_t capacity, int32_t* count);
+int pb_slice_execute_phase(pb_slice* slice, int32_t op, int32_t phase, const void* in, void* out, void* workspace,
+                           void* stream);
+int pb_slice_destroy(pb_slice* slice);
+/* The transfer table of one AllToAllv exchange from `src` to `dst` (one
+ * decomposition slot changes) for the virtual ranks [rank_lo, rank_hi), with
+ * the send and receive block sizes: the same table pb_slice_transfers gives
+ * for such a boundary.  Host geometry only (no device work), for hosts that
+ * route exchanges themselves. */
+int pb_exchange_transfers(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count, int32_t rank_lo,
+                          int32_t rank_hi, pb_slice_transfer* transfers, int32_t capacity, int32_t* count,
+                          int64_t* send_elems, int64_t* recv_elems);
+
 /* ---- spectral multipliers ---------------------------------------------- */
 /* out = m(k) * scale * in on the plan's FORWARD output layout (complex), k the
  * integer wavevector of each element (FFT order; the R2C-reduced axis holds

@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256) stats_kernel(const StatsArgs A) {
     if (bad) atomicOr(A.status + 1, 1);
     __threadfence();
     const unsigned total = gridDim.x * gridDim.y;
-    s_last = (MODE != 1) && (atomicAdd(A.counter, 1u) == total - 1);
+    s_last = (MODE != 1) && A.part == 0 && (atomicAdd(A.counter, 1u) == total - 1);
   }
   __syncthreads();
   if (s_last) {
@@ -321,6 +321,8 @@ __global__ void __launch_bounds__(256) stats_kernel(const StatsArgs A) {
     stats_decide(A);
   }
 }
+
+__global__ void stats_decide_kernel(const StatsArgs A) { stats_decide(A); }
 
 static unsigned grid_for(long long total, int threads, long long cap) {
   long long b = (total + threads - 1) / threads;
@@ -330,6 +332,11 @@ static unsigned grid_for(long long total, int threads, long long cap) {
 }
 
 cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.part == 3) {
+    if (A.extra * A.nplanes <= 0) return cudaSuccess;
+    stats_decide_kernel<<<1, 256, 0, stream>>>(A);
+    return cudaGetLastError();
+  }
   const long long groups = A.extra * A.nplanes * A.pen.nranks;
   if (groups <= 0 || A.max_points <= 0) return cudaSuccess;
   if (groups > 65535 || A.max_points >= (1LL << 32)) return cudaErrorInvalidValue;
@@ -341,8 +348,8 @@ cudaError_t launch_stats(const StatsArgs& A, int real_bytes, cudaStream_t stream
   if (real_bytes == 4) {
     stats_kernel<float, 0><<<grid, threads, 0, stream>>>(A);
   } else {
-    stats_kernel<double, 1><<<grid, threads, 0, stream>>>(A);
-    stats_kernel<double, 2><<<grid, threads, 0, stream>>>(A);
+    if (A.part != 2) stats_kernel<double, 1><<<grid, threads, 0, stream>>>(A);
+    if (A.part != 1) stats_kernel<double, 2><<<grid, threads, 0, stream>>>(A);
   }
   return cudaGetLastError();
 }

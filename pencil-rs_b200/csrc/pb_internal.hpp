@@ -147,6 +147,11 @@ struct StatsArgs {
   unsigned int* counter;  // blocks finished (last-block decision)
   double relative;
   double absolute;
+  // 0: the whole check (statistics, then the last block decides); for a
+  // slice of the ranks, whose statistics are combined across processes
+  // between launches: 1 accumulate (f32 single pass / f64 maxima), 2 the f64
+  // scaled sums, 3 decide only
+  int part;
 };
 
 }  // namespace pb

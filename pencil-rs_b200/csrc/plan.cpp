@@ -267,11 +267,13 @@ struct Stage {
 enum Mode { M_F = 0, M_FS, M_B, M_I, M_AF, M_AFS, M_AB, M_AI, M_COUNT };
 
 struct Step {
-  int type = 0;  // 0 pass, 1 endpoint statistics
+  int type = 0;  // 0 pass, 1 endpoint statistics; in a slice also 2 exchange, 3 statistics reduction
   PassArgs pa{};
   StatsArgs sa{};
   int src_slot = 0;  // -1 caller input, -2 caller output, 0/1 workspace buffers
   int dst_slot = 0;
+  int xchg = -1;     // exchange index (type 2)
+  int reduce = 0;    // type 3: 0 maxima and sums, 1 maxima, 2 sums
 };
 
 struct Program {
@@ -314,6 +316,8 @@ struct pb_plan {
   bool force_generic = false;                // batch building: no standalone register kernels
   bool batch_mr = false;                     // batch building: mixed-radix tiles where the batch kernel has them
   std::map<std::string, int> tuned_lines;    // batch building: autotuned lines per tile by pass shape
+  bool sliced = false;                       // slice building: only virtual ranks [slice_lo, slice_hi)
+  int slice_lo = 0, slice_hi = 0;
   pb::DevPencil spectral_pen{};              // FORWARD output layout (spectral multipliers)
   ~pb_plan() {
     if (arena) cudaFree(arena);
@@ -347,21 +351,25 @@ static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size
     rs *= p.grid[t];
   }
   d.nranks = p.nranks();
-  const std::string key = pencil_key(p, extra);
+  // a slice's table holds its ranks only, addressed from the slice's base
+  const int r_lo = P.sliced ? P.slice_lo : 0;
+  const int r_hi = P.sliced ? P.slice_hi : d.nranks;
+  const std::string key = pencil_key(p, extra) + (P.sliced ? "s" + std::to_string(r_lo) + "-" + std::to_string(r_hi) : "");
   auto it = cache.find(key);
   size_t off;
+  d.nranks = r_hi - r_lo;
   if (it != cache.end()) {
     off = it->second;
   } else {
     const int w = info_words(p.N);
     std::vector<long long> info((size_t)d.nranks * w);
     long long base = 0;
-    for (int r = 0; r < d.nranks; ++r) {
+    for (int r = r_lo; r < r_hi; ++r) {
       long long lo[MAXN], ext[MAXN];
       p.local(r, lo, ext);
       long long len = 1;
       for (int x = 0; x < p.N; ++x) len *= (x == p.perm[p.N - 1]) ? p.inner_span(ext) : ext[x];
-      long long* row = &info[(size_t)r * w];
+      long long* row = &info[(size_t)(r - r_lo) * w];
       row[0] = base;
       row[1] = len;
       long long stride = 1;
@@ -380,7 +388,6 @@ static DevPencil dev_pencil(pb_plan& P, HostArena& A, std::map<std::string, size
     off = A.add(info.data(), info.size() * sizeof(long long));
     cache[key] = off;
   }
-  (void)P;
   d.info = reinterpret_cast<const long long*>(enc(off));
   return d;
 }
@@ -905,6 +912,11 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
   const long long nout = dst.shape[A.a];
   std::vector<TileAddr> tiles((size_t)A.ntiles);
   std::vector<PieceAddr> pieces(direct ? 0 : (size_t)A.ntiles * npieces);
+  // a slice keeps the tiles whose lines lie in its ranks, with addresses from
+  // the bases of its ranks in the source and destination concatenations (the
+  // slice's transitions are closed, so its destination ranks are its own)
+  const long long sbase = P.sliced ? hs.base[P.slice_lo] : 0;
+  const long long dbase = P.sliced ? hd.base[P.slice_lo] : 0;
   long long outer_total = 1;
   for (int i = 0; i < A.nouter_axes; ++i) outer_total *= A.outer_ext[i];
   long long t = 0;
@@ -921,7 +933,8 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
         g[A.a] = 0;
         TileAddr& ta_ = tiles[(size_t)t];
         int r;
-        ta_.src0 = hs.offset(e, g, &r);
+        ta_.src0 = hs.offset(e, g, &r) - sbase;
+        if (P.sliced && (r < P.slice_lo || r >= P.slice_hi)) continue;
         ta_.srcb = (int)hs.stride[r][A.b];
         ta_.lines = c.y;
         ta_.srcq = 0;
@@ -930,7 +943,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
           ta_.srcq = (int)hs.stride[r][A.a];
         }
         if (direct) {
-          ta_.dst0 = hd.offset(e, g, &r);
+          ta_.dst0 = hd.offset(e, g, &r) - dbase;
           ta_.dstb = (int)hd.stride[r][A.b];
         } else {
           ta_.dst0 = 0;
@@ -944,7 +957,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
               continue;
             }
             g[A.a] = st;
-            pa.rowbase = hd.offset(e, g, &r);
+            pa.rowbase = hd.offset(e, g, &r) - dbase;
             // transposed store: stride of k; split direct store: stride between lines
             pa.stride = A.dst_k_contig == 2 ? hd.stride[r][A.b] : hd.stride[r][A.a];
           }
@@ -958,6 +971,11 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
     }
   }
   (void)N;
+  if (P.sliced) {
+    tiles.resize((size_t)t);
+    if (!direct) pieces.resize((size_t)t * npieces);
+    A.ntiles = t;
+  }
   A.tile_tab = enc(P.host.add(tiles.data(), tiles.size() * sizeof(TileAddr)));
   if (!direct) {
     A.piece_tab = enc(P.host.add(pieces.data(), pieces.size() * sizeof(PieceAddr)));
@@ -3399,6 +3417,539 @@ int pb_batch_set_wait_limit(pb_batch* batch, int64_t spins) {
 int pb_batch_destroy(pb_batch* batch) {
   delete batch;
   return PB_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Slices: one process's virtual ranks of a plan split over several GPUs.
+//
+// The reference runs one MPI rank per process and exchanges each distributed
+// transition with one MPI_Alltoallv per sub-communicator
+// (crates/pencil-array/src/alltoallv_transpose.rs:324-367).  Here a process
+// (one GPU) holds a contiguous range [rank_lo, rank_hi) of the virtual ranks;
+// its buffers are the concatenation of those ranks' local arrays.  A slice is
+// the plan restricted to them:
+// * a transition whose data stay inside the slice (every sub-communicator of
+//   the changed grid axis lies in the range, e.g. the rows of a P1 x P2 grid
+//   held by one GPU) stays fused into the pass's stores, as in one-GPU plans;
+// * a transition that crosses slices becomes: the pass stores into its own
+//   stage layout, pack into the reference's segment layout
+//   (transpose.rs:1126-1176), an exchange the host runs (NCCL grouped
+//   send/recv with the segments' counts and displacements; same-slice
+//   segments are device copies), and unpack (transpose.rs:1233-1281);
+// * the C2R spectrum check accumulates the slice's plane statistics, the host
+//   combines them across slices (maxima and sums), and a decide kernel sets
+//   the status word that gates the later passes.
+// Execution is split into phases at those host steps ("boundaries").
+// ===========================================================================
+namespace pb {
+
+struct SliceXchg {
+  Pencil src, dst;
+  int elem_bytes = 0;
+  long long send_elems = 0, recv_elems = 0;
+  std::vector<pb_slice_transfer> transfers;
+  std::vector<XTile> pack_tiles, unpack_tiles;
+  int pack_row = 0, unpack_row = 0;
+  size_t pack_tab = 0, unpack_tab = 0;
+  XposeArgs pack{}, unpack{};
+};
+
+}  // namespace pb
+
+struct pb_slice {
+  const pb_plan* parent = nullptr;
+  std::unique_ptr<pb_plan> T;  // the slice's programs; owns its device tables
+  std::vector<pb::SliceXchg> xchg;
+  std::vector<int> bounds[pb::M_COUNT];  // step index of every boundary
+  size_t slot_bytes = 0, send_off = 0, recv_off = 0, ws_bytes = 0;
+  int acc_groups = 0;
+};
+
+namespace pb {
+
+static long long slice_elems(const Pencil& p, long long extra, int lo, int hi) {
+  long long n = 0;
+  for (int r = lo; r < hi; ++r) n += p.local_len(r) * extra;
+  return n;
+}
+
+// no element moves between a rank inside [lo, hi) and one outside
+static bool slice_closed(const Pencil& A, const Pencil& B, int lo, int hi) {
+  const int R = A.nranks(), N = A.N;
+  std::vector<std::array<long long, 2 * MAXN>> ba(R), bb(R);
+  for (int r = 0; r < R; ++r) {
+    A.local(r, ba[r].data(), ba[r].data() + MAXN);
+    B.local(r, bb[r].data(), bb[r].data() + MAXN);
+  }
+  auto meets = [&](const std::array<long long, 2 * MAXN>& x, const std::array<long long, 2 * MAXN>& y) {
+    for (int a = 0; a < N; ++a) {
+      const long long s0 = std::max(x[a], y[a]), e0 = std::min(x[a] + x[MAXN + a], y[a] + y[MAXN + a]);
+      if (e0 <= s0) return false;
+    }
+    return true;
+  };
+  for (int r = lo; r < hi; ++r)
+    for (int q = 0; q < R; ++q) {
+      if (q >= lo && q < hi) continue;
+      if (meets(ba[r], bb[q]) || meets(ba[q], bb[r])) return false;
+    }
+  return true;
+}
+
+// the exchange from `A` to `B` (one decomposition slot changes) for the
+// slice's ranks: segment-layout send and receive blocks of its ranks,
+// transfers, and the pack / unpack tiles between the slice's concatenated
+// layouts and those blocks
+static SliceXchg slice_exchange(const pb_plan& P, const Pencil& A, const Pencil& B, int elem_bytes,
+                                bool with_tiles = true) {
+  SliceXchg X;
+  X.src = A;
+  X.dst = B;
+  X.elem_bytes = elem_bytes;
+  if (A.N != B.N || A.M != B.M) fail(PB_EUNSUPPORTED);
+  int changed = -1, count = 0;
+  for (int t = 0; t < A.M; ++t)
+    if (A.dec[t] != B.dec[t] || A.grid[t] != B.grid[t]) {
+      changed = t;
+      ++count;
+    }
+  if (count != 1) fail(PB_EUNSUPPORTED_DECOMPOSITION_CHANGE);
+  const int N = A.N, lo = P.slice_lo, hi = P.slice_hi;
+  const long long extra = P.extra;
+  HostLayout ha(A, extra), hb(B, extra);
+  auto ranges = [&](const Pencil& p, const int* c, long long* l, long long* e) {
+    for (int x = 0; x < N; ++x) {
+      l[x] = 0;
+      e[x] = p.shape[x];
+    }
+    for (int t = 0; t < p.M; ++t) {
+      const int ax = p.dec[t];
+      l[ax] = Pencil::part(p.shape[ax], p.grid[t], c[t]);
+      e[ax] = Pencil::part(p.shape[ax], p.grid[t], c[t] + 1) - l[ax];
+    }
+  };
+  auto region = [&](const int* ca, const int* cb, long long* rlo, long long* rext) {
+    long long al[MAXN], ae[MAXN], bl[MAXN], be[MAXN];
+    ranges(A, ca, al, ae);
+    ranges(B, cb, bl, be);
+    long long len = 1;
+    for (int x = 0; x < N; ++x) {
+      const long long s0 = std::max(al[x], bl[x]), e0 = std::min(al[x] + ae[x], bl[x] + be[x]);
+      rlo[x] = s0;
+      rext[x] = e0 > s0 ? e0 - s0 : 0;
+      len *= rext[x];
+    }
+    return len;
+  };
+  const int P_t = A.grid[changed];
+  long long sbase = 0, rbase = 0;
+  for (int r = lo; r < hi; ++r) {
+    int me[MAXM];
+    A.coords(r, me);
+    long long sd = 0, rd = 0;
+    AffineMap ma = rank_map(ha, r), mb = rank_map(hb, r);
+    ma.base -= ha.base[lo];
+    mb.base -= hb.base[lo];
+    for (int p = 0; p < P_t; ++p) {
+      int pc[MAXM];
+      std::memcpy(pc, me, sizeof(pc));
+      pc[changed] = p;
+      int q = 0;
+      for (int t = 0; t < A.M; ++t) q = q * A.grid[t] + pc[t];
+      long long slo[MAXN], sext[MAXN], rlo[MAXN], rext[MAXN];
+      const long long slen = region(me, pc, slo, sext);
+      const long long rlen = region(pc, me, rlo, rext);
+      if (slen * extra > INT_MAX || rlen * extra > INT_MAX) fail(PB_ECOUNT_OVERFLOW);
+      if (slen > 0 && extra > 0) {
+        const long long off = sbase + sd * extra;
+        X.transfers.push_back(pb_slice_transfer{0, r, q, 0, off, slen * extra});
+        if (with_tiles)
+          box_xtiles(N, slo, sext, extra, ma, segment_map(N, off, slen, slo, sext), A.perm[N - 1], N - 1,
+                     X.pack_tiles);
+      }
+      if (rlen > 0 && extra > 0) {
+        const long long off = rbase + rd * extra;
+        X.transfers.push_back(pb_slice_transfer{1, r, q, 0, off, rlen * extra});
+        if (with_tiles)
+          box_xtiles(N, rlo, rext, extra, segment_map(N, off, rlen, rlo, rext), mb, N - 1, B.perm[N - 1],
+                     X.unpack_tiles);
+      }
+      sd += slen;
+      rd += rlen;
+    }
+    sbase += sd * extra;
+    rbase += rd * extra;
+  }
+  X.send_elems = sbase;
+  X.recv_elems = rbase;
+  X.pack_row = A.perm[N - 1] == N - 1;
+  X.unpack_row = B.perm[N - 1] == N - 1;
+  if (elem_bytes != 4 && elem_bytes != 8 && elem_bytes != 16) fail(PB_EUNSUPPORTED);
+  return X;
+}
+
+static void build_slice_program(pb_slice& S, int mode) {
+  pb_plan& P = *S.T;
+  Program& prog = P.prog[mode];
+  prog.steps.clear();
+  prog.has_stats = false;
+  const int N = (int)P.stages.size();
+  const int lo = P.slice_lo, hi = P.slice_hi;
+  const bool fwd = (mode == M_F || mode == M_FS || mode == M_AB || mode == M_AI);
+  std::vector<int> active;
+  for (int i = 0; i < N; ++i) {
+    const int j = fwd ? i : N - 1 - i;
+    if (P.stages[j].kind != SK_ID) active.push_back(j);
+  }
+  const Pencil& start = fwd ? P.fin : P.fout;
+  const Pencil& end = fwd ? P.fout : P.fin;
+  bool cur_complex = fwd ? P.fin_complex : P.fout_complex;
+  const bool end_complex = fwd ? P.fout_complex : P.fin_complex;
+  if (active.empty()) fail(PB_EUNSUPPORTED);
+  Pencil cur = start;
+  int cur_slot = -1;
+  auto other = [](int slot) { return slot == 0 ? 1 : 0; };
+  auto note_slot = [&](const Pencil& p, bool cplx) {
+    const size_t b = (size_t)slice_elems(p, P.extra, lo, hi) * (size_t)P.real_bytes * (cplx ? 2 : 1);
+    S.slot_bytes = std::max(S.slot_bytes, b);
+  };
+  const int npass = (int)active.size();
+  for (int k = 0; k < npass; ++k) {
+    const Stage& st = P.stages[active[k]];
+    const bool last = k + 1 == npass;
+    Pencil target;
+    bool target_complex;
+    if (last) {
+      target = end;
+      target_complex = end_complex;
+    } else {
+      const Stage& nx = P.stages[active[k + 1]];
+      target = fwd ? nx.in : nx.out;
+      target_complex = fwd ? !nx.real_in : !nx.real_out;
+    }
+    Pencil own = fwd ? st.out : st.in;
+    const bool own_complex = fwd ? !st.real_out : !st.real_in;
+    const long long n_axis = (st.kind == SK_R2C) ? P.real_len : st.in.shape[st.axis];
+    LocalOp op = local_op(st, mode, n_axis);
+    if (op.gated) {
+      // the check's statistics: accumulate, combine across slices, decide
+      Step a = make_stats(P, cur, st.axis, mode == M_I);
+      a.src_slot = cur_slot;
+      a.sa.part = 1;
+      prog.steps.push_back(a);
+      S.acc_groups = std::max(S.acc_groups, (int)(a.sa.extra * a.sa.nplanes));
+      Step r;
+      r.type = 3;
+      r.reduce = P.real_bytes == 4 ? 0 : 1;
+      prog.steps.push_back(r);
+      if (P.real_bytes == 8) {
+        Step b = a;
+        b.sa.part = 2;
+        prog.steps.push_back(b);
+        Step r2;
+        r2.type = 3;
+        r2.reduce = 2;
+        prog.steps.push_back(r2);
+      }
+      Step d = a;
+      d.sa.part = 3;
+      prog.steps.push_back(d);
+      prog.has_stats = true;
+    }
+    const bool fused = slice_closed(cur, target, lo, hi);
+    if (!fused && !slice_closed(cur, own, lo, hi)) fail(PB_EUNSUPPORTED);
+    Pencil dst = fused ? target : own;
+    const bool dst_complex = fused ? target_complex : own_complex;
+    const bool to_user = fused && last;
+    if (!to_user) {
+      row_pitch(dst, dst_complex ? 2 * P.real_bytes : P.real_bytes);
+      note_slot(dst, dst_complex);
+    }
+    Step ps = make_pass(P, st, op, cur, dst, cur_complex, dst_complex);
+    if (ps.pa.tile_tab == nullptr) fail(PB_EUNSUPPORTED);  // slices need the host tile tables
+    if (op.gated) ps.pa.gate = reinterpret_cast<const int*>(1);
+    ps.src_slot = cur_slot;
+    ps.dst_slot = to_user ? -2 : other(cur_slot);
+    prog.steps.push_back(ps);
+    cur = dst;
+    cur_complex = dst_complex;
+    cur_slot = ps.dst_slot;
+    if (!fused) {
+      if (!last) row_pitch(target, target_complex ? 2 * P.real_bytes : P.real_bytes);
+      Step x;
+      x.type = 2;
+      x.xchg = (int)S.xchg.size();
+      x.src_slot = cur_slot;
+      x.dst_slot = last ? -2 : other(cur_slot);
+      S.xchg.push_back(slice_exchange(P, cur, target, (target_complex ? 2 : 1) * P.real_bytes));
+      if (!last) note_slot(target, target_complex);
+      prog.steps.push_back(x);
+      cur = target;
+      cur_complex = target_complex;
+      cur_slot = x.dst_slot;
+    }
+  }
+  bool gated = false;
+  for (int i = 0; i < (int)prog.steps.size(); ++i) {
+    Step& st = prog.steps[i];
+    if (st.type == 1 && st.sa.part == 3) gated = true;
+    if (st.type == 0 && gated) st.pa.gate = reinterpret_cast<const int*>(1);
+    if (st.type == 2 || st.type == 3) S.bounds[mode].push_back(i);
+  }
+}
+
+static pb_slice* slice_create(const pb_plan* plan, int lo, int hi) {
+  if (!plan) fail(PB_ENULL);
+  const int R = plan->fin.nranks();
+  if (lo < 0 || hi > R || lo >= hi) fail(PB_EINVALID_ARGUMENT);
+  std::unique_ptr<pb_slice> S(new pb_slice());
+  S->parent = plan;
+  S->T.reset(new pb_plan());
+  pb_plan& T = *S->T;
+  T.real_bytes = plan->real_bytes;
+  adopt_route(T, *plan);
+  T.sliced = true;
+  T.slice_lo = lo;
+  T.slice_hi = hi;
+  int dev = 0;
+  cuda_ok(cudaGetDevice(&dev));
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+    T.max_smem = optin;
+  for (int m = 0; m < M_COUNT; ++m) build_slice_program(*S, m);
+  for (auto& X : S->xchg) {
+    X.pack_tab = T.host.add(X.pack_tiles.data(), X.pack_tiles.size() * sizeof(XTile));
+    X.unpack_tab = T.host.add(X.unpack_tiles.data(), X.unpack_tiles.size() * sizeof(XTile));
+  }
+  if (!T.host.bytes.empty()) {
+    cuda_ok(cudaMalloc(&T.arena, T.host.bytes.size()));
+    cuda_ok(cudaMemcpy(T.arena, T.host.bytes.data(), T.host.bytes.size(), cudaMemcpyHostToDevice));
+  }
+  auto fix = [&](const void*& p) { p = fix_ptr(T, p); };
+  auto fixpen = [&](DevPencil& d) { d.info = reinterpret_cast<const long long*>(fix_ptr(T, d.info)); };
+  for (int m = 0; m < M_COUNT; ++m)
+    for (auto& st : T.prog[m].steps) {
+      if (st.type == 0) {
+        const void* c = st.pa.chunks;
+        fix(c);
+        st.pa.chunks = reinterpret_cast<const int2*>(c);
+        fix(st.pa.twiddle);
+        fix(st.pa.aux0);
+        fix(st.pa.aux1);
+        fix(st.pa.tile_tab);
+        fix(st.pa.piece_tab);
+        st.pa.ktab = reinterpret_cast<const int2*>(fix_ptr(T, st.pa.ktab));
+        fixpen(st.pa.src);
+        fixpen(st.pa.dst);
+      } else if (st.type == 1) {
+        fixpen(st.sa.pen);
+      }
+    }
+  size_t xbuf = 0;
+  for (auto& X : S->xchg) {
+    auto setup = [&](XposeArgs& A, size_t tab, const std::vector<XTile>& v, int row) {
+      A.tiles = reinterpret_cast<const XTile*>(fix_ptr(T, enc(tab)));
+      A.ntiles = (long long)v.size();
+      A.elem_bytes = X.elem_bytes;
+      A.row = row;
+    };
+    setup(X.pack, X.pack_tab, X.pack_tiles, X.pack_row);
+    setup(X.unpack, X.unpack_tab, X.unpack_tiles, X.unpack_row);
+    xbuf = std::max(xbuf, (size_t)std::max(X.send_elems, X.recv_elems) * (size_t)X.elem_bytes);
+  }
+  // workspace: two slots, the send and receive blocks, status words, statistics
+  const size_t slot = (S->slot_bytes + 255) & ~size_t(255);
+  S->slot_bytes = slot;
+  xbuf = (xbuf + 255) & ~size_t(255);
+  S->send_off = 2 * slot;
+  S->recv_off = S->send_off + xbuf;
+  T.status_off = S->recv_off + xbuf;
+  T.acc_off = T.status_off + 256;
+  const size_t acc = (size_t)std::max(S->acc_groups, 1) * 4 * sizeof(double);
+  S->ws_bytes = T.acc_off + ((acc + 255) & ~size_t(255));
+  T.ws_bytes = S->ws_bytes;
+  T.buf_bytes = slot;
+  return S.release();
+}
+
+static void* slice_slot(const pb_slice& S, int slot, const void* in, void* out, void* ws) {
+  if (slot == -1) return const_cast<void*>(in);
+  if (slot == -2) return out;
+  return static_cast<unsigned char*>(ws) + (size_t)slot * S.slot_bytes;
+}
+
+static int slice_phase(pb_slice& S, int op, int phase, const void* in, void* out, void* ws, cudaStream_t s) {
+  pb_plan& P = *S.T;
+  const int mode = user_mode(P, op);
+  Program& prog = P.prog[mode];
+  const std::vector<int>& b = S.bounds[mode];
+  const int nph = (int)b.size() + 1;
+  if (phase < 0 || phase >= nph) fail(PB_EINVALID_ARGUMENT);
+  if (!ws) fail(PB_ENULL);
+  if (reinterpret_cast<uintptr_t>(ws) % 256 != 0) fail(PB_EINVALID_ARGUMENT);
+  unsigned char* w = static_cast<unsigned char*>(ws);
+  int* status = reinterpret_cast<int*>(w + P.status_off);
+  if (phase == 0 && prog.has_stats) cuda_ok(cudaMemsetAsync(status, 0, S.ws_bytes - P.status_off, s));
+  const int first = phase == 0 ? 0 : b[phase - 1] + 1;
+  const int last = phase + 1 < nph ? b[phase] : (int)prog.steps.size();
+  if (phase > 0 && prog.steps[b[phase - 1]].type == 2) {  // the unpack of the exchange before this phase
+    const Step& xs = prog.steps[b[phase - 1]];
+    XposeArgs X = S.xchg[xs.xchg].unpack;
+    X.in = w + S.recv_off;
+    X.out = slice_slot(S, xs.dst_slot, in, out, ws);
+    check_aligned(X.out, false, X.elem_bytes);
+    cuda_ok(launch_xpose(X, s));
+  }
+  for (int i = first; i < last; ++i) {
+    Step& st = prog.steps[i];
+    if (st.type == 0) {
+      PassArgs A = st.pa;
+      A.in = slice_slot(S, st.src_slot, in, out, ws);
+      A.out = slice_slot(S, st.dst_slot, in, out, ws);
+      check_aligned(A.in, A.in_complex != 0, P.real_bytes);
+      check_aligned(A.out, A.out_complex != 0, P.real_bytes);
+      A.gate = (A.gate != nullptr) ? status : nullptr;
+      cuda_ok(launch_pass(A, P.real_bytes, s));
+    } else if (st.type == 1) {
+      StatsArgs St = st.sa;
+      St.data = slice_slot(S, st.src_slot, in, out, ws);
+      St.acc = reinterpret_cast<double*>(w + P.acc_off);
+      St.status = status;
+      St.counter = reinterpret_cast<unsigned int*>(status + 4);
+      cuda_ok(launch_stats(St, P.real_bytes, s));
+    }
+  }
+  if (phase + 1 < nph && prog.steps[b[phase]].type == 2) {  // the pack before the boundary
+    const Step& xs = prog.steps[b[phase]];
+    XposeArgs X = S.xchg[xs.xchg].pack;
+    X.in = slice_slot(S, xs.src_slot, in, out, ws);
+    X.out = w + S.send_off;
+    cuda_ok(launch_xpose(X, s));
+  }
+  return PB_OK;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_slice_create(const pb_plan* plan, int32_t rank_lo, int32_t rank_hi, pb_slice** slice) {
+  return guard([&] {
+    if (!slice) return (int)PB_ENULL;
+    *slice = slice_create(plan, rank_lo, rank_hi);
+    return (int)PB_OK;
+  });
+}
+
+int pb_slice_get_info(const pb_slice* slice, pb_slice_info* info) {
+  return guard([&] {
+    if (!slice || !info) return (int)PB_ENULL;
+    const pb_plan& T = *slice->T;
+    const Pencil& in = T.c2r_family ? T.fout : T.fin;
+    const Pencil& out = T.c2r_family ? T.fin : T.fout;
+    info->rank_lo = T.slice_lo;
+    info->rank_hi = T.slice_hi;
+    info->input_elems = slice_elems(in, T.extra, T.slice_lo, T.slice_hi);
+    info->output_elems = slice_elems(out, T.extra, T.slice_lo, T.slice_hi);
+    info->workspace_bytes = (int64_t)slice->ws_bytes;
+    return (int)PB_OK;
+  });
+}
+
+int pb_slice_phases(const pb_slice* slice, int32_t op, int32_t* count) {
+  return guard([&] {
+    if (!slice || !count) return (int)PB_ENULL;
+    *count = (int)slice->bounds[user_mode(*slice->T, op)].size() + 1;
+    return (int)PB_OK;
+  });
+}
+
+int pb_slice_boundary(const pb_slice* slice, int32_t op, int32_t boundary, pb_slice_boundary_info* out) {
+  return guard([&] {
+    if (!slice || !out) return (int)PB_ENULL;
+    const pb_plan& T = *slice->T;
+    const int mode = user_mode(T, op);
+    const std::vector<int>& b = slice->bounds[mode];
+    if (boundary < 0 || boundary >= (int)b.size()) return (int)PB_EINVALID_ARGUMENT;
+    const Step& st = T.prog[mode].steps[b[boundary]];
+    std::memset(out, 0, sizeof(*out));
+    out->status_offset = (int64_t)T.status_off;
+    out->acc_offset = (int64_t)T.acc_off;
+    out->acc_groups = slice->acc_groups;
+    if (st.type == 2) {
+      const SliceXchg& X = slice->xchg[st.xchg];
+      out->kind = PB_BOUNDARY_EXCHANGE;
+      out->elem_bytes = X.elem_bytes;
+      out->ntransfers = (int32_t)X.transfers.size();
+      out->send_offset = (int64_t)slice->send_off;
+      out->recv_offset = (int64_t)slice->recv_off;
+      out->send_elems = X.send_elems;
+      out->recv_elems = X.recv_elems;
+    } else {
+      out->kind = st.reduce == 0 ? PB_BOUNDARY_REDUCE_MAX_SUM : (st.reduce == 1 ? PB_BOUNDARY_REDUCE_MAX : PB_BOUNDARY_REDUCE_SUM);
+    }
+    return (int)PB_OK;
+  });
+}
+
+int pb_slice_transfers(const pb_slice* slice, int32_t op, int32_t boundary, pb_slice_transfer* transfers,
+                       int32_t capacity, int32_t* count) {
+  return guard([&] {
+    if (!slice || !count) return (int)PB_ENULL;
+    const pb_plan& T = *slice->T;
+    const int mode = user_mode(T, op);
+    const std::vector<int>& b = slice->bounds[mode];
+    if (boundary < 0 || boundary >= (int)b.size()) return (int)PB_EINVALID_ARGUMENT;
+    const Step& st = T.prog[mode].steps[b[boundary]];
+    if (st.type != 2) {
+      *count = 0;
+      return (int)PB_OK;
+    }
+    const auto& v = slice->xchg[st.xchg].transfers;
+    *count = (int32_t)v.size();
+    if (transfers)
+      for (int i = 0; i < (int)v.size() && i < capacity; ++i) transfers[i] = v[i];
+    return (int)PB_OK;
+  });
+}
+
+int pb_slice_execute_phase(pb_slice* slice, int32_t op, int32_t phase, const void* in, void* out, void* workspace,
+                           void* stream) {
+  return guard([&] {
+    if (!slice) return (int)PB_ENULL;
+    return slice_phase(*slice, op, phase, in, out, workspace, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int pb_slice_destroy(pb_slice* slice) {
+  delete slice;
+  return PB_OK;
+}
+
+int pb_exchange_transfers(const pb_pencil_desc* src, const pb_pencil_desc* dst, int64_t extra_count, int32_t rank_lo,
+                          int32_t rank_hi, pb_slice_transfer* transfers, int32_t capacity, int32_t* count,
+                          int64_t* send_elems, int64_t* recv_elems) {
+  return guard([&] {
+    if (!src || !dst || !count) return (int)PB_ENULL;
+    if (extra_count < 0) return (int)PB_EINVALID_ARGUMENT;
+    Pencil A = pencil_from_desc(src), B = pencil_from_desc(dst);
+    same_topology_and_shape(A, B);
+    if (rank_lo < 0 || rank_hi > A.nranks() || rank_lo >= rank_hi) return (int)PB_EINVALID_ARGUMENT;
+    pb_plan P;  // geometry only: no device tables
+    P.extra = extra_count;
+    P.sliced = true;
+    P.slice_lo = rank_lo;
+    P.slice_hi = rank_hi;
+    const SliceXchg X = slice_exchange(P, A, B, 8, false);
+    *count = (int32_t)X.transfers.size();
+    if (transfers)
+      for (int i = 0; i < (int)X.transfers.size() && i < capacity; ++i) transfers[i] = X.transfers[i];
+    if (send_elems) *send_elems = X.send_elems;
+    if (recv_elems) *recv_elems = X.recv_elems;
+    return (int)PB_OK;
+  });
 }
 
 }  // extern "C"

@@ -55,6 +55,22 @@ class PbPlanInfo(C.Structure):
                 ("workspace_bytes", C.c_int64), ("passes_forward", C.c_int32), ("passes_inverse", C.c_int32)]
 
 
+class PbSliceInfo(C.Structure):
+    _fields_ = [("rank_lo", C.c_int32), ("rank_hi", C.c_int32), ("input_elems", C.c_int64),
+                ("output_elems", C.c_int64), ("workspace_bytes", C.c_int64)]
+
+
+class PbSliceBoundary(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("elem_bytes", C.c_int32), ("ntransfers", C.c_int32), ("acc_groups", C.c_int32),
+                ("send_offset", C.c_int64), ("recv_offset", C.c_int64), ("send_elems", C.c_int64),
+                ("recv_elems", C.c_int64), ("acc_offset", C.c_int64), ("status_offset", C.c_int64)]
+
+
+class PbSliceTransfer(C.Structure):
+    _fields_ = [("receive", C.c_int32), ("rank", C.c_int32), ("peer", C.c_int32), ("reserved", C.c_int32),
+                ("offset", C.c_int64), ("count", C.c_int64)]
+
+
 _P = C.c_void_p
 SIGNATURES = {
     "pb_version": ([], C.c_char_p),
@@ -87,6 +103,17 @@ SIGNATURES = {
                       _P, _P], C.c_int),
     "pb_field_write": ([C.c_char_p, C.POINTER(PbPencilDesc), C.c_int32, _P, C.c_int32, _P, _P], C.c_int),
     "pb_field_read": ([C.c_char_p, C.POINTER(PbPencilDesc), C.c_int32, _P, C.c_int32, _P, _P], C.c_int),
+    "pb_slice_create": ([_P, C.c_int32, C.c_int32, C.POINTER(_P)], C.c_int),
+    "pb_slice_get_info": ([_P, C.POINTER(PbSliceInfo)], C.c_int),
+    "pb_slice_phases": ([_P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+    "pb_slice_boundary": ([_P, C.c_int32, C.c_int32, C.POINTER(PbSliceBoundary)], C.c_int),
+    "pb_slice_transfers": ([_P, C.c_int32, C.c_int32, C.POINTER(PbSliceTransfer), C.c_int32, C.POINTER(C.c_int32)],
+                           C.c_int),
+    "pb_slice_execute_phase": ([_P, C.c_int32, C.c_int32, _P, _P, _P, _P], C.c_int),
+    "pb_slice_destroy": ([_P], C.c_int),
+    "pb_exchange_transfers": ([C.POINTER(PbPencilDesc), C.POINTER(PbPencilDesc), C.c_int64, C.c_int32, C.c_int32,
+                               C.POINTER(PbSliceTransfer), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                               C.POINTER(C.c_int64)], C.c_int),
     "pb_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_P)],
                         C.c_int),
     "pb_batch_workspace_bytes": ([_P, C.POINTER(C.c_int64)], C.c_int),

@@ -91,10 +91,11 @@ def test_single_pass_plan_in_place():
 
 
 def test_c2r_plan_in_place_starts_from_the_spectrum():
-    rplan = pb.R2cPlan.from_shape(pb.MpiTopology((2, 2)), (16, 12, 10), (), dtype=torch.float32)
-    spec = rplan.allocate_output()
-    rplan.forward(torch.randn(rplan.info.input_elems, device="cuda"), spec)
-    plan = pb.C2rPlan.from_shape(pb.MpiTopology((2, 2)), (16, 12, 6), 10, (), dtype=torch.float32)
+    # the C2rPlan reduces axis 0; its raw backward (an R2C) of a real field
+    # gives a spectrum its forward accepts
+    plan = pb.C2rPlan.from_shape(pb.MpiTopology((2, 2)), (6, 12, 16), 10, (), dtype=torch.float32)
+    spec = plan.allocate_input()
+    plan.backward(torch.randn(plan.info.output_elems, device="cuda"), spec)
     ref = plan.allocate_output()
     plan.forward(spec, ref)
     arr = plan.allocate_in_place()
