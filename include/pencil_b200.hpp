@@ -210,10 +210,6 @@ class Plan {
 
  protected:
   explicit Plan(pb_plan* h) : h_(h) { check(pb_plan_get_info(h_, &info_), "plan info"); }
-  static pb_plan* adopt(int rc, pb_plan* h, const char* where) {
-    check(rc, where);
-    return h;
-  }
 
  private:
   void run(int32_t op, const void* in, void* out, void* ws, void* stream) const {
@@ -257,9 +253,9 @@ class C2cPlan : public Plan {
     const pb_geom g = detail::geom(topo, shape, extra, layout);
     const std::vector<uint8_t> m = selection.empty() ? std::vector<uint8_t>() : detail::mask(shape.size(), selection);
     pb_plan* h = nullptr;
-    return C2cPlan(adopt(pb_plan_create_c2c(&g, (int32_t)p, m.empty() ? nullptr : m.data(),
-                                            positive.empty() ? nullptr : positive.data(), &h),
-                         h, "C2cPlan::from_shape"));
+    check(pb_plan_create_c2c(&g, (int32_t)p, m.empty() ? nullptr : m.data(),
+                                            positive.empty() ? nullptr : positive.data(), &h), "C2cPlan::from_shape");
+    return C2cPlan(h);
   }
 
  private:
@@ -274,8 +270,8 @@ class R2cPlan : public Plan {
     const pb_geom g = detail::geom(topo, shape, extra, layout);
     const std::vector<uint8_t> m = selection.empty() ? std::vector<uint8_t>() : detail::mask(shape.size(), selection);
     pb_plan* h = nullptr;
-    return R2cPlan(adopt(pb_plan_create_r2c(&g, (int32_t)p, m.empty() ? nullptr : m.data(), &h), h,
-                         "R2cPlan::from_shape"));
+    check(pb_plan_create_r2c(&g, (int32_t)p, m.empty() ? nullptr : m.data(), &h), "R2cPlan::from_shape");
+    return R2cPlan(h);
   }
 
  private:
@@ -292,8 +288,8 @@ class C2rPlan : public Plan {
     const std::vector<uint8_t> m =
         selection.empty() ? std::vector<uint8_t>() : detail::mask(complex_shape.size(), selection);
     pb_plan* h = nullptr;
-    return C2rPlan(adopt(pb_plan_create_c2r(&g, real_len, (int32_t)p, m.empty() ? nullptr : m.data(), &h), h,
-                         "C2rPlan::from_shape"));
+    check(pb_plan_create_c2r(&g, real_len, (int32_t)p, m.empty() ? nullptr : m.data(), &h), "C2rPlan::from_shape");
+    return C2rPlan(h);
   }
 
  private:
@@ -311,8 +307,8 @@ class R2rPlan : public Plan {
     std::vector<int32_t> k(kinds.size());
     for (size_t i = 0; i < kinds.size(); ++i) k[i] = (int32_t)kinds[i];
     pb_plan* h = nullptr;
-    return R2rPlan(adopt(pb_plan_create_r2r(&g, (int32_t)p, complex_values ? 1 : 0, k.data(), &h), h,
-                         "R2rPlan::from_shape"));
+    check(pb_plan_create_r2r(&g, (int32_t)p, complex_values ? 1 : 0, k.data(), &h), "R2rPlan::from_shape");
+    return R2rPlan(h);
   }
 
  protected:
@@ -344,9 +340,9 @@ class MixedC2cPlan : public Plan {
     std::vector<int32_t> k(transforms.size());
     for (size_t i = 0; i < transforms.size(); ++i) k[i] = (int32_t)transforms[i];
     pb_plan* h = nullptr;
-    return MixedC2cPlan(adopt(pb_plan_create_mixed_c2c(&g, (int32_t)p, k.data(),
-                                                       positive.empty() ? nullptr : positive.data(), &h),
-                              h, "MixedC2cPlan::from_shape"));
+    check(pb_plan_create_mixed_c2c(&g, (int32_t)p, k.data(),
+                                                       positive.empty() ? nullptr : positive.data(), &h), "MixedC2cPlan::from_shape");
+    return MixedC2cPlan(h);
   }
 
  private:
@@ -362,8 +358,8 @@ class MixedR2cPlan : public Plan {
     std::vector<int32_t> k(transforms.size());
     for (size_t i = 0; i < transforms.size(); ++i) k[i] = (int32_t)transforms[i];
     pb_plan* h = nullptr;
-    return MixedR2cPlan(adopt(pb_plan_create_mixed_r2c(&g, (int32_t)p, k.data(), &h), h,
-                              "MixedR2cPlan::from_shape"));
+    check(pb_plan_create_mixed_r2c(&g, (int32_t)p, k.data(), &h), "MixedR2cPlan::from_shape");
+    return MixedR2cPlan(h);
   }
 
  private:

@@ -577,13 +577,21 @@ __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, 
 
 constexpr int MR_MAX_PIECES = 64;  // pieces of a transposed store (the plan allows at most 64)
 
+// Outputs per line the row tables of the transposed store hold: N, or 2N for
+// the real-to-real kernel, whose type-IV kinds write n = 2N outputs from an
+// N-point FFT.
+template <int N, bool R2R>
+__host__ __device__ constexpr int mr_table_len() {
+  return R2R ? 2 * N : N;
+}
+
 // Shared memory of one CTA: two buffers of NSEQ padded sequences, the twiddle
 // table, and the destination rows, k table and piece rows of the transposed
 // store.
-template <typename R, int N>
+template <typename R, int N, bool R2R = false>
 __host__ __device__ constexpr size_t mr_smem_bytes() {
-  return (2 * (size_t)MRGeom<R, N>::NSEQ * MRGeom<R, N>::SEQ + ((N + 1) & ~1)) * 2 * sizeof(R) + (size_t)N * 16 +
-         (size_t)MR_MAX_PIECES * 16;
+  return (2 * (size_t)MRGeom<R, N>::NSEQ * MRGeom<R, N>::SEQ + ((N + 1) & ~1)) * 2 * sizeof(R) +
+         (size_t)mr_table_len<N, R2R>() * 16 + (size_t)MR_MAX_PIECES * 16;
 }
 
 template <typename R, int N, bool INV, bool SX, bool DS>
@@ -656,9 +664,10 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   C* b0 = reinterpret_cast<C*>(smem);
   C* b1 = b0 + BUF;
   C* W = b1 + BUF;
+  constexpr int KT = mr_table_len<N, R2R>();
   long long* Atab = reinterpret_cast<long long*>(W + ((N + 1) & ~1));
-  int2* ktab = reinterpret_cast<int2*>(Atab + N);
-  PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + N);
+  int2* ktab = reinterpret_cast<int2*>(Atab + KT);
+  PieceAddr* prow = reinterpret_cast<PieceAddr*>(ktab + KT);
 
   long long tile = first;
   if (tile >= end) return;

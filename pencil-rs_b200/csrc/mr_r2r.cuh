@@ -1,12 +1,14 @@
 // Real-to-real kinds on the mixed-radix pass kernel: the DHT, DCT-II/III,
-// DST-II/III (Makhoul's n-point FFT), DCT-I (even extension, 2(n-1) points)
-// and DST-I (odd extension, 2(n+1) points), for real data (two lines per
+// DST-II/III (Makhoul's n-point FFT), DCT-I (even extension, 2(n-1) points),
+// DST-I (odd extension, 2(n+1) points), for real data (two lines per
 // complex FFT) and complex data (one line per FFT: real and imaginary parts
-// are the pair).  The kinds are the reference's FFTW REDFT/RODFT definitions
+// are the pair), and DCT-IV / DST-IV of even n (one n/2-point FFT per real
+// line, or per component of a complex line, with pre- and post-twiddles).
+// The kinds are the reference's FFTW REDFT/RODFT definitions
 // (crates/pencil-fft/src/r2r.rs:697-848) and the Hartley transform
 // (dht.rs:201-353), computed as in the generic pass kernel: the
 // pre-processing runs in the register-fed stage-0 load, the post-processing in
-// the store.  The type-IV kinds stay on the generic kernel.
+// the store.
 #pragma once
 
 #include "mr_kernel.cuh"
@@ -37,10 +39,63 @@ struct R2rSource {
 };
 
 // Line length n of kind SUB on an N-point FFT: N for the DHT and the type-II
-// and type-III kinds, N/2 + 1 for DCT-I, N/2 - 1 for DST-I.
+// and type-III kinds, N/2 + 1 for DCT-I, N/2 - 1 for DST-I, 2N for the type-IV
+// kinds.
 template <int N, int SUB>
 __host__ __device__ constexpr int r2r_len() {
-  return SUB == S_DCT1 ? N / 2 + 1 : (SUB == S_DST1 ? N / 2 - 1 : N);
+  return SUB == S_DCT1   ? N / 2 + 1
+         : SUB == S_DST1 ? N / 2 - 1
+         : (SUB == S_DCT4 || SUB == S_DST4) ? 2 * N
+                                             : N;
+}
+
+// Type-IV kinds (even n = 2N): each pair of the tile (two real lines, or one
+// complex line) is two FFT sequences, 2p + c for line / component c of pair p.
+// Input q of a sequence is (x[2q] + i x[n-1-2q]) * exp(-i pi (4q+1) / (4n))
+// (aux0), with the input reversed for DST-IV (x[n-1-j]).
+template <typename R, int N, int SUB>
+__device__ __forceinline__ void mr_load_r2r_iv(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                               const PassArgs& A, const TileAddr& ta) {
+  using C = typename Cx<R>::T;
+  using G = MRGeom<R, N>;
+  constexpr int NB = G::NB0;
+  constexpr int R0 = G::R0;
+  constexpr int n = 2 * N;
+  const R zero = R(0);
+  const int L = ta.lines;
+  const bool cplx = A.in_complex != 0;
+  const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
+  const R* __restrict__ inr = reinterpret_cast<const R*>(A.in);
+  const R pf = R(A.pre_factor);
+#pragma unroll
+  for (int u = 0; u < G::U0; ++u) {
+    const int b = threadIdx.x + u * MR_THREADS;
+    const int s = b / NB;
+    const int jb = b - s * NB;
+    const int p = s >> 1, c = s & 1;
+    const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
+    // element j of this sequence's real line: real data line 2p + c, complex
+    // data component c of line p (interleaved (re, im) in units of R)
+    const bool ok = live && (cplx ? p < L : 2 * p + c < L);
+    const long long base = cplx ? 2 * (ta.src0 + (long long)p * ta.srcb) + c : ta.src0 + (long long)(2 * p + c) * ta.srcb;
+    const int step = cplx ? 2 : 1;
+#pragma unroll
+    for (int r = 0; r < R0; ++r) {
+      const int q = jb + r * NB;
+      int j0 = 2 * q, j1 = n - 1 - 2 * q;
+      if (SUB == S_DST4) {
+        j0 = n - 1 - j0;
+        j1 = n - 1 - j1;
+      }
+      R x0 = ok ? inr[base + (long long)j0 * step] : zero;
+      R x1 = ok ? inr[base + (long long)j1 * step] : zero;
+      if (A.pre_mode != W_NONE) {
+        if (weight_hit(A.pre_mode, j0, n)) x0 *= pf;
+        if (weight_hit(A.pre_mode, j1, n)) x1 *= pf;
+      }
+      v[u][r] = cmul(mk<C, R>(x0, x1), aux0[q]);
+    }
+  }
 }
 
 // Stage-0 butterfly inputs of one tile (FFT input q of each pair), for the
@@ -134,21 +189,39 @@ __device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>:
     case S_DST1:
       if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DST1>(v, A, ta);
       break;
+    case S_DCT4: mr_load_r2r_iv<R, N, S_DCT4>(v, A, ta); break;
+    case S_DST4: mr_load_r2r_iv<R, N, S_DST4>(v, A, ta); break;
     default: mr_load_r2r_k<R, N, S_DHT>(v, A, ta); break;
   }
 }
 
 // Outputs k of both lines of a pair (x: first line / real part, y: second
-// line / imaginary part), from the natural-order FFT results `seq`.
+// line / imaginary part), from the natural-order FFT results `seq` (for the
+// type-IV kinds the pair's two sequences, seq and seq + SEQ).
 template <typename R, int N, int SUB>
 __device__ __forceinline__ typename Cx<R>::T r2r_output(const typename Cx<R>::T* seq, int k,
-                                                       const typename Cx<R>::T* __restrict__ aux0) {
+                                                       const typename Cx<R>::T* __restrict__ aux0,
+                                                       const typename Cx<R>::T* __restrict__ aux1) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
   constexpr int n = r2r_len<N, SUB>();
   constexpr int sub = SUB;
   const R h = R(0.5);
   switch (sub) {
+    case S_DCT4:
+    case S_DST4: {
+      // output 2kk = 2 Re(U[kk] w), output n-1-2kk = -2 Im(U[kk] w), w = exp(-i pi kk / n)
+      const bool odd = (k & 1) != 0;
+      const int kk = odd ? (n - 1 - k) >> 1 : k >> 1;
+      const C w = aux1[kk];
+      const C u0 = cmul(seq[G::pad(kk)], w), u1 = cmul(seq[G::SEQ + G::pad(kk)], w);
+      R a = odd ? R(-2) * u0.y : R(2) * u0.x, b = odd ? R(-2) * u1.y : R(2) * u1.x;
+      if (sub == S_DST4 && odd) {
+        a = -a;
+        b = -b;
+      }
+      return mk<C, R>(a, b);
+    }
     case S_DCT2:
     case S_DST2: {
       const int kk = (sub == S_DST2) ? n - 1 - k : k;
@@ -186,8 +259,10 @@ __device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr
                                                const long long* Atab) {
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N>;
-  constexpr int NSEQ = G::NSEQ;
-  constexpr int SEQ = G::SEQ;
+  // pairs of the tile: one FFT sequence each, two for the type-IV kinds
+  constexpr bool IV = SUB == S_DCT4 || SUB == S_DST4;
+  constexpr int NSEQ = IV ? G::NSEQ / 2 : G::NSEQ;
+  constexpr int SEQ = IV ? 2 * G::SEQ : G::SEQ;
   constexpr int n = r2r_len<N, SUB>();
   const int tid = threadIdx.x;
   const int L = ta.lines;
@@ -196,6 +271,7 @@ __device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr
   const R pf = R(A.post_factor);
   const int post_mode = A.post_mode;
   const C* __restrict__ aux0 = reinterpret_cast<const C*>(A.aux0);
+  const C* __restrict__ aux1 = reinterpret_cast<const C*>(A.aux1);
   const bool direct = A.dst_k_contig != 0;
   // destination in units of the real type: a pair at element o is aligned
   // to its two-element vector when a4 + o is even (buffers are aligned to
@@ -211,7 +287,7 @@ __device__ __forceinline__ void mr_store_r2r_k(const PassArgs& A, const TileAddr
       k = i / NSEQ;
     }
     if (cplx ? s >= L : 2 * s >= L) continue;
-    C v = r2r_output<R, N, SUB>(res + s * SEQ, k, aux0);
+    C v = r2r_output<R, N, SUB>(res + s * SEQ, k, aux0, aux1);
     R f = sc;
     if (post_mode != W_NONE && weight_hit(post_mode, k, n)) f *= pf;
     v = scl(v, f);
@@ -253,6 +329,8 @@ __device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& 
     case S_DST1:
       if constexpr (N % 2 == 0) mr_store_r2r_k<R, N, S_DST1>(A, ta, res, Atab);
       break;
+    case S_DCT4: mr_store_r2r_k<R, N, S_DCT4>(A, ta, res, Atab); break;
+    case S_DST4: mr_store_r2r_k<R, N, S_DST4>(A, ta, res, Atab); break;
     default: mr_store_r2r_k<R, N, S_DHT>(A, ta, res, Atab); break;
   }
 }
@@ -289,7 +367,7 @@ __global__ void __launch_bounds__(MR_THREADS, 2) mr_r2r_kernel(const PassArgs A)
 
 template <typename R, int N>
 cudaError_t mr_r2r_launch(const PassArgs& A, cudaStream_t stream) {
-  constexpr size_t smem = mr_smem_bytes<R, N>();
+  constexpr size_t smem = mr_smem_bytes<R, N, true>();
   cudaError_t err = cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
@@ -300,7 +378,7 @@ cudaError_t mr_r2r_launch(const PassArgs& A, cudaStream_t stream) {
 
 template <typename R, int N>
 int mr_r2r_occupancy() {
-  constexpr size_t smem = mr_smem_bytes<R, N>();
+  constexpr size_t smem = mr_smem_bytes<R, N, true>();
   int blocks = 0;
   if (cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)

@@ -1117,7 +1117,8 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   }
   // real-to-real kinds on the mixed-radix kernel (all but the type-IV kinds):
   // the same layout conditions, FFT lengths of kMrR2rLengths
-  if (!A.fast && !P.force_generic && op.kind == P_R2R && op.sub != S_DCT4 && op.sub != S_DST4 &&
+  const bool iv4 = op.sub == S_DCT4 || op.sub == S_DST4;
+  if (!A.fast && !P.force_generic && op.kind == P_R2R && (!iv4 || A.n % 2 == 0) &&
       mr_r2r_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
@@ -1125,7 +1126,8 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
     if (direct || transposed) {
       A.fast = 3;
       A.dst_k_contig = direct ? 1 : 0;
-      L = mr_r2r_lines(A.m, in_complex ? 1 : 0, P.real_bytes);
+      // a pair of lines per FFT sequence; the type-IV kinds take a sequence per line
+      L = mr_r2r_lines(A.m, in_complex ? 1 : 0, P.real_bytes) / (iv4 ? 2 : 1);
       A.lines = L;
     }
   }
@@ -1142,6 +1144,15 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       L = mr_batch_lines(A.m, op.kind);
       A.lines = L;
     }
+  }
+  // the register kernels' row tables hold A.m outputs per line (2 A.m in the
+  // real-to-real kernel): anything longer stays on the generic kernel
+  if (A.fast && A.n_out > (A.fast == 3 ? 2 * A.m : (A.half ? 2 * A.m : A.m))) {
+    A.fast = 0;
+    A.half = 0;
+    A.m = fft_len(op.kind, op.sub, A.n);
+    A.twiddle = enc(roots_table(P, A.m));
+    A.dst_k_contig = (dst.perm[N - 1] == a) ? 1 : 0;
   }
   if (!A.fast) L = choose_lines(P, A, pair_kind ? 1 : 0);
   if (!A.fast && P.force_generic) {

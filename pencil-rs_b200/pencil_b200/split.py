@@ -161,7 +161,11 @@ class SplitPlan:
         b = L.PbSliceBoundary()
         L.check(lib.pb_slice_boundary(self._h, op, k, C.byref(b)), "slice boundary")
         s = torch.cuda.current_stream() if stream is None else stream
-        s.synchronize()  # the phase's device work is done before the host moves its data
+        if self.host_staged:
+            s.synchronize()  # the phase's device work is done before the host copies its blocks
+        # with device transports everything below is ordered on the stream
+        # (NCCL's send/recv and all-reduce wait for it and it waits for them):
+        # the host queues the next phase without waiting for the GPU
         if b.kind == EXCHANGE:
             n = C.c_int32()
             tab = (L.PbSliceTransfer * max(b.ntransfers, 1))()
@@ -169,30 +173,30 @@ class SplitPlan:
             send = ws[b.send_offset:b.send_offset + b.send_elems * b.elem_bytes]
             recv = ws[b.recv_offset:b.recv_offset + b.recv_elems * b.elem_bytes]
             table = transfer_table(tab[:n.value])
-            if self.host_staged:
-                hs, hr = send.cpu(), recv.cpu()
-                exchange(table, hs, hr, b.elem_bytes, self.ranges, self.me, self.group)
-                recv.copy_(hr)
-            else:
-                exchange(table, send, recv, b.elem_bytes, self.ranges, self.me, self.group)
-            torch.cuda.synchronize(ws.device)
+            with torch.cuda.stream(s):
+                if self.host_staged:
+                    hs, hr = send.cpu(), recv.cpu()
+                    exchange(table, hs, hr, b.elem_bytes, self.ranges, self.me, self.group)
+                    recv.copy_(hr)
+                else:
+                    exchange(table, send, recv, b.elem_bytes, self.ranges, self.me, self.group)
             return
         acc = ws[b.acc_offset:b.acc_offset + b.acc_groups * 32].view(torch.float64).view(-1, 4)
         flag = ws[b.status_offset + 4:b.status_offset + 8].view(torch.int32)
         if self.world > 1:
-            dev = torch.device("cpu") if self.host_staged else acc.device
-            mx = acc[:, 0:2].contiguous().to(dev)
-            sm = acc[:, 2:4].contiguous().to(dev)
-            fl = flag.clone().to(dev)
-            if b.kind in (REDUCE_MAX_SUM, REDUCE_MAX):
-                dist.all_reduce(mx, op=dist.ReduceOp.MAX, group=self.group)
-                dist.all_reduce(fl, op=dist.ReduceOp.MAX, group=self.group)
-                acc[:, 0:2] = mx.to(acc.device)
-                flag.copy_(fl.to(flag.device))
-            if b.kind in (REDUCE_MAX_SUM, REDUCE_SUM):
-                dist.all_reduce(sm, op=dist.ReduceOp.SUM, group=self.group)
-                acc[:, 2:4] = sm.to(acc.device)
-        torch.cuda.synchronize(ws.device)
+            with torch.cuda.stream(s):
+                dev = torch.device("cpu") if self.host_staged else acc.device
+                mx = acc[:, 0:2].contiguous().to(dev)
+                sm = acc[:, 2:4].contiguous().to(dev)
+                fl = flag.clone().to(dev)
+                if b.kind in (REDUCE_MAX_SUM, REDUCE_MAX):
+                    dist.all_reduce(mx, op=dist.ReduceOp.MAX, group=self.group)
+                    dist.all_reduce(fl, op=dist.ReduceOp.MAX, group=self.group)
+                    acc[:, 0:2] = mx.to(acc.device)
+                    flag.copy_(fl.to(flag.device))
+                if b.kind in (REDUCE_MAX_SUM, REDUCE_SUM):
+                    dist.all_reduce(sm, op=dist.ReduceOp.SUM, group=self.group)
+                    acc[:, 2:4] = sm.to(acc.device)
 
     def _check_status(self, op, ws, stream):
         b = L.PbSliceBoundary()

@@ -1,9 +1,10 @@
 """The real-to-real kinds on the mixed-radix pass kernel (DHT, DCT-I/II/III,
-DST-I/II/III; the type-IV kinds stay on the generic kernel) against the
-oracle: forward, normalised inverse and raw backward, real and complex data,
-f32 and f64, power-of-two and mixed-radix lengths, on grids whose routes take
-both the direct and the transposed store; the 384-point DST-I runs a
-770-point FFT (radix 11).  Tolerances as in the other parity tests."""
+DST-I/II/III, and DCT-IV / DST-IV of even length through an n/2-point FFT)
+against the oracle: forward, normalised inverse and raw backward, real and
+complex data, f32 and f64, power-of-two and mixed-radix lengths, on grids
+whose routes take both the direct and the transposed store; the 384-point
+DST-I runs a 770-point FFT (radix 11).  Tolerances as in the other parity
+tests."""
 
 import numpy as np
 import pytest
@@ -50,6 +51,27 @@ def test_r2r_kinds_on_the_mixed_radix_kernel(rb, cplx, kind, case):
         check_transform(plan, route, x, 2, rb, cplx, d)
 
 
+# type IV of even n: FFT length n/2 (every axis here has n/2 in the kernel's lengths)
+CASES_IV = [((2, 3), (128, 80, 96)), ((2, 2), (70, 72, 100)), ((3, 2), (384, 64, 98))]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("kind", ["DctIV", "DstIV"])
+@pytest.mark.parametrize("case", range(len(CASES_IV)))
+def test_type_iv_kinds_on_the_mixed_radix_kernel(rb, cplx, kind, case):
+    dims, shape = CASES_IV[case]
+    rng = np.random.default_rng(40 + case)
+    kinds = [kind] * len(shape)
+    dtype = CDT[rb] if cplx else RDT[rb]
+    plan = pb.R2rPlan.from_shape(pb.MpiTopology(dims), shape, (2,), kinds, dtype=dtype)
+    assert plan.step_kernels(L.FORWARD) == ["mixed_radix"] * 3, plan.step_kernels(L.FORWARD)
+    route = po.r2r_route(po.Topology(dims), shape, kinds)
+    x = rand_field(rng, shape, (2,), cplx, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, 2, rb, cplx, d)
+
+
 @pytest.mark.parametrize("rb", [4, 8])
 def test_dst1_384_runs_a_770_point_fft(rb):
     """The mixed-kind workload's DST-I axis: n = 384, FFT length 770 = 2*5*7*11."""
@@ -64,12 +86,14 @@ def test_dst1_384_runs_a_770_point_fft(rb):
         check_transform(plan, route, x, 3, rb, False, d)
 
 
-@pytest.mark.parametrize("kinds", [("DctII", "DstI", "Dht"), ("DstIII", "DctI", "DstII"), ("DctIII", "Dht", "DctI")])
+@pytest.mark.parametrize("kinds", [("DctII", "DstI", "Dht"), ("DstIII", "DctI", "DstII"), ("DctIII", "Dht", "DctI"),
+                                   ("DctIV", "DstIV", "DctIV")])
 @pytest.mark.parametrize("cplx", [False, True])
 def test_r2r_vjp_adjoint_identity_f64_mixed_radix(kinds, cplx):
     """<A x, y> == <x, A^T y> for forward, inverse and backward of the R2R plan."""
     rng = np.random.default_rng(31)
-    plan = pb.R2rPlan.from_shape(pb.MpiTopology((2, 3)), (40, 64, 36), (2,), kinds,
+    shape = (64, 128, 72) if kinds[0] == "DctIV" else (40, 64, 36)
+    plan = pb.R2rPlan.from_shape(pb.MpiTopology((2, 3)), shape, (2,), kinds,
                                  dtype=torch.complex128 if cplx else torch.float64)
     assert "mixed_radix" in plan.step_kernels(L.FORWARD)
 
