@@ -213,6 +213,36 @@ int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capac
  * (7-smooth lengths).  A diagnostic with no counterpart in the reference. */
 int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int32_t capacity, int32_t* count);
 
+/* Autotuner (no counterpart in the reference, whose line FFTs are RustFFT
+ * plans): for every pass of the plan's operations that runs a register kernel,
+ * times the candidate configurations on scratch buffers and keeps the
+ * fastest: the mixed-radix schedule (0: the default, fewest stages with
+ * composite radices up to 16 in f32; 1: radices up to 8, where that differs)
+ * and the persistent grid (1 .. max resident CTAs per SM).  Choices are cached
+ * per pass shape for the process (and in the file named by PB_TUNE_CACHE when
+ * set, shared with the batch tuner) and applied to later plans with the same
+ * pass shapes at creation.  Synchronous; allocates scratch for the timings. */
+int pb_plan_autotune(pb_plan* plan);
+/* Manual override of the same choices for every register-kernel pass: sched
+ * (-1 keeps each pass's, 0 or 1 where the length has it) and ctas_per_sm (0
+ * keeps, else capped at the kernel's occupancy). */
+int pb_plan_set_config(pb_plan* plan, int32_t sched, int32_t ctas_per_sm);
+
+/* Configuration of launch `step` of operation `op` (the order of
+ * pb_plan_steps), a diagnostic. */
+typedef struct pb_step_config {
+  int32_t kernel;     /* as pb_plan_step_kernels */
+  int32_t fft_len;    /* points of one FFT sequence */
+  int32_t lines;      /* lines per tile */
+  int32_t grid_ctas;  /* persistent grid (0: one CTA per tile) */
+  int32_t ctas_per_sm;
+  int32_t sched;      /* mixed-radix schedule */
+  int32_t tuned;      /* 1: chosen by the autotuner */
+  int32_t nradix;
+  int32_t radix[12];  /* stage radices, stage 0 first */
+} pb_step_config;
+int pb_plan_step_config(const pb_plan* plan, int32_t op, int32_t step, pb_step_config* out);
+
 /* Allocation-free execution.  No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they execute (host callbacks,
  * real-time loops, embedders whose device memory is a fixed pre-set budget).

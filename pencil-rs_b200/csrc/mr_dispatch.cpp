@@ -80,9 +80,28 @@ int mr_lines(int m, int kind, int real_bytes) {
   return kind == P_C2C ? e->nseq : 2 * e->nseq;
 }
 
-int mr_occupancy(int m, int real_bytes) {
+int mr_occupancy(int m, int real_bytes, int sched) {
   const MrEntry* e = entry(m, real_bytes);
-  return e ? e->occupancy() : 1;
+  return e ? e->occupancy(sched) : 1;
+}
+
+int mr_schedules(int m, int real_bytes) {
+  const MrEntry* e = entry(m, real_bytes);
+  return e ? e->nsched : 0;
+}
+
+int mr_radices(int m, int real_bytes, int sched, int* radices, int cap) {
+  const MrEntry* e = entry(m, real_bytes);
+  if (!e || sched < 0 || sched >= e->nsched) return 0;
+  for (int i = 0; i < e->nrad[sched] && i < cap; ++i) radices[i] = e->rad[sched][i];
+  return e->nrad[sched];
+}
+
+int mr_r2r_radices(int m, int real_bytes, int* radices, int cap) {
+  const MrEntry* e = r2r_entry(m, real_bytes);
+  if (!e) return 0;
+  for (int i = 0; i < e->nrad[0] && i < cap; ++i) radices[i] = e->rad[0][i];
+  return e->nrad[0];
 }
 
 cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream) {
@@ -103,7 +122,7 @@ int mr_r2r_lines(int m, int complex_data, int real_bytes) {
 
 int mr_r2r_occupancy(int m, int real_bytes) {
   const MrEntry* e = r2r_entry(m, real_bytes);
-  return e ? e->occupancy() : 1;
+  return e ? e->occupancy(0) : 1;
 }
 
 cudaError_t launch_mr_r2r(const PassArgs& A, int real_bytes, cudaStream_t stream) {

@@ -28,6 +28,7 @@
 
 #include <cuda_runtime.h>
 
+#include "mr_lengths.hpp"
 #include "pb_aux.hpp"
 #include "pb_device.cuh"
 #include "pb_fft.cuh"
@@ -124,7 +125,7 @@ __host__ __device__ constexpr int mr_tw_off(const RadixList& L, int ST) {
 }
 
 // Complex elements per tile: 3072 (24 KB) in f32, 1536 (24 KB) in f64.
-template <typename R, int N>
+template <typename R, int N, int S = 0>
 struct MRGeom {
   static constexpr int TILE_ELEMS = sizeof(R) == 4 ? 3072 : 1536;
   static constexpr int FIT = TILE_ELEMS / N;
@@ -141,7 +142,9 @@ struct MRGeom {
   // the stage radices: composites up to 16 in f32 and 8 in f64 (register
   // budget; fewer stages won over full thread use in a per-length sweep), and
   // radix 8 for powers of two (two radix-16 stages leave half the threads idle)
-  static constexpr int MAX_RADIX = (sizeof(R) == 4 && (N & (N - 1)) != 0) ? 16 : 8;
+  // schedule S = 1 caps the radices at 8 in f32 too (the autotuner's
+  // alternative: more stages, each with more butterflies per thread)
+  static constexpr int MAX_RADIX = (S == 0 && sizeof(R) == 4 && (N & (N - 1)) != 0) ? 16 : 8;
   static constexpr RadixList RL = mr_sched(N, NSEQ, MAX_RADIX);
   static constexpr int NST = RL.n;
   static constexpr int R0 = RL.r[0];
@@ -157,11 +160,11 @@ struct MRGeom {
 // W_N^{k*r*N/(NS*RAD)}, outputs (jb - k)*RAD + k + r*NS.  Work item b is
 // butterfly b / NSEQ of sequence b % NSEQ: the lanes of a warp cover NSEQ
 // sequences at a few butterflies, so the twiddle reads are broadcasts.
-template <typename R, int N, int ST, bool INV>
+template <typename R, int N, int ST, bool INV, int S = 0>
 __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ in, typename Cx<R>::T* __restrict__ out,
                                          const typename Cx<R>::T* __restrict__ Wst) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int RAD = G::RL.r[ST];
   constexpr int NS = mr_ns(G::RL, ST);
   constexpr int NB = N / RAD;
@@ -191,23 +194,23 @@ __device__ __forceinline__ void mr_stage(const typename Cx<R>::T* __restrict__ i
 
 // Stages ST .. END-1 of one tile (ST >= 1): stage i reads b0 when i is odd
 // and b1 when it is even (stage 0 writes b0), with a barrier after each.
-template <typename R, int N, bool INV, int ST, int END>
+template <typename R, int N, bool INV, int ST, int END, int S = 0>
 __device__ __forceinline__ void mr_stages_upto(typename Cx<R>::T* b0, typename Cx<R>::T* b1,
                                                const typename Cx<R>::T* Wst) {
   if constexpr (ST < END) {
     if constexpr (ST % 2 == 1)
-      mr_stage<R, N, ST, INV>(b0, b1, Wst);
+      mr_stage<R, N, ST, INV, S>(b0, b1, Wst);
     else
-      mr_stage<R, N, ST, INV>(b1, b0, Wst);
+      mr_stage<R, N, ST, INV, S>(b1, b0, Wst);
     __syncthreads();
-    mr_stages_upto<R, N, INV, ST + 1, END>(b0, b1, Wst);
+    mr_stages_upto<R, N, INV, ST + 1, END, S>(b0, b1, Wst);
   }
 }
 
 // Fills the per-stage twiddle table from the table of N-th roots.
-template <typename R, int N, int ST>
+template <typename R, int N, int ST, int S = 0>
 __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const typename Cx<R>::T* __restrict__ Wg) {
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   if constexpr (ST < G::NST) {
     constexpr int RAD = G::RL.r[ST];
     constexpr int NS = mr_ns(G::RL, ST);
@@ -217,7 +220,7 @@ __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const t
       const int r = i / NS + 1, k = i - (i / NS) * NS;
       Wst[OFF + i] = Wg[k * TW * r];
     }
-    mr_fill_twiddles<R, N, ST + 1>(Wst, Wg);
+    mr_fill_twiddles<R, N, ST + 1, S>(Wst, Wg);
   }
 }
 
@@ -225,11 +228,11 @@ __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const t
 // (sequence b / NB0, index jb) takes elements jb + r*NB0 of its sequence.
 // SX, strided lines (C2C, R2C): item b is butterfly b / NSEQ of sequence
 // b % NSEQ, so the lanes read adjacent lines at each position of the axis.
-template <typename R, int N, bool SX = false>
-__device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0], const PassArgs& A,
+template <typename R, int N, bool SX = false, int S = 0>
+__device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N, S>::U0][MRGeom<R, N, S>::R0], const PassArgs& A,
                                         const TileAddr& ta) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int NB = G::NB0;
   constexpr int R0 = G::R0;
   const R zero = R(0);
@@ -300,11 +303,11 @@ __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N>::U0]
 }
 
 // Stage 0 (no twiddles) on the registers; outputs jb*R0 + r go to `out`.
-template <typename R, int N, bool INV, bool SX = false>
-__device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+template <typename R, int N, bool INV, bool SX = false, int S = 0>
+__device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N, S>::U0][MRGeom<R, N, S>::R0],
                                           typename Cx<R>::T* out) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int NB = G::NB0;
   constexpr int R0 = G::R0;
 #pragma unroll
@@ -326,13 +329,13 @@ __device__ __forceinline__ void mr_stage0(typename Cx<R>::T (&v)[MRGeom<R, N>::U
 // Last stage with the direct C2C or C2R store: in the last Stockham stage
 // (NS = N/RAD) butterfly jb writes outputs jb + r*NB, so each output goes
 // straight to HBM, coalesced across the threads of a sequence.
-template <typename R, int N, bool INV, bool DS>
+template <typename R, int N, bool INV, bool DS, int S = 0>
 __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const TileAddr& ta,
                                                     const typename Cx<R>::T* __restrict__ in,
                                                     const typename Cx<R>::T* __restrict__ W, const long long* Atab,
                                                     const int2* ktab, const PieceAddr* prow) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int ST = G::NST - 1;
   constexpr int RAD = G::RL.r[ST];
   constexpr int NB = N / RAD;
@@ -389,12 +392,12 @@ __device__ __forceinline__ void mr_last_stage_store(const PassArgs& A, const Til
 // one pair to Atab[k] + 2g, a 16-byte vector where aligned in f32.  The lanes
 // of a warp take consecutive g, so they cover whole runs of the destination
 // rows, and no natural-order round through shared memory is needed.
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, int S = 0>
 __device__ __forceinline__ void mr_last_stage_xstore(const PassArgs& A, const TileAddr& ta,
                                                      const typename Cx<R>::T* __restrict__ in,
                                                      const typename Cx<R>::T* __restrict__ W, const long long* Atab) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int ST = G::NST - 1;
   constexpr int RAD = G::RL.r[ST];
   constexpr int NB = N / RAD;
@@ -459,11 +462,11 @@ __device__ __forceinline__ void mr_last_stage_xstore(const PassArgs& A, const Ti
 // transposed store; element (k, line j) of a transposed store goes to
 // Atab[k] + j, each thread writing the pair of lines (j, j+1), as one 16-byte
 // vector where aligned in f32).
-template <typename R, int N, bool DS>
+template <typename R, int N, bool DS, int S = 0>
 __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, const typename Cx<R>::T* res,
                                          const long long* Atab, const int2* ktab, const PieceAddr* prow) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int NSEQ = G::NSEQ;
   constexpr int SEQ = G::SEQ;
   constexpr int H = N / 2 + 1;
@@ -594,19 +597,19 @@ __host__ __device__ constexpr size_t mr_smem_bytes() {
          (size_t)mr_table_len<N, R2R>() * 16 + (size_t)MR_MAX_PIECES * 16;
 }
 
-template <typename R, int N, bool INV, bool SX, bool DS>
+template <typename R, int N, bool INV, bool SX, bool DS, int S = 0>
 __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
-                                        typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
+                                        typename Cx<R>::T (&v)[MRGeom<R, N, S>::U0][MRGeom<R, N, S>::R0],
                                         typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
                                         long long* Atab, const int2* ktab, PieceAddr* prow, const PieceAddr& my_piece,
                                         int npieces) {
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   const int tid = threadIdx.x;
   const bool direct = A.dst_k_contig != 0;  // 2: split across the destination's ranks
   const bool dsplit = DS && A.dst_k_contig == 2;
   const int nout = (A.kind == P_R2C) ? N / 2 + 1 : N;
-  mr_stage0<R, N, INV, SX>(v, b0);
+  mr_stage0<R, N, INV, SX, S>(v, b0);
   if (tid < npieces) prow[tid] = my_piece;
   __syncthreads();
   if (!direct || dsplit) {
@@ -621,21 +624,21 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
   }
   if (direct && A.kind != P_R2C) {
     // stages 1 .. NST-2 in shared memory, the last one to HBM
-    mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
+    mr_stages_upto<R, N, INV, 1, G::NST - 1, S>(b0, b1, W);
     if (G::NST == 2 && dsplit) __syncthreads();  // the row tables above are read next
-    mr_last_stage_store<R, N, INV, DS>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab, ktab, prow);
+    mr_last_stage_store<R, N, INV, DS, S>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab, ktab, prow);
     return;
   }
   if (A.kind == P_C2C) {
     // transposed C2C: the last stage stores from registers; with two stages no
     // barrier follows the row-table writes above before it reads them
-    mr_stages_upto<R, N, INV, 1, G::NST - 1>(b0, b1, W);
+    mr_stages_upto<R, N, INV, 1, G::NST - 1, S>(b0, b1, W);
     if constexpr (G::NST == 2) __syncthreads();
-    mr_last_stage_xstore<R, N, INV>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab);
+    mr_last_stage_xstore<R, N, INV, S>(A, ta, ((G::NST - 2) % 2 == 0) ? b0 : b1, W, Atab);
     return;
   }
-  mr_stages_upto<R, N, INV, 1, G::NST>(b0, b1, W);
-  mr_store<R, N, DS>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab, ktab, prow);
+  mr_stages_upto<R, N, INV, 1, G::NST, S>(b0, b1, W);
+  mr_store<R, N, DS, S>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab, ktab, prow);
 }
 
 // Tiles first, first + step, ... (< end) of one pass: the persistent loop of
@@ -655,11 +658,12 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
                                             const typename Cx<R>::T* W, long long* Atab, const int2* ktab,
                                             PieceAddr* prow, const PieceAddr& my_piece, int npieces);
 
-template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false>
+template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false, int S = 0>
 __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
                                        unsigned char* smem, bool setup) {
+  static_assert(!R2R || S == 0, "the real-to-real kinds run the default schedule");
   using C = typename Cx<R>::T;
-  using G = MRGeom<R, N>;
+  using G = MRGeom<R, N, S>;
   constexpr int BUF = G::NSEQ * G::SEQ;
   C* b0 = reinterpret_cast<C*>(smem);
   C* b1 = b0 + BUF;
@@ -678,7 +682,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
   const int npieces = direct ? 0 : A.npieces;
   if (setup) {
-    mr_fill_twiddles<R, N, 1>(W, reinterpret_cast<const C*>(A.twiddle));
+    mr_fill_twiddles<R, N, 1, S>(W, reinterpret_cast<const C*>(A.twiddle));
     if (!direct)
       for (int k = tid; k < nout; k += MR_THREADS) ktab[k] = A.ktab[k];
   }
@@ -687,7 +691,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   if constexpr (R2R)
     mr_load_r2r<R, N>(v, A, ta);
   else
-    mr_load<R, N, SX>(v, A, ta);
+    mr_load<R, N, SX, S>(v, A, ta);
   TileAddr t1 = ta;
   if (tile + step < end) t1 = load_tile(tiles, tile + step);
   PieceAddr my_piece{0, 0};
@@ -703,7 +707,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
       if constexpr (R2R)
         mr_load_r2r<R, N>(nv, A, t1);
       else
-        mr_load<R, N, SX>(nv, A, t1);
+        mr_load<R, N, SX, S>(nv, A, t1);
       if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
       if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
@@ -714,9 +718,9 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
         mr_tile_r2r<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     } else {
       if (A.inv)
-        mr_tile<R, N, true, SX, DS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile<R, N, true, SX, DS, S>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
       else
-        mr_tile<R, N, false, SX, DS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile<R, N, false, SX, DS, S>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     }
     if (!has_next) break;
     tile += step;
@@ -735,21 +739,31 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
 // 1 strided lines (the source's innermost axis is the tile axis), any store;
 // 2 contiguous lines, split direct store.  Kernels of their own, so that the
 // common one keeps its register allocation.
-template <typename R, int N, int V>
+template <typename R, int N, int V, int S = 0>
 __global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
-  mr_run<R, N, false, V == 1, V != 0>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
+  mr_run<R, N, false, V == 1, V != 0, S>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
 }
 
 inline int mr_variant(const PassArgs& A) { return A.src_k_contig == 0 ? 1 : (A.dst_k_contig == 2 ? 2 : 0); }
 
-// Host entry points of one length (instantiated by mr_kernels.cu).
+// Whether schedule 1 (radices up to 8) differs from the default for this
+// length and precision; only then is it instantiated and tuned.
 template <typename R, int N>
-cudaError_t mr_launch(const PassArgs& A, cudaStream_t stream) {
+constexpr bool mr_sched1_differs() {
+  constexpr RadixList a = MRGeom<R, N, 0>::RL, b = MRGeom<R, N, 1>::RL;
+  if (a.n != b.n) return true;
+  for (int i = 0; i < a.n; ++i)
+    if (a.r[i] != b.r[i]) return true;
+  return false;
+}
+
+template <typename R, int N, int S>
+cudaError_t mr_launch_s(const PassArgs& A, cudaStream_t stream) {
   constexpr size_t smem = mr_smem_bytes<R, N>();
   const int var = mr_variant(A);
-  const auto kern = var == 1 ? mr_kernel<R, N, 1> : var == 2 ? mr_kernel<R, N, 2> : mr_kernel<R, N, 0>;
+  const auto kern = var == 1 ? mr_kernel<R, N, 1, S> : var == 2 ? mr_kernel<R, N, 2, S> : mr_kernel<R, N, 0, S>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
@@ -758,18 +772,51 @@ cudaError_t mr_launch(const PassArgs& A, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-// resident CTAs per SM, the smallest of the variants' figures
+// Host entry points of one length (instantiated by mr_kernels.cu): the
+// schedule is A.sched (0 default, 1 radices up to 8 where that differs).
 template <typename R, int N>
-int mr_occupancy() {
+cudaError_t mr_launch(const PassArgs& A, cudaStream_t stream) {
+  if constexpr (mr_sched1_differs<R, N>())
+    if (A.sched == 1) return mr_launch_s<R, N, 1>(A, stream);
+  return mr_launch_s<R, N, 0>(A, stream);
+}
+
+// resident CTAs per SM of a schedule, the smallest of the variants' figures
+template <typename R, int N, int S>
+int mr_occupancy_s() {
   constexpr size_t smem = mr_smem_bytes<R, N>();
   int best = 0;
-  for (const auto kern : {mr_kernel<R, N, 0>, mr_kernel<R, N, 1>, mr_kernel<R, N, 2>}) {
+  for (const auto kern : {mr_kernel<R, N, 0, S>, mr_kernel<R, N, 1, S>, mr_kernel<R, N, 2, S>}) {
     int blocks = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, MR_THREADS, smem) != cudaSuccess) return 1;
     best = best == 0 ? blocks : std::min(best, blocks);
   }
   return best > 0 ? best : 1;
+}
+
+template <typename R, int N>
+int mr_occupancy(int sched) {
+  if constexpr (mr_sched1_differs<R, N>())
+    if (sched == 1) return mr_occupancy_s<R, N, 1>();
+  return mr_occupancy_s<R, N, 0>();
+}
+
+// The dispatch-table entry of one length: launch, occupancy, sequences per
+// tile, and the radix list of each schedule (stage 0 first).
+template <typename R, int N>
+MrEntry mr_entry() {
+  MrEntry e{};
+  e.launch = &mr_launch<R, N>;
+  e.occupancy = &mr_occupancy<R, N>;
+  e.nseq = MRGeom<R, N>::NSEQ;
+  e.nsched = mr_sched1_differs<R, N>() ? 2 : 1;
+  const RadixList l0 = MRGeom<R, N, 0>::RL, l1 = MRGeom<R, N, 1>::RL;
+  e.nrad[0] = l0.n;
+  e.nrad[1] = l1.n;
+  for (int i = 0; i < l0.n && i < 12; ++i) e.rad[0][i] = l0.r[i];
+  for (int i = 0; i < l1.n && i < 12; ++i) e.rad[1][i] = l1.r[i];
+  return e;
 }
 
 }  // namespace pb

@@ -19,8 +19,8 @@ template <int I>
 static void mr_fill_one(MrEntry* f32, MrEntry* f64) {
   if constexpr (I % MR_GROUPS == MR_GROUP) {
     constexpr int N = kMrLengths[I];
-    f32[I] = MrEntry{&mr_launch<float, N>, &mr_occupancy<float, N>, MRGeom<float, N>::NSEQ};
-    f64[I] = MrEntry{&mr_launch<double, N>, &mr_occupancy<double, N>, MRGeom<double, N>::NSEQ};
+    f32[I] = mr_entry<float, N>();
+    f64[I] = mr_entry<double, N>();
   } else {
     (void)f32;
     (void)f64;

@@ -40,8 +40,11 @@ constexpr int kMrR2rCount = sizeof(kMrR2rLengths) / sizeof(kMrR2rLengths[0]);
 // Entry points of one (precision, length) instantiation.
 struct MrEntry {
   cudaError_t (*launch)(const PassArgs&, cudaStream_t);
-  int (*occupancy)();
-  int nseq;  // complex sequences per tile
+  int (*occupancy)(int sched);  // resident CTAs per SM of a schedule
+  int nseq;                     // complex sequences per tile
+  int nsched;                   // schedules available (1 or 2)
+  int nrad[2];                  // stages of each schedule
+  int rad[2][12];               // their radices, stage 0 first
 };
 
 // Filled by group g: entries i with i % MR_GROUPS == g of both tables.

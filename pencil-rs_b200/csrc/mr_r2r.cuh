@@ -377,7 +377,7 @@ cudaError_t mr_r2r_launch(const PassArgs& A, cudaStream_t stream) {
 }
 
 template <typename R, int N>
-int mr_r2r_occupancy() {
+int mr_r2r_occupancy(int /*sched: the real-to-real kinds run the default schedule*/) {
   constexpr size_t smem = mr_smem_bytes<R, N, true>();
   int blocks = 0;
   if (cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -386,6 +386,19 @@ int mr_r2r_occupancy() {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_r2r_kernel<R, N>, MR_THREADS, smem) != cudaSuccess)
     return 1;
   return blocks > 0 ? blocks : 1;
+}
+
+template <typename R, int N>
+MrEntry mr_r2r_entry() {
+  MrEntry e{};
+  e.launch = &mr_r2r_launch<R, N>;
+  e.occupancy = &mr_r2r_occupancy<R, N>;
+  e.nseq = MRGeom<R, N>::NSEQ;
+  e.nsched = 1;
+  const RadixList l0 = MRGeom<R, N>::RL;
+  e.nrad[0] = l0.n;
+  for (int i = 0; i < l0.n && i < 12; ++i) e.rad[0][i] = l0.r[i];
+  return e;
 }
 
 }  // namespace pb

@@ -19,8 +19,8 @@ template <int I>
 static void mr_r2r_fill_one(MrEntry* f32, MrEntry* f64) {
   if constexpr (I % MR_GROUPS == MR_GROUP) {
     constexpr int N = kMrR2rLengths[I];
-    f32[I] = MrEntry{&mr_r2r_launch<float, N>, &mr_r2r_occupancy<float, N>, MRGeom<float, N>::NSEQ};
-    f64[I] = MrEntry{&mr_r2r_launch<double, N>, &mr_r2r_occupancy<double, N>, MRGeom<double, N>::NSEQ};
+    f32[I] = mr_r2r_entry<float, N>();
+    f64[I] = mr_r2r_entry<double, N>();
   } else {
     (void)f32;
     (void)f64;

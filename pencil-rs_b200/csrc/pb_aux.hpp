@@ -123,7 +123,12 @@ int mr_r2r_occupancy(int m, int real_bytes);
 bool mr_supported(int m, int real_bytes);
 cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int mr_lines(int m, int kind, int real_bytes);
-int mr_occupancy(int m, int real_bytes);
+int mr_occupancy(int m, int real_bytes, int sched = 0);
+// schedules of a length (1, or 2 when radices capped at 8 give another one)
+// and the radix list of one (stage 0 first); 0 when the length has none
+int mr_schedules(int m, int real_bytes);
+int mr_radices(int m, int real_bytes, int sched, int* radices, int cap);
+int mr_r2r_radices(int m, int real_bytes, int* radices, int cap);
 // mixed-radix tile code inside the persistent batch kernel (f32, lengths of
 // kBatchMrLengths): support, lines per tile and shared memory per CTA
 bool mr_batch_supported(int m, int real_bytes);

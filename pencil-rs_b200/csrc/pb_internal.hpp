@@ -114,6 +114,7 @@ struct PassArgs {
   const int2* ktab;       // per output index k: (piece, local index along the transform axis)
   int npieces;
   int grid_ctas;          // persistent grid size
+  int sched;              // mixed-radix schedule: 0 default, 1 radices up to 8 (autotuner)
   int batch_chunk;        // batch kernel: tiles per work item
 };
 

@@ -316,6 +316,7 @@ struct pb_plan {
   bool force_generic = false;                // batch building: no standalone register kernels
   bool batch_mr = false;                     // batch building: mixed-radix tiles where the batch kernel has them
   std::map<std::string, int> tuned_lines;    // batch building: autotuned lines per tile by pass shape
+  bool tuned = false;                        // pb_plan_autotune chose the register kernels' configurations
   bool sliced = false;                       // slice building: only virtual ranks [slice_lo, slice_hi)
   int slice_lo = 0, slice_hi = 0;
   pb::DevPencil spectral_pen{};              // FORWARD output layout (spectral multipliers)
@@ -1336,6 +1337,8 @@ static void build_program(pb_plan& P, int mode) {
   }
 }
 
+static void apply_cached_tuning(pb_plan& P);  // the autotuner's cached choices (end of file)
+
 static void finalize(pb_plan& P) {
   int dev = 0;
   cuda_ok(cudaGetDevice(&dev));
@@ -1343,6 +1346,7 @@ static void finalize(pb_plan& P) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
     P.max_smem = optin;
   for (int m = 0; m < M_COUNT; ++m) build_program(P, m);
+  apply_cached_tuning(P);
   P.spectral_pen = dev_pencil(P, P.host, P.cache, P.fout, P.extra);
   // upload tables
   if (!P.host.bytes.empty()) {
@@ -3964,3 +3968,192 @@ int pb_exchange_transfers(const pb_pencil_desc* src, const pb_pencil_desc* dst, 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Autotuner of the register kernels' runtime configuration
+// ===========================================================================
+namespace pb {
+
+static std::string reg_key(const PassArgs& A, int real_bytes) {
+  return "reg:" + pass_key(A, real_bytes) + "f" + std::to_string(A.fast) + "h" + std::to_string(A.half) + "l" +
+         std::to_string(A.lines) + "T" + std::to_string(A.ntiles) + "p" + std::to_string(A.npieces);
+}
+
+static int reg_occupancy(const PassArgs& A, int real_bytes, int sched) {
+  return A.fast == 3   ? mr_r2r_occupancy(A.m, real_bytes)
+         : A.fast == 2 ? mr_occupancy(A.m, real_bytes, sched)
+         : A.half      ? pow2_half_occupancy(A.m, A.kind)
+                       : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig == 1, real_bytes);
+}
+
+static int sm_count() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+// applies a cached choice ("reg:" keys of the tuner cache) to every pass of P
+static void apply_reg_tuning(pb_plan& P) {
+  const int sms = sm_count();
+  for (int m = 0; m < M_COUNT; ++m)
+    for (Step& st : P.prog[m].steps) {
+      if (st.type != 0 || !st.pa.fast) continue;
+      auto it = g_tune_cache.find(reg_key(st.pa, P.real_bytes));
+      if (it == g_tune_cache.end()) continue;
+      st.pa.sched = it->second / 1000;
+      st.pa.grid_ctas = sms * (it->second % 1000);
+      P.tuned = true;
+    }
+}
+
+static void apply_cached_tuning(pb_plan& P) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  tune_cache_load();
+  apply_reg_tuning(P);
+}
+
+static int autotune_plan(pb_plan* plan) {
+  if (!plan) return PB_ENULL;
+  pb_plan& P = *plan;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  tune_cache_load();
+  const int sms = sm_count();
+  // scratch large enough for any pass's source and destination
+  size_t big = std::max(layout_bytes(P, false), layout_bytes(P, true));
+  big = std::max(big, P.buf_bytes);
+  void* sa = nullptr;
+  void* sb = nullptr;
+  cuda_ok(cudaMalloc(&sa, big));
+  if (cudaMalloc(&sb, big) != cudaSuccess) {
+    cudaFree(sa);
+    fail(PB_ECUDA);
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = PB_OK;
+  if (cudaMemset(sa, 0, big) != cudaSuccess || cudaMemset(sb, 0, big) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    rc = PB_ECUDA;
+  for (int m = 0; m < M_COUNT && rc == PB_OK; ++m)
+    for (Step& st : P.prog[m].steps) {
+      if (st.type != 0 || !st.pa.fast) continue;
+      const std::string key = reg_key(st.pa, P.real_bytes);
+      if (g_tune_cache.count(key)) continue;
+      const int nsched = st.pa.fast == 2 ? std::max(1, mr_schedules(st.pa.m, P.real_bytes)) : 1;
+      float best = 1e30f;
+      int best_code = st.pa.sched * 1000 + std::max(1, st.pa.grid_ctas / sms);
+      for (int sc = 0; sc < nsched && rc == PB_OK; ++sc) {
+        const int occ = std::max(1, reg_occupancy(st.pa, P.real_bytes, sc));
+        for (int c = 1; c <= occ && rc == PB_OK; ++c) {
+          PassArgs A = st.pa;
+          A.in = sa;
+          A.out = sb;
+          A.gate = nullptr;
+          A.sched = sc;
+          A.grid_ctas = sms * c;
+          float ms = 0.f;
+          if (launch_pass(A, P.real_bytes, 0) != cudaSuccess || cudaEventRecord(e0, 0) != cudaSuccess) {
+            rc = PB_ECUDA;
+            break;
+          }
+          for (int r = 0; r < 3; ++r)
+            if (launch_pass(A, P.real_bytes, 0) != cudaSuccess) rc = PB_ECUDA;
+          if (rc != PB_OK || cudaEventRecord(e1, 0) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+              cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = PB_ECUDA;
+            break;
+          }
+          if (ms < best) {
+            best = ms;
+            best_code = sc * 1000 + c;
+          }
+        }
+      }
+      if (rc == PB_OK) g_tune_cache[key] = best_code;
+    }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(sa);
+  cudaFree(sb);
+  if (rc != PB_OK) return rc;
+  tune_cache_store();
+  apply_reg_tuning(P);
+  P.tuned = true;
+  return PB_OK;
+}
+
+static int pow2_radices(int m, int* r, int cap) {
+  int k = 0, n = 0;
+  while ((1 << k) < m) ++k;
+  if (k % 3 == 1 && n < cap) r[n++] = 2;
+  if (k % 3 == 2 && n < cap) r[n++] = 4;
+  for (int i = 0; i < k / 3 && n < cap; ++i) r[n++] = 8;
+  return n;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_plan_autotune(pb_plan* plan) {
+  return guard([&] { return autotune_plan(plan); });
+}
+
+int pb_plan_set_config(pb_plan* plan, int32_t sched, int32_t ctas_per_sm) {
+  return guard([&] {
+    if (!plan) return (int)PB_ENULL;
+    if (sched < -1 || sched > 1 || ctas_per_sm < 0) return (int)PB_EINVALID_ARGUMENT;
+    const int sms = sm_count();
+    for (int m = 0; m < M_COUNT; ++m)
+      for (Step& st : plan->prog[m].steps) {
+        if (st.type != 0 || !st.pa.fast) continue;
+        int sc = st.pa.sched;
+        if (sched >= 0 && st.pa.fast == 2) sc = sched < mr_schedules(st.pa.m, plan->real_bytes) ? sched : 0;
+        int c = ctas_per_sm;
+        if (c > 0) c = std::min(c, std::max(1, reg_occupancy(st.pa, plan->real_bytes, sc)));
+        else c = std::max(1, std::min(st.pa.grid_ctas / sms, reg_occupancy(st.pa, plan->real_bytes, sc)));
+        st.pa.sched = sc;
+        st.pa.grid_ctas = sms * c;
+      }
+    return (int)PB_OK;
+  });
+}
+
+int pb_plan_step_config(const pb_plan* plan, int32_t op, int32_t step, pb_step_config* out) {
+  return guard([&] {
+    if (!plan || !out) return (int)PB_ENULL;
+    const Program& prog = plan->prog[user_mode(*plan, op)];
+    if (step < 0 || step >= (int)prog.steps.size()) return (int)PB_EINVALID_ARGUMENT;
+    const Step& st = prog.steps[step];
+    std::memset(out, 0, sizeof(*out));
+    if (st.type != 0) {
+      out->kernel = 1;
+      return (int)PB_OK;
+    }
+    const PassArgs& A = st.pa;
+    const int sms = sm_count();
+    out->kernel = A.fast == 1 ? 2 : (A.fast == 2 || A.fast == 3) ? 3 : 0;
+    out->fft_len = A.m;
+    out->lines = A.lines;
+    out->grid_ctas = A.fast ? (int)std::min<long long>(A.grid_ctas, A.ntiles) : 0;
+    out->ctas_per_sm = A.fast ? std::max(1, A.grid_ctas / sms) : 0;
+    out->sched = A.sched;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      out->tuned = (A.fast && g_tune_cache.count(reg_key(A, plan->real_bytes))) ? 1 : 0;
+    }
+    if (A.fast == 2)
+      out->nradix = mr_radices(A.m, plan->real_bytes, A.sched, out->radix, 12);
+    else if (A.fast == 3)
+      out->nradix = mr_r2r_radices(A.m, plan->real_bytes, out->radix, 12);
+    else if (A.fast == 1)
+      out->nradix = pow2_radices(A.m, out->radix, 12);
+    else {
+      out->nradix = std::min(A.nstages, 12);
+      for (int i = 0; i < out->nradix; ++i) out->radix[i] = A.radix[i];
+    }
+    return (int)PB_OK;
+  });
+}
+
+}  // extern "C"
+

@@ -71,6 +71,12 @@ class PbSliceTransfer(C.Structure):
                 ("offset", C.c_int64), ("count", C.c_int64)]
 
 
+class PbStepConfig(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("fft_len", C.c_int32), ("lines", C.c_int32), ("grid_ctas", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("sched", C.c_int32), ("tuned", C.c_int32), ("nradix", C.c_int32),
+                ("radix", C.c_int32 * 12)]
+
+
 _P = C.c_void_p
 SIGNATURES = {
     "pb_version": ([], C.c_char_p),
@@ -93,6 +99,9 @@ SIGNATURES = {
     "pb_execute_no_alloc": ([_P, C.c_int32, _P, _P, _P], C.c_int),
     "pb_plan_steps": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "pb_plan_step_kernels": ([_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+    "pb_plan_autotune": ([_P], C.c_int),
+    "pb_plan_set_config": ([_P, C.c_int32, C.c_int32], C.c_int),
+    "pb_plan_step_config": ([_P, C.c_int32, C.c_int32, C.POINTER(PbStepConfig)], C.c_int),
     "pb_execute_status_async": ([_P, _P, _P, _P], C.c_int),
     "pb_execute_timed": ([_P, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_float), C.c_int32,
                           C.POINTER(C.c_int32)], C.c_int),

@@ -356,6 +356,31 @@ class _Plan:
     def backward_in_place(self, array, workspace=None, stream=None):
         self._in_place(L.BACKWARD, array, workspace, stream)
 
+    def autotune(self) -> None:
+        """Times the register kernels' candidate configurations (mixed-radix
+        schedule, CTAs per SM) for every pass and keeps the fastest; choices
+        are cached per pass shape (PB_TUNE_CACHE persists them)."""
+        L.check(L.load().pb_plan_autotune(self._h), "autotune")
+
+    def set_config(self, sched: int = -1, ctas_per_sm: int = 0) -> None:
+        """Pins the register kernels' schedule (0 / 1, -1 keeps) and CTAs per
+        SM (0 keeps) for every pass."""
+        L.check(L.load().pb_plan_set_config(self._h, int(sched), int(ctas_per_sm)), "set_config")
+
+    def step_configs(self, op) -> list:
+        """Per launch of `op`: kernel family, FFT length, lines per tile,
+        persistent grid, CTAs per SM, schedule, radices and whether the
+        autotuner chose it."""
+        names = ("generic", "check", "pow2", "mixed_radix")
+        out = []
+        for i in range(len(self.step_kinds(op))):
+            c = L.PbStepConfig()
+            L.check(L.load().pb_plan_step_config(self._h, op, i, C.byref(c)), "step config")
+            out.append({"kernel": names[c.kernel], "fft_len": c.fft_len, "lines": c.lines, "grid_ctas": c.grid_ctas,
+                        "ctas_per_sm": c.ctas_per_sm, "sched": c.sched, "tuned": bool(c.tuned),
+                        "radices": [c.radix[k] for k in range(c.nradix)]})
+        return out
+
     _forward_checks = False
     _reverse_checks = False
 
