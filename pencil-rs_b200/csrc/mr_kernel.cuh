@@ -740,7 +740,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
 // 2 contiguous lines, split direct store.  Kernels of their own, so that the
 // common one keeps its register allocation.
 template <typename R, int N, int V, int S = 0>
-__global__ void __launch_bounds__(MR_THREADS, 2) mr_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(MR_THREADS, mr_min_ctas((int)sizeof(R), N, S)) mr_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
   mr_run<R, N, false, V == 1, V != 0, S>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);

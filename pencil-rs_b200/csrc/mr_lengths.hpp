@@ -16,6 +16,31 @@ constexpr int kMrLengths[] = {35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  
                               245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375,
                               378, 384, 392, 400, 405, 420, 432, 441, 448, 450, 480, 486, 490, 500, 504};
 constexpr int kMrCount = sizeof(kMrLengths) / sizeof(kMrLengths[0]);
+
+// Resident CTAs per SM the kernels are compiled for (the register budget
+// 65536 / (256 threads x CTAs): 128 registers at 2, 80 at 3).  f32 lengths up
+// to 512 take 3: more warps hide the shared-memory and barrier latency that
+// bounds these kernels (a per-length sweep of 2^25-element C2C and R2C passes:
+// 0.82-0.95 of the 2-CTA time on most lengths; the real-to-real kinds
+// 0.70-0.90 on every length).  The exceptions below keep 2 with the default
+// schedule: their radix-16 and radix-15 stages spill at 80 registers and lost
+// (1.02-1.37x) in that sweep.  f64 and lengths above 512 keep 2.
+constexpr int kMrTwoCtaLengths[] = {45, 75, 81, 90, 135, 160, 168, 180, 192, 196, 210, 216, 224, 225, 240, 360};
+
+__host__ __device__ constexpr bool mr_two_cta_length(int N) {
+  for (int n : kMrTwoCtaLengths)
+    if (n == N) return true;
+  return false;
+}
+
+// CTAs per SM of the mixed-radix kernel for precision `real_bytes`, length N
+// and schedule S (1: radices up to 8, fewer registers per butterfly).
+__host__ __device__ constexpr int mr_min_ctas(int real_bytes, int N, int S) {
+  return (real_bytes != 4 || N > 512) ? 2 : (S == 1 ? 3 : (mr_two_cta_length(N) ? 2 : 3));
+}
+
+// The same for the real-to-real kinds (default schedule only).
+__host__ __device__ constexpr int mr_r2r_min_ctas(int real_bytes, int N) { return (real_bytes == 4 && N <= 512) ? 3 : 2; }
 constexpr int MR_GROUPS = 8;
 
 // Lengths whose passes the persistent batch kernel (pass_kernel.cu) runs with

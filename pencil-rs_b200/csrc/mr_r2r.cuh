@@ -359,7 +359,7 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
 }
 
 template <typename R, int N>
-__global__ void __launch_bounds__(MR_THREADS, 2) mr_r2r_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(MR_THREADS, mr_r2r_min_ctas((int)sizeof(R), N)) mr_r2r_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
   mr_run<R, N, true>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
