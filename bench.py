@@ -161,9 +161,11 @@ def reference_arm(args):
 def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids=64):
     """Ragged batch: 64 C2C f32 grids, each axis length drawn (seed 4) from the
     55 numbers 2^a 3^b 5^c 7^d in [32, 256], 16 grids (25%) with an extra dim
-    of 2, forward + inverse.  One graph-replayed persistent launch for the whole
-    batch against per-grid launches of the plain kernels (pb_execute per grid
-    and direction), at the same accuracy bound."""
+    of 2, forward + inverse.  One graph launch for the whole batch -- the
+    default branch mode (the plans' own kernels on 2 parallel graph branches)
+    and the persistent work-queue kernel -- against per-grid launches of the
+    plain kernels (pb_execute per grid and direction), at the same accuracy
+    bound."""
     from pencil_b200 import workloads
     work = workloads.ragged_batch(4)
     shapes = [s for s, _ in work][:ngrids]
@@ -203,6 +205,28 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids
 
     times = {}
     with torch.cuda.stream(stream):
+        # the persistent work-queue kernel first, then the default branch mode
+        batch.set_mode("queue")
+        qws = batch.allocate_workspace(dev)
+
+        def queued():
+            batch.execute([xs, mids, ends], qws, stream)
+
+        for _ in range(warmup):
+            queued()
+        stream.synchronize()
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(steps):
+            queued()
+        q1.record(stream)
+        stream.synchronize()
+        times["queue"] = pbd.max_over_ranks(q0.elapsed_time(q1) / steps)
+        batch.status(qws, stream)
+        del qws
+        batch.set_mode("branches", 2)
+        bws = batch.allocate_workspace(dev)
         for name, fn in (("batch", batched), ("per_grid", per_grid)):
             for _ in range(warmup):
                 fn()
@@ -230,7 +254,10 @@ def batch_section(pb, L, torch, dev, steps=10, warmup=3, rank=0, world=1, ngrids
     nbytes = pbd.sum_over_ranks(nbytes)
     rt_b, rt_p, diff = (pbd.max_over_ranks(v) for v in (rt_b, rt_p, diff))
     return {"grids": len(shapes), "grids_per_gpu": len(mine), "with_extra": len(with_extra & set(range(len(shapes)))), "ms_batch_graph": times["batch"], "ms_per_grid_launches": times["per_grid"],
-            "speedup": times["per_grid"] / times["batch"], "gbs_batch": nbytes / (times["batch"] * 1e-3) / 1e9,
+            "batch_mode": "branches: one graph of the plans' own pass kernels on 2 parallel branches",
+            "ms_batch_queue_kernel": times["queue"],
+            "speedup": times["per_grid"] / times["batch"], "speedup_queue_kernel": times["per_grid"] / times["queue"],
+            "gbs_batch": nbytes / (times["batch"] * 1e-3) / 1e9,
             "launches_batch": 1,
             "launches_per_grid": int(pbd.sum_over_ranks(sum(p.info.passes_forward + p.info.passes_inverse for p in plans))),
             "roundtrip_rel_l2_batch": rt_b, "roundtrip_rel_l2_per_grid": rt_p, "batch_vs_per_grid_rel_l2": diff,

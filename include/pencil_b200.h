@@ -417,20 +417,33 @@ int pb_pointwise(int32_t op, int32_t scalar, const pb_pencil_desc* pencil, int32
 /* The collections API (crates/pencil-fft/src/distributed/collections.rs:1-17)
  * runs forward_many as a sequential loop over arrays of ONE plan.  A batch here
  * holds any number of plans of one precision (different shapes, extras and
- * layouts) and an operation chain (e.g. FORWARD then INVERSE); one execution is
- * ONE persistent kernel launch over a level-ordered (plan, pass, tile) work
- * queue, replayed from a CUDA graph on a non-default stream.  Tile heights are
- * chosen by an autotuner that caches its choice per pass shape (process-wide;
- * persisted in the file named by PB_TUNE_CACHE when set).  Plans whose chain
- * needs the C2R spectrum check are not accepted (PB_EUNSUPPORTED). */
+ * layouts) and an operation chain (e.g. FORWARD then INVERSE).  One execution
+ * is one CUDA graph launch on a non-default stream, in one of two modes:
+ *  - PB_BATCH_QUEUE: ONE persistent kernel over a level-ordered (plan, pass,
+ *    tile) work queue with bounded dependency waits; tile heights chosen by an
+ *    autotuner that caches its choice per pass shape;
+ *  - PB_BATCH_BRANCHES (the default, 2 branches): the member plans' own pass
+ *    kernels, the plans split over parallel graph branches balanced by bytes
+ *    (largest first), each plan's chain in order on its branch.
+ * With `autotune` set, creation also tunes the member plans' register passes
+ * (pb_plan_autotune; the choices are cached per pass shape, persisted in the
+ * file named by PB_TUNE_CACHE when set).  Plans whose chain needs the C2R
+ * spectrum check are not accepted (PB_EUNSUPPORTED). */
+#define PB_BATCH_QUEUE 0
+#define PB_BATCH_BRANCHES 1
 int pb_batch_create(pb_plan* const* plans, int32_t count, const int32_t* ops, int32_t nops, int32_t autotune,
                     pb_batch** batch);
+/* Selects the execution mode and, for PB_BATCH_BRANCHES, the number of
+ * parallel branches (1..16); the next execution re-captures its graph.  The
+ * workspace size (pb_batch_workspace_bytes) depends on the mode: query it
+ * again after a change. */
+int pb_batch_set_mode(pb_batch* batch, int32_t mode, int32_t branches);
 int pb_batch_workspace_bytes(const pb_batch* batch, int64_t* bytes);
 /* buffers: (nops + 1) * count device pointers; buffers[k*count + i] is plan i's
  * input of op k (k < nops) and its output of op k-1 (k > 0). */
 int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, void* stream);
 /* Waits for `stream`; PB_ETIMEOUT if a bounded dependency wait in the last
- * execution gave up (its tiles were skipped), else PB_OK. */
+ * execution gave up (its tiles were skipped; queue mode only), else PB_OK. */
 int pb_batch_status(pb_batch* batch, void* workspace, void* stream);
 /* Bound of each dependency wait inside the batch kernel, in steps of about
  * 100 ns (default 2^24, about 1.7 s).  A wait that runs out sets the batch's

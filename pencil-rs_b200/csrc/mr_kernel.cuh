@@ -226,8 +226,9 @@ __device__ __forceinline__ void mr_fill_twiddles(typename Cx<R>::T* Wst, const t
 
 // Loads the stage-0 butterfly inputs of one tile into registers: butterfly b
 // (sequence b / NB0, index jb) takes elements jb + r*NB0 of its sequence.
-// SX, strided lines (C2C, R2C): item b is butterfly b / NSEQ of sequence
-// b % NSEQ, so the lanes read adjacent lines at each position of the axis.
+// SX, strided lines (C2C, R2C, C2R): item b is butterfly b / NSEQ of
+// sequence b % NSEQ, so the lanes read adjacent lines at each position of the
+// axis (element q of a line at q * srcq).
 template <typename R, int N, bool SX = false, int S = 0>
 __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N, S>::U0][MRGeom<R, N, S>::R0], const PassArgs& A,
                                         const TileAddr& ta) {
@@ -284,8 +285,9 @@ __device__ __forceinline__ void mr_load(typename Cx<R>::T (&v)[MRGeom<R, N, S>::
         const int q = jb + r * NB;
         const bool mirror = 2 * q > N;
         const int hq = mirror ? N - q : q;
-        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
-        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
+        const long long e = SX ? (long long)hq * ta.srcq : (long long)hq;
+        C X = ok0 ? in[b0 + e] : mk<C, R>(zero, zero);
+        C Y = ok1 ? in[b1 + e] : mk<C, R>(zero, zero);
         const bool edge = (hq == 0) || (2 * hq == N);
         if (mirror) {
           X.y = -X.y;
@@ -648,10 +650,10 @@ __device__ __forceinline__ void mr_tile(const PassArgs& A, const TileAddr& ta,
 // chunk belonged to the same pass).  Ends with this CTA's last store still
 // reading shared memory: the caller places a barrier before reusing it.
 // the real-to-real kinds (mr_r2r.cuh)
-template <typename R, int N>
+template <typename R, int N, bool SX>
 __device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                             const PassArgs& A, const TileAddr& ta);
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, bool SX>
 __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& ta,
                                             typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                             typename Cx<R>::T* b0, typename Cx<R>::T* b1,
@@ -689,7 +691,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   TileAddr ta = load_tile(tiles, tile);
   C v[G::U0][G::R0];
   if constexpr (R2R)
-    mr_load_r2r<R, N>(v, A, ta);
+    mr_load_r2r<R, N, SX>(v, A, ta);
   else
     mr_load<R, N, SX, S>(v, A, ta);
   TileAddr t1 = ta;
@@ -705,7 +707,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
     C nv[G::U0][G::R0];
     if (has_next) {
       if constexpr (R2R)
-        mr_load_r2r<R, N>(nv, A, t1);
+        mr_load_r2r<R, N, SX>(nv, A, t1);
       else
         mr_load<R, N, SX, S>(nv, A, t1);
       if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
@@ -713,9 +715,9 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
     }
     if constexpr (R2R) {
       if (A.inv)
-        mr_tile_r2r<R, N, true>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile_r2r<R, N, true, SX>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
       else
-        mr_tile_r2r<R, N, false>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+        mr_tile_r2r<R, N, false, SX>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     } else {
       if (A.inv)
         mr_tile<R, N, true, SX, DS, S>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);

@@ -8,7 +8,11 @@
 // (crates/pencil-fft/src/r2r.rs:697-848) and the Hartley transform
 // (dht.rs:201-353), computed as in the generic pass kernel: the
 // pre-processing runs in the register-fed stage-0 load, the post-processing in
-// the store.
+// the store.  SX (strided lines, permute_dims = false): the tile's lines are
+// adjacent along the source's innermost axis, element q of a line at
+// q * srcq; the lanes of a warp then take adjacent sequences at each position
+// (item b is butterfly b / NSEQ of sequence b % NSEQ) so that they read
+// adjacent lines.
 #pragma once
 
 #include "mr_kernel.cuh"
@@ -17,22 +21,23 @@ namespace pb {
 
 // Element idx of the tile's pair s: lines (2s, 2s+1) of real data as (x, y),
 // or complex line s; the adjoint pre-weight of idx applied.
-template <typename R>
+template <typename R, bool SX = false>
 struct R2rSource {
   using C = typename Cx<R>::T;
   const R* inr;
   const C* inc;
-  long long b0, b1;
+  long long b0, b1, q;
   bool ok0, ok1, cplx;
   int n, pre_mode;
   R pre_f;
   __device__ __forceinline__ C get(int idx) const {
     const R zero = R(0);
+    const long long e = SX ? (long long)idx * q : (long long)idx;
     C z;
     if (cplx)
-      z = ok0 ? inc[b0 + idx] : mk<C, R>(zero, zero);
+      z = ok0 ? inc[b0 + e] : mk<C, R>(zero, zero);
     else
-      z = mk<C, R>(ok0 ? inr[b0 + idx] : zero, ok1 ? inr[b1 + idx] : zero);
+      z = mk<C, R>(ok0 ? inr[b0 + e] : zero, ok1 ? inr[b1 + e] : zero);
     if (pre_mode != W_NONE && weight_hit(pre_mode, idx, n)) z = scl(z, pre_f);
     return z;
   }
@@ -53,7 +58,7 @@ __host__ __device__ constexpr int r2r_len() {
 // complex line) is two FFT sequences, 2p + c for line / component c of pair p.
 // Input q of a sequence is (x[2q] + i x[n-1-2q]) * exp(-i pi (4q+1) / (4n))
 // (aux0), with the input reversed for DST-IV (x[n-1-j]).
-template <typename R, int N, int SUB>
+template <typename R, int N, int SUB, bool SX>
 __device__ __forceinline__ void mr_load_r2r_iv(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                                const PassArgs& A, const TileAddr& ta) {
   using C = typename Cx<R>::T;
@@ -70,15 +75,15 @@ __device__ __forceinline__ void mr_load_r2r_iv(typename Cx<R>::T (&v)[MRGeom<R, 
 #pragma unroll
   for (int u = 0; u < G::U0; ++u) {
     const int b = threadIdx.x + u * MR_THREADS;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = SX ? b % G::NSEQ : b / NB;
+    const int jb = SX ? b / G::NSEQ : b - s * NB;
     const int p = s >> 1, c = s & 1;
     const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
     // element j of this sequence's real line: real data line 2p + c, complex
     // data component c of line p (interleaved (re, im) in units of R)
     const bool ok = live && (cplx ? p < L : 2 * p + c < L);
     const long long base = cplx ? 2 * (ta.src0 + (long long)p * ta.srcb) + c : ta.src0 + (long long)(2 * p + c) * ta.srcb;
-    const int step = cplx ? 2 : 1;
+    const long long step = (cplx ? 2 : 1) * (SX ? (long long)ta.srcq : 1LL);
 #pragma unroll
     for (int r = 0; r < R0; ++r) {
       const int q = jb + r * NB;
@@ -87,8 +92,8 @@ __device__ __forceinline__ void mr_load_r2r_iv(typename Cx<R>::T (&v)[MRGeom<R, 
         j0 = n - 1 - j0;
         j1 = n - 1 - j1;
       }
-      R x0 = ok ? inr[base + (long long)j0 * step] : zero;
-      R x1 = ok ? inr[base + (long long)j1 * step] : zero;
+      R x0 = ok ? inr[base + j0 * step] : zero;
+      R x1 = ok ? inr[base + j1 * step] : zero;
       if (A.pre_mode != W_NONE) {
         if (weight_hit(A.pre_mode, j0, n)) x0 *= pf;
         if (weight_hit(A.pre_mode, j1, n)) x1 *= pf;
@@ -101,7 +106,7 @@ __device__ __forceinline__ void mr_load_r2r_iv(typename Cx<R>::T (&v)[MRGeom<R, 
 // Stage-0 butterfly inputs of one tile (FFT input q of each pair), for the
 // kind SUB (a template parameter, so every index below is compile-time but
 // the butterfly index).
-template <typename R, int N, int SUB>
+template <typename R, int N, int SUB, bool SX>
 __device__ __forceinline__ void mr_load_r2r_k(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                               const PassArgs& A, const TileAddr& ta) {
   using C = typename Cx<R>::T;
@@ -116,10 +121,11 @@ __device__ __forceinline__ void mr_load_r2r_k(typename Cx<R>::T (&v)[MRGeom<R, N
 #pragma unroll
   for (int u = 0; u < G::U0; ++u) {
     const int b = threadIdx.x + u * MR_THREADS;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = SX ? b % G::NSEQ : b / NB;
+    const int jb = SX ? b / G::NSEQ : b - s * NB;
     const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
-    R2rSource<R> src;
+    R2rSource<R, SX> src;
+    src.q = ta.srcq;
     src.cplx = A.in_complex != 0;
     src.inr = reinterpret_cast<const R*>(A.in);
     src.inc = reinterpret_cast<const C*>(A.in);
@@ -175,23 +181,23 @@ __device__ __forceinline__ void mr_load_r2r_k(typename Cx<R>::T (&v)[MRGeom<R, N
   }
 }
 
-template <typename R, int N>
+template <typename R, int N, bool SX>
 __device__ __forceinline__ void mr_load_r2r(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                             const PassArgs& A, const TileAddr& ta) {
   switch (A.sub) {
-    case S_DCT2: mr_load_r2r_k<R, N, S_DCT2>(v, A, ta); break;
-    case S_DST2: mr_load_r2r_k<R, N, S_DST2>(v, A, ta); break;
-    case S_DCT3: mr_load_r2r_k<R, N, S_DCT3>(v, A, ta); break;
-    case S_DST3: mr_load_r2r_k<R, N, S_DST3>(v, A, ta); break;
+    case S_DCT2: mr_load_r2r_k<R, N, S_DCT2, SX>(v, A, ta); break;
+    case S_DST2: mr_load_r2r_k<R, N, S_DST2, SX>(v, A, ta); break;
+    case S_DCT3: mr_load_r2r_k<R, N, S_DCT3, SX>(v, A, ta); break;
+    case S_DST3: mr_load_r2r_k<R, N, S_DST3, SX>(v, A, ta); break;
     case S_DCT1:
-      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DCT1>(v, A, ta);
+      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DCT1, SX>(v, A, ta);
       break;
     case S_DST1:
-      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DST1>(v, A, ta);
+      if constexpr (N % 2 == 0) mr_load_r2r_k<R, N, S_DST1, SX>(v, A, ta);
       break;
-    case S_DCT4: mr_load_r2r_iv<R, N, S_DCT4>(v, A, ta); break;
-    case S_DST4: mr_load_r2r_iv<R, N, S_DST4>(v, A, ta); break;
-    default: mr_load_r2r_k<R, N, S_DHT>(v, A, ta); break;
+    case S_DCT4: mr_load_r2r_iv<R, N, S_DCT4, SX>(v, A, ta); break;
+    case S_DST4: mr_load_r2r_iv<R, N, S_DST4, SX>(v, A, ta); break;
+    default: mr_load_r2r_k<R, N, S_DHT, SX>(v, A, ta); break;
   }
 }
 
@@ -336,7 +342,7 @@ __device__ __forceinline__ void mr_store_r2r(const PassArgs& A, const TileAddr& 
 }
 
 // Transform and store of one tile whose stage-0 inputs are in `v`.
-template <typename R, int N, bool INV>
+template <typename R, int N, bool INV, bool SX>
 __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& ta,
                                             typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                             typename Cx<R>::T* b0, typename Cx<R>::T* b1,
@@ -344,7 +350,7 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
                                             PieceAddr* prow, const PieceAddr& my_piece, int npieces) {
   using G = MRGeom<R, N>;
   const int tid = threadIdx.x;
-  mr_stage0<R, N, INV>(v, b0);
+  mr_stage0<R, N, INV, SX>(v, b0);
   if (tid < npieces) prow[tid] = my_piece;
   __syncthreads();
   if (!A.dst_k_contig) {
@@ -358,34 +364,38 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
   mr_store_r2r<R, N>(A, ta, ((G::NST - 1) % 2 == 0) ? b0 : b1, Atab);
 }
 
-template <typename R, int N>
+// V = 0: lines contiguous in the source; 1: strided lines (SX).
+template <typename R, int N, int V>
 __global__ void __launch_bounds__(MR_THREADS, mr_r2r_min_ctas((int)sizeof(R), N)) mr_r2r_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
-  mr_run<R, N, true>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
+  mr_run<R, N, true, V == 1>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
 }
 
 template <typename R, int N>
 cudaError_t mr_r2r_launch(const PassArgs& A, cudaStream_t stream) {
   constexpr size_t smem = mr_smem_bytes<R, N, true>();
-  cudaError_t err = cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const auto kern = A.src_k_contig == 0 ? mr_r2r_kernel<R, N, 1> : mr_r2r_kernel<R, N, 0>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
   if (grid > A.ntiles) grid = A.ntiles;
-  mr_r2r_kernel<R, N><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
+  kern<<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
   return cudaGetLastError();
 }
 
+// resident CTAs per SM, the smaller of the two variants' figures
 template <typename R, int N>
 int mr_r2r_occupancy(int /*sched: the real-to-real kinds run the default schedule*/) {
   constexpr size_t smem = mr_smem_bytes<R, N, true>();
-  int blocks = 0;
-  if (cudaFuncSetAttribute(mr_r2r_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
-    return 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_r2r_kernel<R, N>, MR_THREADS, smem) != cudaSuccess)
-    return 1;
-  return blocks > 0 ? blocks : 1;
+  int best = 0;
+  for (const auto kern : {mr_r2r_kernel<R, N, 0>, mr_r2r_kernel<R, N, 1>}) {
+    int blocks = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, MR_THREADS, smem) != cudaSuccess) return 1;
+    best = best == 0 ? blocks : std::min(best, blocks);
+  }
+  return best > 0 ? best : 1;
 }
 
 template <typename R, int N>

@@ -1073,7 +1073,8 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   // the source's innermost axis, which the register kernel loads across lines
   // (the tile axis may be split in either layout: the chunks are cut at both
   // partitions of it, and the row tables are built per tile)
-  const bool src_strided = (op.kind == P_C2C || op.kind == P_R2C) && src.perm[N - 1] == b && b != a;
+  const bool src_strided =
+      (op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && src.perm[N - 1] == b && b != a;
   if ((op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && pow2 &&
       (src.perm[N - 1] == a || src_strided) && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
@@ -1086,7 +1087,7 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
     if (direct || transposed || dsplit) {
       A.fast = 1;
       A.dst_k_contig = direct ? 1 : (dsplit ? 2 : 0);
-      if (pow2_half_supported(A.m / 2, op.kind, direct ? 1 : 0, P.real_bytes)) {
+      if (!src_strided && pow2_half_supported(A.m / 2, op.kind, direct ? 1 : 0, P.real_bytes)) {
         // one real output line as an m/2-point complex sequence: 8-byte
         // stores of the real lines, split twiddles W_N^c for c <= m/16
         A.half = 1;
@@ -1116,14 +1117,16 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.lines = L;
     }
   }
-  // real-to-real kinds on the mixed-radix kernel (all but the type-IV kinds):
-  // the same layout conditions, FFT lengths of kMrR2rLengths
+  // real-to-real kinds on the mixed-radix kernel (the type-IV kinds for even
+  // n): contiguous or strided source lines, a direct or transposed store, FFT
+  // lengths of kMrR2rLengths
   const bool iv4 = op.sub == S_DCT4 || op.sub == S_DST4;
+  const bool r2r_strided = src.perm[N - 1] == b && b != a;
   if (!A.fast && !P.force_generic && op.kind == P_R2R && (!iv4 || A.n % 2 == 0) &&
-      mr_r2r_supported(A.m, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+      mr_r2r_supported(A.m, P.real_bytes) && (src.perm[N - 1] == a || r2r_strided) && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
-    const bool transposed = !direct && dst.perm[N - 1] == b && dst.split_of(b) < 0 && (ta < 0 || dst.grid[ta] <= 64);
+    const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
     if (direct || transposed) {
       A.fast = 3;
       A.dst_k_contig = direct ? 1 : 0;
@@ -3036,12 +3039,25 @@ struct pb_batch {
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   long long spin_limit = 1LL << 24;  // __nanosleep(100) steps of a dependency wait (about 1.7 s)
+  // branch mode: the member plans' own pass kernels, captured into one graph
+  // as `branches` parallel chains of plans (each plan's op chain in order)
+  int mode = PB_BATCH_BRANCHES;
+  int branches = 2;
+  std::vector<int> ops;
+  std::vector<long long> weight;    // elements moved by each plan's op chain
+  std::vector<int> branch_of;       // plan -> branch
+  std::vector<size_t> branch_off;   // workspace offset of each branch
+  size_t branch_bytes = 0;          // workspace of all branches
+  std::vector<cudaStream_t> bstreams;
+  std::vector<cudaEvent_t> bevents;  // [0] the fork, [1 + b] branch b's join
   ~pb_batch() {
     if (graph) cudaGraphExecDestroy(graph);
     if (d_descs) cudaFree(d_descs);
     if (d_item_start) cudaFree(d_item_start);
     if (d_dep) cudaFree(d_dep);
     if (h_descs) cudaFreeHost(h_descs);
+    for (cudaStream_t st : bstreams) cudaStreamDestroy(st);
+    for (cudaEvent_t e : bevents) cudaEventDestroy(e);
   }
 };
 
@@ -3167,6 +3183,34 @@ static void autotune_pass(pb_plan& T, const pb_plan& plan, int mode, int step, v
 }
 
 static int user_mode_batch(const pb_plan& P, int op) { return user_mode(P, op); }
+
+static int autotune_plan(pb_plan* plan);  // the register-kernel autotuner (end of file)
+
+// Branch mode: plans to branches, largest first onto the least loaded
+// branch (by elements moved), and each branch's workspace slice, sized for
+// the largest member plan (a branch runs its plans one after another).
+static void batch_assign_branches(pb_batch& B) {
+  const int nb = std::max(1, std::min(B.branches, B.count));
+  std::vector<int> order(B.count);
+  for (int i = 0; i < B.count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B.weight[a] > B.weight[b]; });
+  std::vector<long long> load(nb, 0);
+  std::vector<size_t> need(nb, 0);
+  B.branch_of.assign(B.count, 0);
+  for (int i : order) {
+    const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    B.branch_of[i] = b;
+    load[b] += B.weight[i];
+    need[b] = std::max(need[b], (size_t)B.plans[i]->ws_bytes);
+  }
+  B.branch_off.assign(nb, 0);
+  size_t off = 0;
+  for (int b = 0; b < nb; ++b) {
+    B.branch_off[b] = off;
+    off += (need[b] + 255) & ~size_t(255);
+  }
+  B.branch_bytes = off;
+}
 
 static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, int nops, int autotune) {
   if (!plans || !ops || count <= 0 || nops <= 0) fail(PB_EINVALID_ARGUMENT);
@@ -3309,6 +3353,22 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
   if (nd) cuda_ok(cudaMemcpy(B->d_dep, B->dep.data(), nd * sizeof(int), cudaMemcpyHostToDevice));
   cuda_ok(cudaMallocHost(reinterpret_cast<void**>(&B->h_descs), std::max<size_t>(nd, 1) * sizeof(PassArgs)));
   B->grid = sms * batch_occupancy(B->real_bytes, B->smem);
+
+  // branch mode: the op chain and the bytes each plan moves through it
+  B->ops.assign(ops, ops + nops);
+  for (int i = 0; i < count; ++i) {
+    const pb_plan& p = *B->plans[i];
+    long long w = 0;
+    for (int k = 0; k < nops; ++k)
+      w += (long long)p.prog[user_mode(p, ops[k])].steps.size() * (p.fin.total(p.extra) + p.fout.total(p.extra));
+    B->weight.push_back(w);
+  }
+  batch_assign_branches(*B);
+  if (autotune)
+    for (pb_plan* p : B->plans) {
+      const int rc = autotune_plan(p);
+      if (rc != PB_OK) fail(rc);
+    }
   return B.release();
 }
 
@@ -3318,8 +3378,81 @@ static void* batch_slot(const pb_batch& B, int plan, int slot, void* const* buff
   return buffers[(size_t)set * B.count + plan];
 }
 
+// Plan i's op chain on stream `st` with the branch's workspace slice.
+static void batch_run_plan(pb_batch& B, int i, void* const* buffers, void* ws, cudaStream_t st) {
+  void* bws = static_cast<unsigned char*>(ws) + B.branch_off[B.branch_of[i]];
+  for (int k = 0; k < B.nops; ++k) {
+    const void* in = buffers[(size_t)k * B.count + i];
+    void* out = buffers[(size_t)(k + 1) * B.count + i];
+    const int rc = run(B.plans[i], B.ops[k], in, out, bws, st, nullptr, 0, nullptr);
+    if (rc != PB_OK) fail(rc);
+  }
+}
+
+// Branch mode: one graph whose branches each run a share of the plans with
+// their own pass kernels; forked from and joined back into `s`.
+static int batch_execute_branches(pb_batch* B, void* const* buffers, void* ws, cudaStream_t s) {
+  const int nb = (int)B->branch_off.size();
+  if (reinterpret_cast<uintptr_t>(ws) % 256 != 0) fail(PB_EINVALID_ARGUMENT);
+  if (s == nullptr) {  // the legacy stream cannot be captured: the plans in order
+    for (int i = 0; i < B->count; ++i) batch_run_plan(*B, i, buffers, ws, s);
+    return PB_OK;
+  }
+  std::vector<const void*> now((size_t)(B->nops + 1) * B->count + 1);
+  for (size_t i = 0; i + 1 < now.size(); ++i) now[i] = buffers[i];
+  now.back() = ws;
+  if (now != B->bound || !B->graph || B->graph_stream != s) {
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    B->bound.clear();
+    for (int b = (int)B->bstreams.size(); b < nb; ++b) {
+      cudaStream_t st;
+      cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      B->bstreams.push_back(st);
+    }
+    while ((int)B->bevents.size() < nb + 1) {
+      cudaEvent_t e;
+      cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      B->bevents.push_back(e);
+    }
+    cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int forked = 0;
+    int rc = PB_OK;
+    try {
+      cuda_ok(cudaEventRecord(B->bevents[0], s));
+      for (int b = 0; b < nb; ++b) {
+        cuda_ok(cudaStreamWaitEvent(B->bstreams[b], B->bevents[0], 0));
+        ++forked;
+        for (int i = 0; i < B->count; ++i)
+          if (B->branch_of[i] == b) batch_run_plan(*B, i, buffers, ws, B->bstreams[b]);
+      }
+    } catch (const PbError& e) {
+      rc = e.code;
+    }
+    // join every forked branch, also after an error, so that the capture ends cleanly
+    for (int b = 0; b < forked; ++b) {
+      cudaEventRecord(B->bevents[1 + b], B->bstreams[b]);
+      cudaStreamWaitEvent(s, B->bevents[1 + b], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (rc == PB_OK && ec != cudaSuccess) rc = PB_ECUDA;
+    if (rc == PB_OK && cudaGraphInstantiate(&B->graph, g, 0) != cudaSuccess) {
+      B->graph = nullptr;
+      rc = PB_ECUDA;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (rc != PB_OK) fail(rc);
+    B->graph_stream = s;
+    B->bound = now;
+  }
+  cuda_ok(cudaGraphLaunch(B->graph, s));
+  return PB_OK;
+}
+
 static int batch_execute(pb_batch* B, void* const* buffers, void* ws, cudaStream_t s) {
   if (!buffers || !ws) fail(PB_ENULL);
+  if (B->mode == PB_BATCH_BRANCHES) return batch_execute_branches(B, buffers, ws, s);
   std::vector<const void*> now((size_t)(B->nops + 1) * B->count + 1);
   for (size_t i = 0; i + 1 < now.size(); ++i) now[i] = buffers[i];
   now.back() = ws;
@@ -3394,8 +3527,26 @@ int pb_batch_create(pb_plan* const* plans, int32_t count, const int32_t* ops, in
 
 int pb_batch_workspace_bytes(const pb_batch* batch, int64_t* bytes) {
   if (!batch || !bytes) return PB_ENULL;
-  *bytes = (int64_t)batch->ws_bytes;
+  *bytes = (int64_t)std::max(batch->ws_bytes, batch->branch_bytes);
   return PB_OK;
+}
+
+int pb_batch_set_mode(pb_batch* batch, int32_t mode, int32_t branches) {
+  return guard([&] {
+    if (!batch) return (int)PB_ENULL;
+    if ((mode != PB_BATCH_QUEUE && mode != PB_BATCH_BRANCHES) || (mode == PB_BATCH_BRANCHES && (branches < 1 || branches > 16)))
+      return (int)PB_EINVALID_ARGUMENT;
+    batch->mode = mode;
+    if (mode == PB_BATCH_BRANCHES) {
+      batch->branches = branches;
+      batch_assign_branches(*batch);
+    }
+    // the next execution captures (and, in queue mode, uploads its descriptors) again
+    if (batch->graph) cudaGraphExecDestroy(batch->graph);
+    batch->graph = nullptr;
+    batch->bound.clear();
+    return (int)PB_OK;
+  });
 }
 
 int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, void* stream) {
@@ -3408,6 +3559,10 @@ int pb_batch_execute(pb_batch* batch, void* const* buffers, void* workspace, voi
 int pb_batch_status(pb_batch* batch, void* workspace, void* stream) {
   return guard([&] {
     if (!batch || !workspace) return (int)PB_ENULL;
+    if (batch->mode == PB_BATCH_BRANCHES) {  // no device waits in branch mode
+      cuda_ok(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+      return (int)PB_OK;
+    }
     int err = 0;
     cuda_ok(cudaMemcpyAsync(&err, static_cast<unsigned char*>(workspace) + batch->ctrl_off + 8, sizeof(int),
                             cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));

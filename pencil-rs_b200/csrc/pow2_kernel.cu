@@ -132,7 +132,7 @@ __device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const Pas
     // slot/t are g and b: sequences LPT*g + i, inputs b + T*m along the
     // strided axis (stride srcq), adjacent lines srcb apart
     const int g = slot, b = t;
-    if constexpr (LPT == 2 && sizeof(R) == 4) {
+    if constexpr (LPT == 2 && sizeof(R) == 4 && KIND != P_C2R) {
       // f32, two sequences per thread: its adjacent lines (C2C 2g, 2g+1; R2C
       // 4g .. 4g+3) are 16 contiguous bytes at each position, one vector load
       // where aligned
@@ -172,10 +172,29 @@ __device__ __forceinline__ void p2_fetch(P2Raw<R, KIND, LPT, FH>& raw, const Pas
         if constexpr (KIND == P_C2C) {
           const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
           raw.a[i][m] = sq < L ? in[ta.src0 + (long long)sq * ta.srcb + q] : z;
-        } else {  // P_R2C: lines 2sq and 2sq + 1 packed as x + iy
+        } else if constexpr (KIND == P_R2C) {  // lines 2sq and 2sq + 1 packed as x + iy
           const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
           const long long o = ta.src0 + (long long)(2 * sq) * ta.srcb + q;
           raw.a[i][m] = mk<C, R>(2 * sq < L ? in[o] : zero, 2 * sq + 1 < L ? in[o + ta.srcb] : zero);
+        } else {  // P_C2R: the Hermitian extensions of half spectra 2sq, 2sq + 1 as X + iY
+          const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
+          const int pq = b + T * m;
+          const bool mirror = pq > N / 2;
+          const int hq = mirror ? N - pq : pq;
+          const long long o = ta.src0 + (long long)(2 * sq) * ta.srcb + (long long)hq * ta.srcq;
+          C X = 2 * sq < L ? in[o] : z;
+          C Y = 2 * sq + 1 < L ? in[o + ta.srcb] : z;
+          const bool edge = (hq == 0) || (hq == N / 2);
+          if (mirror) {
+            X.y = -X.y;
+            Y.y = -Y.y;
+          }
+          if (edge) {
+            X.y = zero;
+            Y.y = zero;
+          }
+          const R w = (A.pre_mode == W_HALF_INTERIOR && !edge) ? R(A.pre_factor) : R(1);
+          raw.a[i][m] = mk<C, R>((X.x - Y.y) * w, (X.y + Y.x) * w);
         }
       }
     }
@@ -358,7 +377,7 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   constexpr int NOUT = (KIND == P_R2C) ? H : N;
   constexpr int NST = S::NST;
   constexpr int LAST = MD::LAST;
-  constexpr bool FH = MD::FIRST_H;
+  constexpr bool FH = MD::FIRST_H && !SX;  // strided C2R lines take the across-lines first stage
   constexpr bool DLIKE = DIRECT || DSPLIT;  // line-major outputs, coalesced along k
   constexpr bool SMEM_STORE = !(DLIKE && KIND != P_R2C) && LAST == P2_LAST_NAT;
   static_assert(!DSPLIT || (!DIRECT && KIND != P_C2R), "split direct stores: C2C and R2C");
@@ -378,7 +397,6 @@ __global__ void __launch_bounds__(P2_THREADS, 2) pow2_kernel(const PassArgs A) {
   const int slot = tid / T;
   const int t = tid - slot * T;
   // first stage (SX: g = tid % SLOTS, b = tid / SLOTS)
-  static_assert(!(SX && FH), "strided C2R lines take the generic kernel");
   const int fs = FH ? tid / (T / 2) : (SX ? tid % SLOTS : slot);
   const int fc = FH ? tid % (T / 2) : (SX ? tid / SLOTS : t);
   // last stage
@@ -948,10 +966,9 @@ static size_t p2_smem(int kind) {
 template <typename R, int N, int KIND, bool INV, bool DIRECT, bool DSPLIT = false>
 static cudaError_t p2_launch(const PassArgs& A, cudaStream_t stream) {
   const size_t smem = p2_smem<R, N>(KIND);
-  // strided source lines: C2C and R2C only (C2R lines are planned contiguous)
-  constexpr bool SXOK = KIND != P_C2R;
-  auto fn = (SXOK && A.src_k_contig == 0) ? pow2_kernel<R, N, KIND, INV, DIRECT, SXOK, DSPLIT>
-                                          : pow2_kernel<R, N, KIND, INV, DIRECT, false, DSPLIT>;
+  // strided source lines (the tile's lines adjacent along the source's innermost axis)
+  auto fn = A.src_k_contig == 0 ? pow2_kernel<R, N, KIND, INV, DIRECT, true, DSPLIT>
+                                : pow2_kernel<R, N, KIND, INV, DIRECT, false, DSPLIT>;
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;

@@ -129,6 +129,7 @@ SIGNATURES = {
     "pb_batch_execute": ([_P, C.POINTER(_P), _P, _P], C.c_int),
     "pb_batch_status": ([_P, _P, _P], C.c_int),
     "pb_batch_set_wait_limit": ([_P, C.c_int64], C.c_int),
+    "pb_batch_set_mode": ([_P, C.c_int32, C.c_int32], C.c_int),
     "pb_batch_destroy": ([_P], C.c_int),
     "pb_transpose_create_alltoallv": ([C.POINTER(PbPencilDesc), C.POINTER(PbPencilDesc), C.c_int64, C.c_int32,
                                        C.POINTER(_P)], C.c_int),

@@ -665,18 +665,26 @@ class SpatialRemapPlan:
 
 
 class PlanBatch:
-    """A ragged batch of plans run as ONE persistent launch per execution.
+    """A ragged batch of plans run as one CUDA graph launch per execution.
 
     The reference's collections (``forward_many``, collections.rs) loop over
     arrays of one plan; here every plan may differ (shape, extra dims,
     layout), and an operation chain such as ``("forward", "inverse")`` runs in
-    the same launch.  Executions on a non-default stream are replayed from a
-    CUDA graph.
+    the same launch.  ``mode``:
+
+    * ``"branches"`` (default): the plans' own pass kernels, the plans spread
+      over ``branches`` parallel graph branches balanced by bytes;
+    * ``"queue"``: one persistent kernel over a level-ordered (plan, pass,
+      tile) work queue with bounded dependency waits.
+
+    ``autotune`` tunes the generic tile heights of the queue and the member
+    plans' register passes (cached per pass shape).
     """
 
     _OPS = {"forward": L.FORWARD, "inverse": L.INVERSE, "backward": L.BACKWARD}
+    _MODES = {"queue": 0, "branches": 1}
 
-    def __init__(self, plans, ops=("forward", "inverse"), autotune=True):
+    def __init__(self, plans, ops=("forward", "inverse"), autotune=True, mode="branches", branches=2):
         self.plans = list(plans)
         self.ops = tuple(ops)
         n = len(self.plans)
@@ -685,8 +693,14 @@ class PlanBatch:
         h = C.c_void_p()
         L.check(L.load().pb_batch_create(arr, n, opa, len(ops), 1 if autotune else 0, C.byref(h)), "batch")
         self._h = h
+        self.set_mode(mode, branches)
+
+    def set_mode(self, mode: str, branches: int = 2) -> None:
+        """Selects the execution mode; the workspace size may change with it."""
+        L.check(L.load().pb_batch_set_mode(self._h, self._MODES[mode], int(branches)), "batch mode")
+        self.mode = mode
         b = C.c_int64()
-        L.check(L.load().pb_batch_workspace_bytes(h, C.byref(b)), "batch workspace")
+        L.check(L.load().pb_batch_workspace_bytes(self._h, C.byref(b)), "batch workspace")
         self.workspace_bytes = b.value
 
     def allocate_workspace(self, device="cuda"):

@@ -1,7 +1,9 @@
-"""Ragged batch (one persistent launch over many plans): the 64-grid seed-4
-workload with every grid against a float64 FFT, smaller batches against the
-oracle, graph replay and rebinding of buffers, and the bounded dependency
-wait made to run out."""
+"""Ragged batch (one graph launch over many plans), in both modes -- the
+persistent work-queue kernel and parallel graph branches of the plans' own
+kernels: the 64-grid seed-4 workload with every grid against a float64 FFT,
+smaller batches against the oracle, graph replay and rebinding of buffers,
+mode switches, and the queue kernel's bounded dependency wait made to run
+out."""
 
 import math
 
@@ -24,8 +26,12 @@ CASES = [((1, 1), (36, 40, 42), ()), ((2, 2), (32, 48, 50), (2,)), ((1, 1), (45,
          ((2, 1), (30, 30, 30), ()), ((1, 2), (64, 32, 16), (2,)), ((1, 1), (35, 49, 63), ())]
 
 
+MODES = [("queue", 1), ("branches", 2), ("branches", 3)]
+
+
+@pytest.mark.parametrize("mode,branches", MODES)
 @pytest.mark.parametrize("rb", [4, 8])
-def test_ragged_batch_matches_per_plan_execution(rb):
+def test_ragged_batch_matches_per_plan_execution(rb, mode, branches):
     rng = np.random.default_rng(12)
     cdt = torch.complex64 if rb == 4 else torch.complex128
     plans, xs = [], []
@@ -35,7 +41,7 @@ def test_ragged_batch_matches_per_plan_execution(rb):
         e = int(np.prod(extra)) if extra else 1
         x = rng.standard_normal((e,) + shape) + 1j * rng.standard_normal((e,) + shape)
         xs.append(to_device(po.flat_concat(po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), cdt))
-    batch = pb.PlanBatch(plans, ("forward", "inverse"))
+    batch = pb.PlanBatch(plans, ("forward", "inverse"), mode=mode, branches=branches)
     ws = batch.allocate_workspace()
     mids = [p.allocate_output() for p in plans]
     ends = [p.allocate_input() for p in plans]
@@ -54,6 +60,8 @@ def test_ragged_batch_matches_per_plan_execution(rb):
         n = int(np.prod(shape))
         assert rel_l2(to_host(mid), to_host(ref_mid)) <= fft_bound(rb, n)
         assert rel_l2(to_host(end), to_host(x)) <= fft_bound(rb, n)
+        if mode == "branches":  # the plans' own kernels: the same bits
+            assert torch.equal(mid, ref_mid) and torch.equal(end, ref_end)
     # every batched forward and inverse against the oracle
     for plan, x, mid, end, (dims, shape, extra) in zip(plans, xs, mids, ends, CASES):
         e = int(np.prod(extra)) if extra else 1
@@ -82,7 +90,8 @@ def test_batch_rejects_chains_with_a_spectrum_check():
     pb.PlanBatch([plan], ("forward",))  # the forward chain has no check
 
 
-def test_config5_every_grid_against_float64():
+@pytest.mark.parametrize("mode", ["queue", "branches"])
+def test_config5_every_grid_against_float64(mode):
     """The 64-grid seed-4 workload (axis lengths from the 55 7-smooth numbers in
     [32, 256], 16 grids with an extra dim of 2), forward + inverse in one
     batch launch; each grid's spectrum against torch's complex128 fftn of its
@@ -98,7 +107,7 @@ def test_config5_every_grid_against_float64():
         xs.append(plan.input_pencil.scatter(g, e).contiguous())
         globs.append(g)
         plans.append(plan)
-    batch = pb.PlanBatch(plans, ("forward", "inverse"))
+    batch = pb.PlanBatch(plans, ("forward", "inverse"), mode=mode)
     ws = batch.allocate_workspace()
     mids = [p.allocate_output() for p in plans]
     ends = [p.allocate_input() for p in plans]
@@ -120,7 +129,7 @@ def test_config5_every_grid_against_float64():
         assert ef <= bound, (shape, extra, ef)
         assert ei <= bound, (shape, extra, ei)
         worst_f, worst_i = max(worst_f, ef), max(worst_i, ei)
-    print(f"\nconfig 5 (64 grids): worst forward rel-L2 {worst_f:.3e}, worst inverse {worst_i:.3e}")
+    print(f"\nconfig 5 (64 grids, {mode}): worst forward rel-L2 {worst_f:.3e}, worst inverse {worst_i:.3e}")
 
 
 def test_batch_dependency_wait_runs_out_and_recovers():
@@ -130,7 +139,7 @@ def test_batch_dependency_wait_runs_out_and_recovers():
     correct again."""
     plan = pb.C2cPlan.from_shape(pb.MpiTopology((1, 1)), (64, 64, 64), (), dtype=torch.complex64)
     x = torch.randn(plan.info.input_elems, dtype=torch.complex64, device="cuda")
-    batch = pb.PlanBatch([plan], ("forward", "inverse"), autotune=False)
+    batch = pb.PlanBatch([plan], ("forward", "inverse"), autotune=False, mode="queue")
     ws = batch.allocate_workspace()
     mid, end = plan.allocate_output(), plan.allocate_input()
     stream = torch.cuda.Stream()
@@ -151,3 +160,41 @@ def test_batch_dependency_wait_runs_out_and_recovers():
     torch.cuda.synchronize()
     assert rel_l2(to_host(mid), to_host(ref_mid)) <= fft_bound(4, 64 ** 3)
     assert rel_l2(to_host(end), to_host(x)) <= fft_bound(4, 64 ** 3)
+
+
+def test_batch_mode_switches_and_the_legacy_stream():
+    """One batch switched between modes and branch counts, and executed on the
+    legacy default stream (no capture: the plans run in order), gives the same
+    bits in branch mode and results within the bound in queue mode."""
+    shapes = [(40, 36, 48), (64, 30, 32), (25, 27, 28), (50, 42, 36), (32, 32, 32)]
+    plans = [pb.C2cPlan.from_shape(pb.MpiTopology((1, 2)), s, (), dtype=torch.complex64) for s in shapes]
+    xs = [torch.randn(p.info.input_elems, dtype=torch.complex64, device="cuda") for p in plans]
+    refs = []
+    for p, x in zip(plans, xs):
+        m = p.allocate_output()
+        p.forward(x, m)
+        refs.append(m)
+    batch = pb.PlanBatch(plans, ("forward",), autotune=False)
+    stream = torch.cuda.Stream()
+    for mode, branches in (("branches", 4), ("queue", 1), ("branches", 1), ("branches", 16)):
+        batch.set_mode(mode, branches)
+        ws = batch.allocate_workspace()
+        outs = [p.allocate_output() for p in plans]
+        with torch.cuda.stream(stream):
+            batch.execute([xs, outs], ws, stream)
+            batch.status(ws, stream)
+        torch.cuda.synchronize()
+        for o, r, s in zip(outs, refs, shapes):
+            if mode == "branches":
+                assert torch.equal(o, r), (mode, branches, s)
+            else:
+                assert rel_l2(to_host(o), to_host(r)) <= fft_bound(4, int(np.prod(s)))
+    batch.set_mode("branches", 2)
+    ws = batch.allocate_workspace()
+    outs = [p.allocate_output() for p in plans]
+    batch.execute([xs, outs], ws)  # the current (legacy default) stream
+    batch.status(ws)
+    torch.cuda.synchronize()
+    assert all(torch.equal(o, r) for o, r in zip(outs, refs))
+    with pytest.raises(pb.PencilError):
+        batch.set_mode("branches", 17)

@@ -571,3 +571,91 @@ def test_outputs_only_8_byte_aligned_match_aligned_outputs(shape, dims):
     torch.cuda.synchronize()
     assert torch.equal(shifted, ref)
     assert torch.equal(back, back_ref)
+
+
+STRIDED_C2R_CASES = [((2, 2), 64, (12, 40), ()), ((2, 3), 256, (20, 18), (2,)), ((2, 2), 90, (16, 24), ()),
+                     ((3, 2), 384, (9, 32), ()), ((2, 2), 10, (6, 8), ())]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,n,rest,extra", STRIDED_C2R_CASES)
+def test_c2r_strided_lines_match_oracle(rb, dims, n, rest, extra):
+    """C2R passes over strided lines (permute_dims = false): a C2rPlan reduces
+    axis 0, the outermost in the identity memory order, so its complex half
+    spectra are strided; power-of-two and 7-smooth lengths run the register
+    kernels' across-lines first stage (n = 10 stays on the generic kernel).
+    Forward (raw C2R) and backward (raw R2C) against the oracle."""
+    from pencil_b200 import _lib as L
+    rng = np.random.default_rng(21)
+    e = int(np.prod(extra)) if extra else 1
+    topo = pb.MpiTopology(dims)
+    lay = pb.DistributedLayout(False)
+    cshape = (n // 2 + 1,) + rest
+    plan = pb.C2rPlan.from_shape(topo, cshape, n, extra, layout=lay, dtype=RDT[rb])
+    kinds = plan.step_kernels(L.FORWARD)
+    if n >= 32:  # the C2R pass is the last launch (after the spectrum check)
+        assert kinds[-1] in ("pow2", "mixed_radix"), kinds
+    route = po.c2r_route(po.Topology(dims), cshape, n, None, False)
+    real_pen = oracle_pencil(plan.output_pencil)
+    x = rand_field(rng, (n,) + rest, extra, False, rb)
+    spec_locs = po.execute_forward(route, po.scatter(real_pen, x, (e,)))
+    spec = po.flat_concat(spec_locs)
+    got = run_plan(plan, "backward", po.flat_concat(po.scatter(real_pen, x, (e,))), RDT[rb], CDT[rb],
+                   plan.info.input_elems)
+    assert rel_l2(got, spec) <= fft_bound(rb, x.size)
+    back = po.execute_reverse(route, spec_locs, False, NPR[rb])
+    got = run_plan(plan, "forward", spec.astype(NPC[rb]), CDT[rb], RDT[rb], plan.info.output_elems)
+    assert rel_l2(got, po.flat_concat(back).real) <= fft_bound(rb, x.size)
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+def test_r2c_selection_strided_inverse_matches_oracle(rb):
+    """An R2C plan selecting axes 0 and 1 reduces axis 1; with permute_dims =
+    false that axis is strided, so the inverse's C2R pass loads across lines."""
+    from pencil_b200 import _lib as L
+    rng = np.random.default_rng(22)
+    dims, shape = (2, 2), (48, 128, 20)
+    topo = pb.MpiTopology(dims)
+    lay = pb.DistributedLayout(False)
+    plan = pb.R2cPlan.from_shape(topo, shape, (), selection=[0, 1], layout=lay, dtype=RDT[rb])
+    assert "generic" not in plan.step_kernels(L.INVERSE), plan.step_kernels(L.INVERSE)
+    route = po.r2c_route(po.Topology(dims), shape, [0, 1], False)
+    x = rand_field(rng, shape, (), False, rb)
+    check_transform(plan, route, x, 1, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (1,))), (1,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, 1, rb, True, d)
+
+
+# FFT lengths on the register kernel: n for the II/III kinds and the DHT,
+# 2(n+1) for DST-I (35 -> 72), 2(n-1) for DCT-I (37 -> 72), n/2 for type IV
+STRIDED_R2R_CASES = [((2, 3), (40, 35, 48), (3,), ("DctII", "DstI", "Dht")),
+                     ((2, 2), (64, 50, 37), (), ("DctIV", "DstIII", "DctI")),
+                     ((3, 2), (45, 32, 84), (2,), ("DstII", "DctIII", "DstIV"))]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape,extra,kinds", STRIDED_R2R_CASES)
+def test_r2r_strided_lines_match_oracle(rb, cplx, dims, shape, extra, kinds):
+    """Real-to-real passes over strided lines (permute_dims = false) on the
+    mixed-radix kernel's across-lines load, real and complex values, every
+    kind family (Makhoul, symmetric extensions, type IV, DHT), against the
+    oracle forward / inverse / backward.  In the identity memory order the
+    passes over axes 1 and 0 read strided lines; the first pass (axis 2,
+    contiguous) stores into a layout that splits axis 2 and stays on the
+    generic kernel."""
+    from pencil_b200 import _lib as L
+    rng = np.random.default_rng(23)
+    e = int(np.prod(extra)) if extra else 1
+    topo = pb.MpiTopology(dims)
+    lay = pb.DistributedLayout(False)
+    dtype = CDT[rb] if cplx else RDT[rb]
+    plan = pb.R2rPlan.from_shape(topo, shape, extra, kinds, layout=lay, dtype=dtype)
+    for op in (L.FORWARD, L.INVERSE):
+        assert plan.step_kernels(op).count("mixed_radix") >= 2, plan.step_kernels(op)
+    route = po.r2r_route(po.Topology(dims), shape, list(kinds), False)
+    x = rand_field(rng, shape, extra, cplx, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, e, rb, cplx, d)
