@@ -36,7 +36,9 @@ POW2 = [32, 64, 128, 256, 512, 1024, 2048]
 MR = [35, 36, 40, 42, 45, 48, 49, 50, 54, 56, 60, 63, 70, 72, 75, 80, 81, 84, 90, 96, 98, 100, 105, 108, 112, 120,
       125, 126, 135, 140, 144, 147, 150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
       245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375, 378, 384, 392, 400, 405, 420,
-      432, 441, 448, 450, 480, 486, 490, 500, 504]
+      432, 441, 448, 450, 480, 486, 490, 500, 504, 525, 540, 560, 567, 576, 588, 600, 625, 630, 640, 648, 672,
+      675, 686, 700, 720, 729, 735, 750, 756, 768, 784, 800, 810, 840, 864, 875, 882, 896, 900, 945, 960, 972,
+      980, 1000, 1008]
 # the mixed-radix kernel also runs the real-to-real kinds on powers of two and
 # on 770 (mr_lengths.hpp, kMrR2rLengths)
 MR_ALL = sorted(MR + [32, 64, 128, 256, 512, 770])

@@ -1,5 +1,5 @@
 // Line lengths served by the mixed-radix pass kernel (mr_kernel.cuh): the
-// 79 numbers 2^a 3^b 5^c 7^d in [35, 504] that are not powers of two.  The
+// 115 numbers 2^a 3^b 5^c 7^d in [35, 1008] that are not powers of two.  The
 // kernels are split over MR_GROUPS translation units (mr_kernels.cu compiled
 // once per group) so that they build in parallel.
 #pragma once
@@ -14,7 +14,10 @@ constexpr int kMrLengths[] = {35,  36,  40,  42,  45,  48,  49,  50,  54,  56,  
                               81,  84,  90,  96,  98,  100, 105, 108, 112, 120, 125, 126, 135, 140, 144, 147,
                               150, 160, 162, 168, 175, 180, 189, 192, 196, 200, 210, 216, 224, 225, 240, 243,
                               245, 250, 252, 270, 280, 288, 294, 300, 315, 320, 324, 336, 343, 350, 360, 375,
-                              378, 384, 392, 400, 405, 420, 432, 441, 448, 450, 480, 486, 490, 500, 504};
+                              378, 384, 392, 400, 405, 420, 432, 441, 448, 450, 480, 486, 490, 500, 504,
+                              525, 540, 560, 567, 576, 588, 600, 625, 630, 640, 648, 672, 675, 686, 700, 720,
+                              729, 735, 750, 756, 768, 784, 800, 810, 840, 864, 875, 882, 896, 900, 945, 960,
+                              972, 980, 1000, 1008};
 constexpr int kMrCount = sizeof(kMrLengths) / sizeof(kMrLengths[0]);
 
 // Resident CTAs per SM the kernels are compiled for (the register budget

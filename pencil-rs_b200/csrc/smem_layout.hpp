@@ -112,7 +112,43 @@ __host__ __device__ constexpr SmemLayout mr_layout(int N, int real_bytes) {
     case 500: return real_bytes == 4 ? SmemLayout{0, 500} : SmemLayout{2, 628};
     case 504: return real_bytes == 4 ? SmemLayout{3, 572} : SmemLayout{3, 572};
     case 512: return real_bytes == 4 ? SmemLayout{4, 548} : SmemLayout{3, 580};
+    case 525: return real_bytes == 4 ? SmemLayout{0, 532} : SmemLayout{0, 532};
+    case 540: return real_bytes == 4 ? SmemLayout{0, 540} : SmemLayout{0, 540};
+    case 560: return real_bytes == 4 ? SmemLayout{0, 564} : SmemLayout{0, 564};
+    case 567: return real_bytes == 4 ? SmemLayout{0, 572} : SmemLayout{0, 572};
+    case 576: return real_bytes == 4 ? SmemLayout{0, 580} : SmemLayout{4, 612};
+    case 588: return real_bytes == 4 ? SmemLayout{2, 740} : SmemLayout{0, 588};
+    case 600: return real_bytes == 4 ? SmemLayout{0, 612} : SmemLayout{0, 604};
+    case 625: return real_bytes == 4 ? SmemLayout{0, 628} : SmemLayout{0, 628};
+    case 630: return real_bytes == 4 ? SmemLayout{0, 636} : SmemLayout{0, 636};
+    case 640: return real_bytes == 4 ? SmemLayout{0, 644} : SmemLayout{0, 644};
+    case 648: return real_bytes == 4 ? SmemLayout{3, 740} : SmemLayout{5, 668};
+    case 672: return real_bytes == 4 ? SmemLayout{2, 844} : SmemLayout{0, 676};
+    case 675: return real_bytes == 4 ? SmemLayout{0, 684} : SmemLayout{0, 676};
+    case 686: return real_bytes == 4 ? SmemLayout{0, 692} : SmemLayout{0, 692};
+    case 700: return real_bytes == 4 ? SmemLayout{0, 700} : SmemLayout{0, 700};
+    case 720: return real_bytes == 4 ? SmemLayout{4, 764} : SmemLayout{0, 724};
+    case 729: return real_bytes == 4 ? SmemLayout{0, 732} : SmemLayout{0, 732};
+    case 735: return real_bytes == 4 ? SmemLayout{0, 740} : SmemLayout{0, 740};
+    case 750: return real_bytes == 4 ? SmemLayout{0, 756} : SmemLayout{0, 756};
+    case 756: return real_bytes == 4 ? SmemLayout{2, 948} : SmemLayout{0, 756};
+    case 768: return real_bytes == 4 ? SmemLayout{2, 964} : SmemLayout{0, 772};
     case 770: return real_bytes == 4 ? SmemLayout{0, 780} : SmemLayout{0, 772};
+    case 784: return real_bytes == 4 ? SmemLayout{0, 788} : SmemLayout{0, 788};
+    case 800: return real_bytes == 4 ? SmemLayout{4, 852} : SmemLayout{3, 900};
+    case 810: return real_bytes == 4 ? SmemLayout{0, 812} : SmemLayout{0, 812};
+    case 840: return real_bytes == 4 ? SmemLayout{0, 852} : SmemLayout{0, 844};
+    case 864: return real_bytes == 4 ? SmemLayout{4, 932} : SmemLayout{3, 972};
+    case 875: return real_bytes == 4 ? SmemLayout{0, 876} : SmemLayout{0, 876};
+    case 882: return real_bytes == 4 ? SmemLayout{0, 884} : SmemLayout{0, 884};
+    case 896: return real_bytes == 4 ? SmemLayout{0, 900} : SmemLayout{0, 900};
+    case 900: return real_bytes == 4 ? SmemLayout{0, 900} : SmemLayout{0, 900};
+    case 945: return real_bytes == 4 ? SmemLayout{0, 948} : SmemLayout{0, 948};
+    case 960: return real_bytes == 4 ? SmemLayout{4, 1020} : SmemLayout{3, 1084};
+    case 972: return real_bytes == 4 ? SmemLayout{0, 972} : SmemLayout{0, 972};
+    case 980: return real_bytes == 4 ? SmemLayout{0, 980} : SmemLayout{2, 1228};
+    case 1000: return real_bytes == 4 ? SmemLayout{0, 1012} : SmemLayout{3, 1124};
+    case 1008: return real_bytes == 4 ? SmemLayout{0, 1012} : SmemLayout{3, 1140};
     default: return SmemLayout{3, N + N / 8 + 1};
   }
 }

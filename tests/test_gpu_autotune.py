@@ -2,8 +2,8 @@
 (pb_plan_autotune / pb_plan_set_config / pb_plan_step_config).
 
 * Schedule 1 (radices up to 8) of the mixed-radix kernel is a kernel of its
-  own: every f32 length runs it here against the oracle, C2C forward /
-  inverse / backward and R2C / C2R.
+  own: every f32 length runs it here against the oracle (C2C forward /
+  inverse / backward and R2C / C2R up to 504, C2C above).
 * The persistent grid does not change the arithmetic: fewer CTAs per SM give
   bit-identical results.
 * The autotuner marks the passes it chose, keeps the results within the
@@ -31,7 +31,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 import pencil_b200 as pb  # noqa: E402
 from pencil_b200 import _lib as L  # noqa: E402
 
-from test_gpu_mixed_radix import GRIDS, SHAPES  # noqa: E402
+from test_gpu_mixed_radix import GRIDS, LONG, SHAPES  # noqa: E402
 from test_gpu_parity import CDT, RDT, check_transform, rand_field  # noqa: E402
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -61,6 +61,20 @@ def test_schedule_one_on_every_length(idx):
                      po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (1,))), (1,))
     for d in ("inv", "bwd"):
         check_transform(plan, route, spec, 1, 4, True, d)
+
+
+@pytest.mark.parametrize("idx", range(len(LONG)))
+def test_schedule_one_on_the_long_lengths(idx):
+    n = LONG[idx]
+    shape = (20, 16, n) if idx % 2 == 0 else (n, 16, 20)
+    dims = GRIDS[idx % len(GRIDS)]
+    rng = np.random.default_rng(500 + idx)
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), dtype=CDT[4])
+    plan.set_config(sched=1)
+    route = po.c2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, (), True, 4)
+    for d in ("fwd", "inv"):
+        check_transform(plan, route, x, 1, 4, True, d)
 
 
 @pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])

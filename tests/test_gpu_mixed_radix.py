@@ -1,5 +1,5 @@
 """The register-fed mixed-radix pass kernel (7-smooth lengths that are not
-powers of two) against the oracle: every one of its 79 lengths in C2C
+powers of two) against the oracle: every one of its 115 lengths in C2C
 forward/inverse/backward and R2C/C2R, f32 and f64, on pencil grids whose
 routes take both the direct and the transposed store.  Tolerances as in the
 other parity tests: rel-L2 <= 1e-6*log2(N) (f32) / 1e-14*log2(N) (f64)."""
@@ -122,3 +122,35 @@ def test_mixed_radix_vjp_adjoint_identity_f64(family):
         lhs = _dot(to_host(ax), to_host(y))
         rhs = _dot(to_host(x), to_host(aty))
         assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (op, lhs, rhs)
+
+
+LONG = [525, 540, 560, 567, 576, 588, 600, 625, 630, 640, 648, 672, 675, 686, 700, 720, 729, 735, 750, 756, 768,
+        784, 800, 810, 840, 864, 875, 882, 896, 900, 945, 960, 972, 980, 1000, 1008]
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("idx", range(len(LONG)))
+def test_mixed_radix_long_lengths(rb, idx):
+    """The 7-smooth lengths above 512 (tiles of 4 sequences in f32, 2 in f64),
+    the long axis first (transposed stores out of it) or last (contiguous
+    lines, direct stores): C2C forward / inverse / backward and R2C / C2R
+    against the oracle."""
+    n = LONG[idx]
+    shape = (n, 16, 20) if idx % 2 == 0 else (20, 16, n)
+    dims = GRIDS[idx % len(GRIDS)]
+    rng = np.random.default_rng(400 + idx)
+    topo = pb.MpiTopology(dims)
+    plan = pb.C2cPlan.from_shape(topo, shape, (), dtype=CDT[rb])
+    assert "mixed_radix" in plan.step_kernels(L.FORWARD) + plan.step_kernels(L.INVERSE)
+    route = po.c2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, (), True, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, 1, rb, True, d)
+    plan = pb.R2cPlan.from_shape(topo, shape, (), dtype=RDT[rb])
+    route = po.r2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, (), False, rb)
+    check_transform(plan, route, x, 1, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (1,))), (1,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, 1, rb, True, d)
