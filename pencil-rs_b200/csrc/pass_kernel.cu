@@ -12,9 +12,11 @@
 // FFT core: Stockham autosort, mixed radix 2/3/4/5/7/8 with compile-time
 // butterflies plus an O(R) generic radix for other primes, twiddles from a
 // table of m-th roots of unity generated on the host in extended precision
-// and rounded once to the plan type.  R2C/C2R use the two-real-lines-in-one-
-// complex-FFT split; DCT/DST II/III use Makhoul's n-point reordering with
-// pre/post twiddles; DCT/DST IV use an n/2-point complex FFT (even n); type I
+// and rounded once to the plan type; lengths with a prime factor above 31
+// take Bluestein's chirp-z form over a power-of-two FFT (fft_run).  R2C/C2R
+// use the two-real-lines-in-one-complex-FFT split; DCT/DST II/III use
+// Makhoul's n-point reordering with pre/post twiddles; DCT/DST IV use an
+// n/2-point complex FFT (even n); type I
 // kinds use the symmetric/antisymmetric extension of a line pair; the DHT is
 // the Hartley combination of a pair's FFT.  Every real-valued kind processes
 // two real lines (or the two components of one complex line) per complex FFT.
@@ -89,7 +91,7 @@ __device__ void fft_stage_generic(const C* __restrict__ in, C* __restrict__ out,
 }
 
 template <typename C, bool INV>
-__device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const PassArgs& A) {
+__device__ C* fft_stages(C* b0, C* b1, int nseq, int m, int ld, const C* W, const PassArgs& A) {
   C* in = b0;
   C* out = b1;
   int Ns = 1;
@@ -113,6 +115,44 @@ __device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const P
   return in;
 }
 
+// The m-point FFT of nseq sequences in b0 (element j of sequence s at
+// s*ld + j), result in the returned buffer.  Direct Stockham stages, or for
+// A.bs_m2 > 0 Bluestein's chirp-z form: with w_j = exp(-+i pi j^2/m) (the
+// pass's sign, A.bs_chirp), X_k = w_k * sum_j (x_j w_j) conj(w)_{k-j}, the
+// sum a cyclic convolution of length M = bs_m2 computed as a forward M-point
+// FFT, a product with the precomputed transform of the conjugate chirp
+// (A.bs_kernel, with the 1/M of the inverse), and an inverse M-point FFT.
+// W then holds the M-th roots and A.radix the M-point radices.
+template <typename C, bool INV>
+__device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const PassArgs& A) {
+  if (A.bs_m2 == 0) return fft_stages<C, INV>(b0, b1, nseq, m, ld, W, A);
+  using R = decltype(W[0].x);
+  const int M = A.bs_m2;
+  const int lg = __ffs(M) - 1;
+  const C* __restrict__ chirp = reinterpret_cast<const C*>(A.bs_chirp);
+  const C* __restrict__ ker = reinterpret_cast<const C*>(A.bs_kernel);
+  const int total = nseq * M;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int s = t >> lg, j = t & (M - 1);
+    b1[s * ld + j] = j < m ? cmul(b0[s * ld + j], chirp[j]) : mk<C, R>(R(0), R(0));
+  }
+  __syncthreads();
+  C* f = fft_stages<C, false>(b1, b0, nseq, M, ld, W, A);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int s = t >> lg, j = t & (M - 1);
+    f[s * ld + j] = cmul(f[s * ld + j], ker[j]);
+  }
+  __syncthreads();
+  C* g = fft_stages<C, true>(f, f == b0 ? b1 : b0, nseq, M, ld, W, A);
+  const int tm = nseq * m;
+  for (int t = threadIdx.x; t < tm; t += blockDim.x) {
+    const int s = t / m, k = t - s * m;
+    g[s * ld + k] = cmul(g[s * ld + k], chirp[k]);
+  }
+  __syncthreads();
+  return g;
+}
+
 // One tile of a pass: gather, transform, scatter.  `smem` is the block's
 // dynamic shared memory (pass_smem_bytes(A) bytes).
 template <typename R>
@@ -127,7 +167,8 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   int* dS = sS + nin;
   size_t off = ((size_t)(nin + nout) * 12 + 15) & ~size_t(15);
   C* W = reinterpret_cast<C*>(smem + off);
-  C* buf0 = W + ((m + 1) & ~1);
+  const int mw = A.bs_m2 ? A.bs_m2 : m;  // twiddle entries: the Bluestein FFT's length
+  C* buf0 = W + ((mw + 1) & ~1);
   C* buf1 = buf0 + A.buf_elems;
   const int tid = threadIdx.x, nt = blockDim.x;
 
@@ -193,7 +234,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& A, long long t, unsign
   const unsigned m_n = fdiv_magic(A.n), m_2n = fdiv_magic(2 * A.n), m_h = fdiv_magic(A.n / 2 + 1);
   const C* Wg = reinterpret_cast<const C*>(A.twiddle);
   if (Wg != nullptr)
-    for (int i = tid; i < m; i += nt) W[i] = Wg[i];
+    for (int i = tid; i < mw; i += nt) W[i] = Wg[i];
   __syncthreads();
 
   const int total_in = L * nin;
@@ -692,7 +733,7 @@ size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
   if (A.fast == 2 && mr_batch_supported(A.m, real_bytes)) return mr_batch_smem(A.m);
   const size_t cbytes = 2 * (size_t)real_bytes;
   size_t off = ((size_t)(A.n_in + A.n_out) * 12 + 15) & ~size_t(15);
-  off += (size_t)((A.m + 1) & ~1) * cbytes;
+  off += (size_t)(((A.bs_m2 ? A.bs_m2 : A.m) + 1) & ~1) * cbytes;
   off += 2 * (size_t)A.buf_elems * cbytes;
   return off;
 }

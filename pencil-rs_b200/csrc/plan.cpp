@@ -704,6 +704,109 @@ static std::vector<int> radices(int m) {
   return r;
 }
 
+// Bluestein: the convolution length (a power of two >= 2m - 1) when m has a
+// prime factor above 31 -- where the generic kernel's O(p) radix costs more
+// per point than two power-of-two FFTs of about 2-4 m points -- and the three
+// M-point buffers fit shared memory (M <= 4096 f32, 2048 f64); else 0.
+static int bluestein_len(int m, int real_bytes) {
+  int r = m, big = 1;
+  for (int p = 2; (long long)p * p <= r; ++p)
+    while (r % p == 0) {
+      big = std::max(big, p);
+      r /= p;
+    }
+  big = std::max(big, r);
+  if (big <= 31) return 0;
+  int M = 1;
+  while (M < 2 * m - 1) M <<= 1;
+  return M <= (real_bytes == 4 ? 4096 : 2048) ? M : 0;
+}
+
+// The chirp w_j = exp(-i pi j^2 / m) of a forward pass (conjugated for an
+// inverse one), j < m, with j^2 reduced mod 2m in integers so that the angle
+// stays exact; rounded once to the plan type.
+static size_t chirp_table(pb_plan& P, int m, int inv) {
+  const std::string key = "BC" + std::to_string(m) + "i" + std::to_string(inv) + "r" + std::to_string(P.real_bytes);
+  auto it = P.cache.find(key);
+  if (it != P.cache.end()) return it->second;
+  const long double pi = 3.14159265358979323846264338327950288L;
+  std::vector<double> d(2 * (size_t)m);
+  for (int j = 0; j < m; ++j) {
+    const long long q = ((long long)j * j) % (2LL * m);
+    const long double th = (inv ? 1.0L : -1.0L) * pi * (long double)q / (long double)m;
+    d[2 * j] = (double)cosl(th);
+    d[2 * j + 1] = (double)sinl(th);
+  }
+  size_t off;
+  if (P.real_bytes == 4) {
+    std::vector<float> f(d.begin(), d.end());
+    off = P.host.add(f.data(), f.size() * sizeof(float));
+  } else {
+    off = P.host.add(d.data(), d.size() * sizeof(double));
+  }
+  P.cache[key] = off;
+  return off;
+}
+
+// The DFT (negative exponent) of the M-periodic conjugate chirp b_j =
+// conj(w_j), b_{M-j} = b_j (0 < j < m), zero elsewhere, divided by M: the
+// convolution's kernel.  Radix-2 FFT in long double, rounded once.
+static size_t bluestein_kernel_table(pb_plan& P, int m, int M, int inv) {
+  const std::string key =
+      "BK" + std::to_string(m) + "_" + std::to_string(M) + "i" + std::to_string(inv) + "r" + std::to_string(P.real_bytes);
+  auto it = P.cache.find(key);
+  if (it != P.cache.end()) return it->second;
+  const long double pi = 3.14159265358979323846264338327950288L;
+  std::vector<long double> re(M, 0.0L), im(M, 0.0L);
+  for (int j = 0; j < m; ++j) {
+    const long long q = ((long long)j * j) % (2LL * m);
+    const long double th = (inv ? -1.0L : 1.0L) * pi * (long double)q / (long double)m;  // conj(w_j)
+    re[j] = cosl(th);
+    im[j] = sinl(th);
+    if (j > 0) {
+      re[M - j] = re[j];
+      im[M - j] = im[j];
+    }
+  }
+  // bit-reversal permutation, then iterative butterflies
+  for (int i = 1, j = 0; i < M; ++i) {
+    int bit = M >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  for (int len = 2; len <= M; len <<= 1) {
+    for (int i = 0; i < M; i += len)
+      for (int k = 0; k < len / 2; ++k) {
+        const long double th = -2.0L * pi * (long double)k / (long double)len;
+        const long double c = cosl(th), sn = sinl(th);
+        const int a = i + k, b = i + k + len / 2;
+        const long double xr = re[b] * c - im[b] * sn, xi = re[b] * sn + im[b] * c;
+        re[b] = re[a] - xr;
+        im[b] = im[a] - xi;
+        re[a] += xr;
+        im[a] += xi;
+      }
+  }
+  std::vector<double> d(2 * (size_t)M);
+  for (int k = 0; k < M; ++k) {
+    d[2 * k] = (double)(re[k] / (long double)M);
+    d[2 * k + 1] = (double)(im[k] / (long double)M);
+  }
+  size_t off;
+  if (P.real_bytes == 4) {
+    std::vector<float> f(d.begin(), d.end());
+    off = P.host.add(f.data(), f.size() * sizeof(float));
+  } else {
+    off = P.host.add(d.data(), d.size() * sizeof(double));
+  }
+  P.cache[key] = off;
+  return off;
+}
+
 static int fft_len(int kind, int sub, int n) {
   switch (kind) {
     case P_COPY: return 1;
@@ -1025,15 +1128,26 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   A.m = fft_len(op.kind, op.sub, A.n);
   if (A.m > (1 << 20)) fail(PB_EUNSUPPORTED);
   if (op.kind != P_COPY) {
-    auto r = radices(A.m);
+    // Bluestein: the generic kernel runs an M-point FFT (radices, roots) in
+    // place of the m-point one; the register kernels never take such lengths
+    const int M = bluestein_len(A.m, P.real_bytes);
+    auto r = radices(M ? M : A.m);
     A.nstages = (int)r.size();
     for (int i = 0; i < A.nstages; ++i) A.radix[i] = r[i];
-    A.twiddle = enc(roots_table(P, A.m));
+    A.twiddle = enc(roots_table(P, M ? M : A.m));
+    if (M) {
+      A.bs_m2 = M;
+      A.bs_chirp = enc(chirp_table(P, A.m, A.inv));
+      A.bs_kernel = enc(bluestein_kernel_table(P, A.m, M, A.inv));
+    }
   } else {
     A.nstages = 0;
     A.twiddle = nullptr;
   }
-  A.ld = A.m + ((A.m % 8 == 0) ? 1 : 0);
+  {
+    const int fl = A.bs_m2 ? A.bs_m2 : A.m;
+    A.ld = fl + ((fl % 8 == 0) ? 1 : 0);
+  }
   if (op.kind == P_COPY) A.ld = 1;
   // kind-specific twiddles (exp(i*pi*(ks*k+k0)/den))
   if (op.kind == P_R2R) {
@@ -1374,6 +1488,8 @@ static void finalize(pb_plan& P) {
         fix(s.pa.twiddle);
         fix(s.pa.aux0);
         fix(s.pa.aux1);
+        fix(s.pa.bs_chirp);
+        fix(s.pa.bs_kernel);
         fix(s.pa.tile_tab);
         fix(s.pa.piece_tab);
         const void* kt = s.pa.ktab;
@@ -2179,6 +2295,8 @@ static void upload_steps(pb_plan& P, std::vector<Step>& steps) {
     fix(s.pa.twiddle);
     fix(s.pa.aux0);
     fix(s.pa.aux1);
+    fix(s.pa.bs_chirp);
+    fix(s.pa.bs_kernel);
     fix(s.pa.tile_tab);
     fix(s.pa.piece_tab);
     const void* kt = s.pa.ktab;
@@ -3147,6 +3265,8 @@ static void autotune_pass(pb_plan& T, const pb_plan& plan, int mode, int step, v
     fix(st.pa.twiddle);
     fix(st.pa.aux0);
     fix(st.pa.aux1);
+    fix(st.pa.bs_chirp);
+    fix(st.pa.bs_kernel);
     fix(st.pa.tile_tab);
     fix(st.pa.piece_tab);
     const void* kt = st.pa.ktab;
@@ -3337,6 +3457,8 @@ static pb_batch* batch_create(pb_plan* const* plans, int count, const int* ops, 
     fix(d.pa.twiddle);
     fix(d.pa.aux0);
     fix(d.pa.aux1);
+    fix(d.pa.bs_chirp);
+    fix(d.pa.bs_kernel);
     fix(d.pa.tile_tab);
     fix(d.pa.piece_tab);
     d.pa.ktab = reinterpret_cast<const int2*>(fix_ptr(T, d.pa.ktab));
@@ -3908,6 +4030,8 @@ static pb_slice* slice_create(const pb_plan* plan, int lo, int hi) {
         fix(st.pa.twiddle);
         fix(st.pa.aux0);
         fix(st.pa.aux1);
+        fix(st.pa.bs_chirp);
+        fix(st.pa.bs_kernel);
         fix(st.pa.tile_tab);
         fix(st.pa.piece_tab);
         st.pa.ktab = reinterpret_cast<const int2*>(fix_ptr(T, st.pa.ktab));

@@ -1,0 +1,88 @@
+"""Lengths with a prime factor above 31 on the generic kernel: the FFT core
+runs Bluestein's chirp-z form (the m-point DFT as a cyclic convolution over a
+power-of-two FFT) instead of an O(p) radix.  C2C, R2C / C2R and the
+real-to-real kinds whose FFT length has such a factor (DCT-II of 101, DST-I of
+100 -> 202 = 2 * 101, DHT of 67, DCT-IV of 94 -> 47), f32 and f64, against the
+oracle's float64 DFT within the usual bound."""
+
+import numpy as np
+import pytest
+
+import pencil_oracle as po
+from pb_testutil import oracle_pencil
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import pencil_b200 as pb  # noqa: E402
+from pencil_b200 import _lib as L  # noqa: E402
+
+from test_gpu_parity import CDT, RDT, check_transform, rand_field  # noqa: E402
+
+C2C_CASES = [((2, 2), (37, 12, 41)), ((2, 3), (101, 8, 10)), ((1, 3), (9, 6, 257)), ((2, 2), (1021, 4, 6)),
+             ((2, 1), (12, 514, 5))]
+
+
+def _bluestein_steps(plan, op):
+    """Launches of `op` on the generic kernel whose radices are all powers of
+    two although their FFT length is not (the Bluestein form)."""
+    out = []
+    for c in plan.step_configs(op):
+        n = c["fft_len"]
+        if c["kernel"] == "generic" and n & (n - 1) and c["radices"] and all(r in (2, 4, 8) for r in c["radices"]):
+            out.append(n)
+    return out
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape", C2C_CASES)
+def test_c2c_prime_lengths(rb, dims, shape):
+    rng = np.random.default_rng(31)
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), dtype=CDT[rb])
+    assert _bluestein_steps(plan, L.FORWARD), plan.step_configs(L.FORWARD)
+    route = po.c2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, (), True, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, 1, rb, True, d)
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("dims,shape,extra", [((2, 2), (10, 12, 127), ()), ((2, 3), (53, 9, 8), (2,))])
+def test_r2c_prime_lengths(rb, dims, shape, extra):
+    rng = np.random.default_rng(32)
+    e = int(np.prod(extra)) if extra else 1
+    plan = pb.R2cPlan.from_shape(pb.MpiTopology(dims), shape, extra, dtype=RDT[rb])
+    assert _bluestein_steps(plan, L.FORWARD) and _bluestein_steps(plan, L.INVERSE)
+    route = po.r2c_route(po.Topology(dims), shape)
+    x = rand_field(rng, shape, extra, False, rb)
+    check_transform(plan, route, x, e, rb, False, "fwd")
+    spec = po.gather(oracle_pencil(plan.output_pencil),
+                     po.execute_forward(route, po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), (e,))
+    for d in ("inv", "bwd"):
+        check_transform(plan, route, spec, e, rb, True, d)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("rb", [4, 8])
+@pytest.mark.parametrize("shape,kinds", [((101, 100, 67), ("DctII", "DstI", "Dht")),
+                                         ((94, 37, 12), ("DctIV", "DstIII", "DctI"))])
+def test_r2r_prime_fft_lengths(rb, cplx, shape, kinds):
+    rng = np.random.default_rng(33)
+    dims = (2, 3)
+    dtype = CDT[rb] if cplx else RDT[rb]
+    plan = pb.R2rPlan.from_shape(pb.MpiTopology(dims), shape, (2,), kinds, dtype=dtype)
+    assert _bluestein_steps(plan, L.FORWARD)
+    route = po.r2r_route(po.Topology(dims), shape, list(kinds))
+    x = rand_field(rng, shape, (2,), cplx, rb)
+    for d in ("fwd", "inv", "bwd"):
+        check_transform(plan, route, x, 2, rb, cplx, d)
+
+
+def test_small_prime_factors_keep_the_direct_radices():
+    # 62 = 2 * 31: largest prime 31, the direct generic radices
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology((1, 1)), (62, 8, 8), (), dtype=torch.complex64)
+    cfg = [c for c in plan.step_configs(L.FORWARD) if c["fft_len"] == 62]
+    assert cfg and 31 in cfg[0]["radices"], cfg
