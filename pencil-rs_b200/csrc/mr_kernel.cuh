@@ -582,12 +582,11 @@ __device__ __forceinline__ void mr_store(const PassArgs& A, const TileAddr& ta, 
 
 constexpr int MR_MAX_PIECES = 64;  // pieces of a transposed store (the plan allows at most 64)
 
-// Outputs per line the row tables of the transposed store hold: N, or 2N for
-// the real-to-real kernel, whose type-IV kinds write n = 2N outputs from an
-// N-point FFT.
+// Outputs per line the row tables of the transposed store hold: N, or
+// mr_r2r_table_len(N) for the real-to-real kernel.
 template <int N, bool R2R>
 __host__ __device__ constexpr int mr_table_len() {
-  return R2R ? 2 * N : N;
+  return R2R ? mr_r2r_table_len(N) : N;
 }
 
 // Shared memory of one CTA: two buffers of NSEQ padded sequences, the twiddle

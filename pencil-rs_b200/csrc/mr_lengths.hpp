@@ -42,8 +42,19 @@ __host__ __device__ constexpr int mr_min_ctas(int real_bytes, int N, int S) {
   return (real_bytes != 4 || N > 512) ? 2 : (S == 1 ? 3 : (mr_two_cta_length(N) ? 2 : 3));
 }
 
-// The same for the real-to-real kinds (default schedule only).
-__host__ __device__ constexpr int mr_r2r_min_ctas(int real_bytes, int N) { return (real_bytes == 4 && N <= 512) ? 3 : 2; }
+// The same for the real-to-real kinds (default schedule only).  The 770-point
+// kernel (the DST-I of a 384-point axis) takes 3 as well: with its row tables
+// sized for the DST-I's outputs (mr_r2r_table_len) three CTAs fit in shared
+// memory.
+__host__ __device__ constexpr int mr_r2r_min_ctas(int real_bytes, int N) {
+  return (real_bytes == 4 && (N <= 512 || N == 770)) ? 3 : 2;
+}
+
+// Outputs per line that the real-to-real kernel's row tables hold for FFT
+// length N: 2N up to 512 (the type-IV kinds write n = 2N outputs from an
+// N-point FFT), N above (770 serves the DST-I of 384, 384 outputs).  The host
+// keeps passes with more outputs on the generic kernel.
+__host__ __device__ constexpr int mr_r2r_table_len(int N) { return N <= 512 ? 2 * N : N; }
 constexpr int MR_GROUPS = 8;
 
 // Lengths whose passes the persistent batch kernel (pass_kernel.cu) runs with

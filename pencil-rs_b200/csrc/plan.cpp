@@ -33,6 +33,7 @@
 #include <string>
 #include <vector>
 
+#include "mr_lengths.hpp"
 #include "pb_aux.hpp"
 #include "pencil_b200.h"
 
@@ -1263,9 +1264,10 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.lines = L;
     }
   }
-  // the register kernels' row tables hold A.m outputs per line (2 A.m in the
-  // real-to-real kernel): anything longer stays on the generic kernel
-  if (A.fast && A.n_out > (A.fast == 3 ? 2 * A.m : (A.half ? 2 * A.m : A.m))) {
+  // the register kernels' row tables hold A.m outputs per line
+  // (mr_r2r_table_len in the real-to-real kernel): anything longer stays on
+  // the generic kernel
+  if (A.fast && A.n_out > (A.fast == 3 ? mr_r2r_table_len(A.m) : (A.half ? 2 * A.m : A.m))) {
     A.fast = 0;
     A.half = 0;
     A.m = fft_len(op.kind, op.sub, A.n);
