@@ -739,6 +739,7 @@ size_t pass_smem_bytes(const PassArgs& A, int real_bytes) {
 }
 
 cudaError_t launch_pass(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  if (A.fast == 4) return launch_mr_bs(A, real_bytes, stream);
   if (A.fast == 3) return launch_mr_r2r(A, real_bytes, stream);
   if (A.fast == 2) return launch_mr(A, real_bytes, stream);
   if (A.fast) return launch_pow2(A, real_bytes, stream);

@@ -1096,7 +1096,8 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
   if (A.fast && !P.force_generic) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int occ = A.fast == 3   ? mr_r2r_occupancy(A.m, P.real_bytes)
+    const int occ = A.fast == 4   ? mr_bs_occupancy(A.bs_m2, P.real_bytes)
+                    : A.fast == 3 ? mr_r2r_occupancy(A.m, P.real_bytes)
                     : A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
                     : A.half      ? pow2_half_occupancy(A.m, A.kind)
                                   : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig == 1, P.real_bytes);
@@ -1247,6 +1248,21 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
       A.dst_k_contig = direct ? 1 : 0;
       // a pair of lines per FFT sequence; the type-IV kinds take a sequence per line
       L = mr_r2r_lines(A.m, in_complex ? 1 : 0, P.real_bytes) / (iv4 ? 2 : 1);
+      A.lines = L;
+    }
+  }
+  // Bluestein lengths (a prime factor above 31) of C2C passes on the
+  // mixed-radix kernel: the convolution's two power-of-two FFTs in registers
+  // and shared memory; contiguous source lines, direct or transposed store
+  if (!A.fast && !P.force_generic && op.kind == P_C2C && A.bs_m2 && mr_bs_supported(A.bs_m2, P.real_bytes) &&
+      src.perm[N - 1] == a && src.split_of(a) < 0) {
+    const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
+    const int ta = dst.split_of(a);
+    const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
+    if (direct || transposed) {
+      A.fast = 4;
+      A.dst_k_contig = direct ? 1 : 0;
+      L = mr_bs_lines(A.bs_m2, P.real_bytes);
       A.lines = L;
     }
   }
@@ -2120,7 +2136,7 @@ int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int3
     const Program& prog = plan->prog[user_mode(*plan, op)];
     int n = 0;
     for (const Step& s : prog.steps) {
-      const int k = s.type != 0 ? 1 : (s.pa.fast == 1 ? 2 : (s.pa.fast >= 2 ? 3 : 0));
+      const int k = s.type != 0 ? 1 : (s.pa.fast == 1 ? 2 : (s.pa.fast == 4 ? 4 : (s.pa.fast >= 2 ? 3 : 0)));
       if (kernels && n < capacity) kernels[n] = k;
       ++n;
     }
@@ -4261,7 +4277,8 @@ static std::string reg_key(const PassArgs& A, int real_bytes) {
 }
 
 static int reg_occupancy(const PassArgs& A, int real_bytes, int sched) {
-  return A.fast == 3   ? mr_r2r_occupancy(A.m, real_bytes)
+  return A.fast == 4   ? mr_bs_occupancy(A.bs_m2, real_bytes)
+         : A.fast == 3 ? mr_r2r_occupancy(A.m, real_bytes)
          : A.fast == 2 ? mr_occupancy(A.m, real_bytes, sched)
          : A.half      ? pow2_half_occupancy(A.m, A.kind)
                        : pow2_occupancy(A.m, A.kind, A.inv, A.dst_k_contig == 1, real_bytes);
@@ -4412,7 +4429,7 @@ int pb_plan_step_config(const pb_plan* plan, int32_t op, int32_t step, pb_step_c
     }
     const PassArgs& A = st.pa;
     const int sms = sm_count();
-    out->kernel = A.fast == 1 ? 2 : (A.fast == 2 || A.fast == 3) ? 3 : 0;
+    out->kernel = A.fast == 1 ? 2 : (A.fast == 2 || A.fast == 3) ? 3 : (A.fast == 4 ? 4 : 0);
     out->fft_len = A.m;
     out->lines = A.lines;
     out->grid_ctas = A.fast ? (int)std::min<long long>(A.grid_ctas, A.ntiles) : 0;
@@ -4428,6 +4445,8 @@ int pb_plan_step_config(const pb_plan* plan, int32_t op, int32_t step, pb_step_c
       out->nradix = mr_r2r_radices(A.m, plan->real_bytes, out->radix, 12);
     else if (A.fast == 1)
       out->nradix = pow2_radices(A.m, out->radix, 12);
+    else if (A.fast == 4)
+      out->nradix = pow2_radices(A.bs_m2, out->radix, 12);
     else {
       out->nradix = std::min(A.nstages, 12);
       for (int i = 0; i < out->nradix; ++i) out->radix[i] = A.radix[i];

@@ -316,12 +316,14 @@ class _Plan:
 
     def step_kernels(self, op) -> list:
         """Kernel family of each launch of one operation: "generic", "check",
-        "pow2" (register-resident power-of-two pass) or "mixed_radix"."""
+        "pow2" (register-resident power-of-two pass), "mixed_radix" or
+        "bluestein" (a C2C length with a prime factor above 31 on the
+        mixed-radix kernel)."""
         cap = 64
         ks = (C.c_int32 * cap)()
         cnt = C.c_int32()
         L.check(L.load().pb_plan_step_kernels(self._h, op, ks, cap, C.byref(cnt)), "step kernels")
-        names = ("generic", "check", "pow2", "mixed_radix")
+        names = ("generic", "check", "pow2", "mixed_radix", "bluestein")
         return [names[ks[i]] for i in range(cnt.value)]
 
     # in-place single-allocation arrays (C2cInPlaceArray / R2cInPlaceArray)
@@ -371,7 +373,7 @@ class _Plan:
         """Per launch of `op`: kernel family, FFT length, lines per tile,
         persistent grid, CTAs per SM, schedule, radices and whether the
         autotuner chose it."""
-        names = ("generic", "check", "pow2", "mixed_radix")
+        names = ("generic", "check", "pow2", "mixed_radix", "bluestein")
         out = []
         for i in range(len(self.step_kinds(op))):
             c = L.PbStepConfig()

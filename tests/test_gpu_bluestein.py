@@ -1,9 +1,11 @@
-"""Lengths with a prime factor above 31 on the generic kernel: the FFT core
-runs Bluestein's chirp-z form (the m-point DFT as a cyclic convolution over a
-power-of-two FFT) instead of an O(p) radix.  C2C, R2C / C2R and the
-real-to-real kinds whose FFT length has such a factor (DCT-II of 101, DST-I of
-100 -> 202 = 2 * 101, DHT of 67, DCT-IV of 94 -> 47), f32 and f64, against the
-oracle's float64 DFT within the usual bound."""
+"""Lengths with a prime factor above 31 run Bluestein's chirp-z form (the
+m-point DFT as a cyclic convolution over a power-of-two FFT) instead of an
+O(p) radix: C2C passes over contiguous lines on the mixed-radix kernel
+("bluestein", convolution lengths up to 1024), everything else in the generic
+kernel's FFT core -- strided C2C lines, R2C / C2R and the real-to-real kinds
+whose FFT length has such a factor (DCT-II of 101, DST-I of 100 -> 202 =
+2 * 101, DHT of 67, DCT-IV of 94 -> 47).  f32 and f64, against the oracle's
+float64 DFT within the usual bound."""
 
 import numpy as np
 import pytest
@@ -26,24 +28,33 @@ C2C_CASES = [((2, 2), (37, 12, 41)), ((2, 3), (101, 8, 10)), ((1, 3), (9, 6, 257
              ((2, 1), (12, 514, 5))]
 
 
-def _bluestein_steps(plan, op):
-    """Launches of `op` on the generic kernel whose radices are all powers of
-    two although their FFT length is not (the Bluestein form)."""
+def _bluestein_steps(plan, op, kernels=("generic", "bluestein")):
+    """Launches of `op` whose radices are all powers of two although their FFT
+    length is not (the Bluestein form), on the given kernel families."""
     out = []
     for c in plan.step_configs(op):
         n = c["fft_len"]
-        if c["kernel"] == "generic" and n & (n - 1) and c["radices"] and all(r in (2, 4, 8) for r in c["radices"]):
+        if c["kernel"] in kernels and n & (n - 1) and c["radices"] and all(r in (2, 4, 8) for r in c["radices"]):
             out.append(n)
     return out
 
 
+@pytest.mark.parametrize("permute", [True, False])
 @pytest.mark.parametrize("rb", [4, 8])
 @pytest.mark.parametrize("dims,shape", C2C_CASES)
-def test_c2c_prime_lengths(rb, dims, shape):
+def test_c2c_prime_lengths(rb, dims, shape, permute):
+    """permute_dims = true: the contiguous C2C passes take the mixed-radix
+    Bluestein kernel (up to 512 points; 1021 needs a 2048-point convolution
+    and stays on the generic kernel); false: strided lines, the generic
+    kernel's Bluestein core."""
     rng = np.random.default_rng(31)
-    plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), dtype=CDT[rb])
+    lay = pb.DistributedLayout(permute)
+    plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), layout=lay, dtype=CDT[rb])
     assert _bluestein_steps(plan, L.FORWARD), plan.step_configs(L.FORWARD)
-    route = po.c2c_route(po.Topology(dims), shape)
+    if permute and max(shape) <= 512:
+        for op in (L.FORWARD, L.INVERSE):
+            assert _bluestein_steps(plan, op, ("bluestein",)), plan.step_configs(op)
+    route = po.c2c_route(po.Topology(dims), shape, None, permute)
     x = rand_field(rng, shape, (), True, rb)
     for d in ("fwd", "inv", "bwd"):
         check_transform(plan, route, x, 1, rb, True, d)
