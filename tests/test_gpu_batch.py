@@ -198,3 +198,34 @@ def test_batch_mode_switches_and_the_legacy_stream():
     assert all(torch.equal(o, r) for o, r in zip(outs, refs))
     with pytest.raises(pb.PencilError):
         batch.set_mode("branches", 17)
+
+
+@pytest.mark.parametrize("mode", ["queue", "branches"])
+def test_batch_with_bluestein_lengths(mode):
+    """Grids whose axes have prime factors above 31: the queue kernel's generic
+    tiles run the Bluestein form of the FFT core, the branch mode the plans'
+    own passes (the mixed-radix Bluestein kernel for contiguous C2C lines);
+    both against per-plan execution and the oracle's float64 DFT."""
+    rng = np.random.default_rng(41)
+    cases = [((1, 1), (37, 40, 41), ()), ((2, 1), (101, 12, 10), (2,)), ((1, 2), (9, 127, 8), ())]
+    plans, xs = [], []
+    for dims, shape, extra in cases:
+        plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, extra, dtype=torch.complex64)
+        e = int(np.prod(extra)) if extra else 1
+        x = rng.standard_normal((e,) + shape) + 1j * rng.standard_normal((e,) + shape)
+        xs.append(to_device(po.flat_concat(po.scatter(oracle_pencil(plan.input_pencil), x, (e,))), torch.complex64))
+        plans.append(plan)
+    batch = pb.PlanBatch(plans, ("forward",), mode=mode)
+    ws = batch.allocate_workspace()
+    outs = [p.allocate_output() for p in plans]
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        batch.execute([xs, outs], ws, stream)
+        batch.status(ws, stream)
+    torch.cuda.synchronize()
+    for plan, x, out, (dims, shape, extra) in zip(plans, xs, outs, cases):
+        e = int(np.prod(extra)) if extra else 1
+        route = po.c2c_route(po.Topology(dims), shape)
+        locs = po.split_flat(oracle_pencil(plan.input_pencil), to_host(x).astype(np.complex128), e)
+        exp = po.flat_concat(po.execute_forward(route, locs))
+        assert rel_l2(to_host(out), exp) <= fft_bound(4, int(np.prod(shape))), (mode, shape)
