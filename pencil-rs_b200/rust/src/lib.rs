@@ -971,3 +971,95 @@ pub fn read_field<T>(path: &str, pencil: &Pencil, extra: &[usize], scalar: i32, 
         sys::pb_field_read(c.as_ptr(), &pencil.desc, e.len() as i32, e.as_ptr(), scalar, data.as_mut_ptr() as *mut c_void, ptr::null_mut())
     })
 }
+
+// ---------------------------------------------------------------------------
+// ragged batches (the collections' forward_many, many plans in one launch)
+// ---------------------------------------------------------------------------
+
+/// Execution mode of a [`PlanBatch`].
+#[derive(Clone, Copy, Debug, PartialEq, Eq)]
+pub enum BatchMode {
+    /// One graph of the member plans' own pass kernels on `n` parallel branches.
+    Branches(i32),
+    /// One persistent kernel over a level-ordered work queue.
+    Queue,
+}
+
+/// A ragged batch: any plans of one precision and one operation chain (e.g.
+/// forward then inverse), run as one CUDA graph launch per execution on a
+/// non-default stream (`forward_many`, collections.rs:164-206, is a loop over
+/// one plan's arrays).  The plans must outlive the batch.
+pub struct PlanBatch {
+    raw: *mut sys::pb_batch,
+    count: usize,
+    nops: usize,
+    workspace_bytes: usize,
+}
+
+unsafe impl Send for PlanBatch {}
+
+impl PlanBatch {
+    /// `plans` as raw handles of the plan types (`Transform::raw_handle`);
+    /// `ops` from `sys::PB_FORWARD` / `PB_INVERSE` / `PB_BACKWARD`.
+    pub fn new(plans: &[*mut sys::pb_plan], ops: &[i32], autotune: bool) -> Result<Self> {
+        let mut raw: *mut sys::pb_batch = ptr::null_mut();
+        check(unsafe {
+            sys::pb_batch_create(plans.as_ptr(), plans.len() as i32, ops.as_ptr(), ops.len() as i32,
+                                 if autotune { 1 } else { 0 }, &mut raw)
+        })?;
+        let mut b = PlanBatch { raw, count: plans.len(), nops: ops.len(), workspace_bytes: 0 };
+        b.refresh_workspace()?;
+        Ok(b)
+    }
+
+    fn refresh_workspace(&mut self) -> Result<()> {
+        let mut bytes = 0i64;
+        check(unsafe { sys::pb_batch_workspace_bytes(self.raw, &mut bytes) })?;
+        self.workspace_bytes = bytes as usize;
+        Ok(())
+    }
+
+    /// Selects the mode; the workspace size may change with it.
+    pub fn set_mode(&mut self, mode: BatchMode) -> Result<()> {
+        let (m, n) = match mode {
+            BatchMode::Branches(n) => (sys::PB_BATCH_BRANCHES, n),
+            BatchMode::Queue => (sys::PB_BATCH_QUEUE, 1),
+        };
+        check(unsafe { sys::pb_batch_set_mode(self.raw, m, n) })?;
+        self.refresh_workspace()
+    }
+
+    pub fn workspace_bytes(&self) -> usize {
+        self.workspace_bytes
+    }
+
+    /// `buffers[k * count + i]`: plan i's input of op k and output of op k-1
+    /// (device pointers, `(ops + 1) * count` of them).
+    pub fn execute(&mut self, buffers: &[*mut c_void], workspace: &mut DeviceBuffer<u8>, stream: Stream) -> Result<()> {
+        if buffers.len() != (self.nops + 1) * self.count || workspace.len() < self.workspace_bytes {
+            return Err(Error(sys::PB_EINVALID_ARGUMENT));
+        }
+        check(unsafe {
+            sys::pb_batch_execute(self.raw, buffers.as_ptr(), workspace.as_mut_ptr() as *mut c_void, stream.0)
+        })
+    }
+
+    /// Waits for `stream`; `PB_ETIMEOUT` if a dependency wait of the queue
+    /// kernel gave up.
+    pub fn status(&mut self, workspace: &mut DeviceBuffer<u8>, stream: Stream) -> Result<()> {
+        check(unsafe { sys::pb_batch_status(self.raw, workspace.as_mut_ptr() as *mut c_void, stream.0) })
+    }
+}
+
+impl Drop for PlanBatch {
+    fn drop(&mut self) {
+        unsafe { sys::pb_batch_destroy(self.raw) };
+    }
+}
+
+impl<I: Copy + Default, O: Copy + Default> Transform<I, O> {
+    /// The plan's C-ABI handle, for [`PlanBatch::new`].
+    pub fn raw_handle(&self) -> *mut sys::pb_plan {
+        self.core.raw
+    }
+}
