@@ -2,7 +2,8 @@
 // prime factor above 31, contiguous in the source, direct or transposed store.
 // The m-point DFT is X_k = w_k * sum_j (x_j w_j) conj(w)_{k-j} with
 // w_j = exp(-+i pi j^2 / m) (the pass's sign, A.bs_chirp); the sum is a cyclic
-// convolution of length N = A.bs_m2 (a power of two >= 2m - 1).  One tile of
+// convolution of length N = A.bs_m2 (the smallest of kBluesteinLengths
+// >= 2m - 1).  One tile of
 // NSEQ lines runs, without leaving shared memory:
 //   * the stage-0 load of the lines times the chirp, zero past m (registers);
 //   * the forward N-point Stockham FFT (mr_stage0, mr_stages_upto);
@@ -116,10 +117,11 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
   }
 }
 
-// f32 up to 512 points: three CTAs per SM (80 registers, no spills); a
-// tile's ten or so barriers leave the SM idle at two.
+// Resident CTAs per SM as for the C2C kernel of the same length (three in
+// f32 up to 512 points where the default schedule does not spill at 80
+// registers): a tile's ten or so barriers leave the SM idle at two.
 template <typename R, int N>
-__global__ void __launch_bounds__(MR_THREADS, (sizeof(R) == 4 && N <= 512) ? 3 : 2) mr_bs_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(MR_THREADS, mr_min_ctas((int)sizeof(R), N, 0)) mr_bs_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
   mr_run<R, N, false, false, false, 0, true>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);

@@ -57,6 +57,15 @@ __host__ __device__ constexpr int mr_r2r_min_ctas(int real_bytes, int N) {
 __host__ __device__ constexpr int mr_r2r_table_len(int N) { return N <= 512 ? 2 * N : N; }
 constexpr int MR_GROUPS = 8;
 
+// Convolution lengths of Bluestein passes up to 1024 points: the smallest entry
+// >= 2m - 1 is taken (powers of two and 7-smooth lengths between them, so
+// that the convolution stays within about 1.8x of 2m); mr_bs.cuh is
+// instantiated for each.  Longer convolutions (generic kernel only) are powers
+// of two.
+constexpr int kBluesteinLengths[] = {80,  96,  112, 128, 160, 192, 224, 256, 288,
+                                     320, 384, 448, 512, 576, 640, 768, 896, 1024};
+constexpr int kBluesteinCount = sizeof(kBluesteinLengths) / sizeof(kBluesteinLengths[0]);
+
 // Lengths whose passes the persistent batch kernel (pass_kernel.cu) runs with
 // the mixed-radix tile code, f32 only: the 7-smooth numbers in [32, 256],
 // powers of two included.  Other passes of a batch take the generic tile code.

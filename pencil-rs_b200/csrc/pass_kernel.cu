@@ -13,7 +13,7 @@
 // butterflies plus an O(R) generic radix for other primes, twiddles from a
 // table of m-th roots of unity generated on the host in extended precision
 // and rounded once to the plan type; lengths with a prime factor above 31
-// take Bluestein's chirp-z form over a power-of-two FFT (fft_run).  R2C/C2R
+// take Bluestein's chirp-z form over a 7-smooth FFT (fft_run).  R2C/C2R
 // use the two-real-lines-in-one-complex-FFT split; DCT/DST II/III use
 // Makhoul's n-point reordering with pre/post twiddles; DCT/DST IV use an
 // n/2-point complex FFT (even n); type I
@@ -117,7 +117,7 @@ __device__ C* fft_stages(C* b0, C* b1, int nseq, int m, int ld, const C* W, cons
 
 // The m-point FFT of nseq sequences in b0 (element j of sequence s at
 // s*ld + j), result in the returned buffer.  Direct Stockham stages, or for
-// A.bs_m2 > 0 Bluestein's chirp-z form: with w_j = exp(-+i pi j^2/m) (the
+// A.bs_m2 > 0 Bluestein's chirp-z form (M = bs_m2, 7-smooth): with w_j = exp(-+i pi j^2/m) (the
 // pass's sign, A.bs_chirp), X_k = w_k * sum_j (x_j w_j) conj(w)_{k-j}, the
 // sum a cyclic convolution of length M = bs_m2 computed as a forward M-point
 // FFT, a product with the precomputed transform of the conjugate chirp
@@ -128,18 +128,18 @@ __device__ C* fft_run(C* b0, C* b1, int nseq, int m, int ld, const C* W, const P
   if (A.bs_m2 == 0) return fft_stages<C, INV>(b0, b1, nseq, m, ld, W, A);
   using R = decltype(W[0].x);
   const int M = A.bs_m2;
-  const int lg = __ffs(M) - 1;
+  const unsigned mM = fdiv_magic(M);
   const C* __restrict__ chirp = reinterpret_cast<const C*>(A.bs_chirp);
   const C* __restrict__ ker = reinterpret_cast<const C*>(A.bs_kernel);
   const int total = nseq * M;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int s = t >> lg, j = t & (M - 1);
+    const int s = (int)fdiv(t, M, mM), j = t - s * M;
     b1[s * ld + j] = j < m ? cmul(b0[s * ld + j], chirp[j]) : mk<C, R>(R(0), R(0));
   }
   __syncthreads();
   C* f = fft_stages<C, false>(b1, b0, nseq, M, ld, W, A);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int s = t >> lg, j = t & (M - 1);
+    const int s = (int)fdiv(t, M, mM), j = t - s * M;
     f[s * ld + j] = cmul(f[s * ld + j], ker[j]);
   }
   __syncthreads();

@@ -120,7 +120,7 @@ cudaError_t launch_mr_r2r(const PassArgs& A, int real_bytes, cudaStream_t stream
 int mr_r2r_lines(int m, int complex_data, int real_bytes);
 int mr_r2r_occupancy(int m, int real_bytes);
 // Bluestein C2C passes on the mixed-radix kernel (mr_bs.cuh): convolution
-// length M = A.bs_m2 in 64 .. 1024
+// length M = A.bs_m2 one of kBluesteinLengths
 bool mr_bs_supported(int M, int real_bytes);
 cudaError_t launch_mr_bs(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int mr_bs_lines(int M, int real_bytes);

@@ -116,10 +116,9 @@ struct PassArgs {
   int grid_ctas;          // persistent grid size
   int sched;              // mixed-radix schedule: 0 default, 1 radices up to 8 (autotuner)
   int batch_chunk;        // batch kernel: tiles per work item
-  // Bluestein (chirp-z) form of the generic kernel's FFT, for lengths m with a
-  // large prime factor: the m-point DFT as a cyclic convolution of length
-  // bs_m2 (a power of two >= 2m - 1); radix[] / nstages / twiddle then
-  // describe the bs_m2-point FFT
+  // Bluestein (chirp-z) form of the FFT, for lengths m with a large prime
+  // factor: the m-point DFT as a cyclic convolution of length bs_m2 (7-smooth,
+  // >= 2m - 1); radix[] / nstages / twiddle then describe the bs_m2-point FFT
   int bs_m2;              // 0: direct FFT of length m
   const void* bs_chirp;   // m entries exp(-+i pi j^2 / m), the sign of the pass's direction
   const void* bs_kernel;  // bs_m2 entries: the DFT of the conjugate chirp (periodic), / bs_m2

@@ -718,6 +718,8 @@ static int bluestein_len(int m, int real_bytes) {
     }
   big = std::max(big, r);
   if (big <= 31) return 0;
+  for (int L : kBluesteinLengths)
+    if (L >= 2 * m - 1) return L;
   int M = 1;
   while (M < 2 * m - 1) M <<= 1;
   return M <= (real_bytes == 4 ? 4096 : 2048) ? M : 0;
@@ -751,7 +753,8 @@ static size_t chirp_table(pb_plan& P, int m, int inv) {
 
 // The DFT (negative exponent) of the M-periodic conjugate chirp b_j =
 // conj(w_j), b_{M-j} = b_j (0 < j < m), zero elsewhere, divided by M: the
-// convolution's kernel.  Radix-2 FFT in long double, rounded once.
+// convolution's kernel.  In long double, rounded once: a radix-2 FFT for
+// powers of two, else the direct sum with exact angle indices (j k mod M).
 static size_t bluestein_kernel_table(pb_plan& P, int m, int M, int inv) {
   const std::string key =
       "BK" + std::to_string(m) + "_" + std::to_string(M) + "i" + std::to_string(inv) + "r" + std::to_string(P.real_bytes);
@@ -769,6 +772,29 @@ static size_t bluestein_kernel_table(pb_plan& P, int m, int M, int inv) {
       im[M - j] = im[j];
     }
   }
+  if (M & (M - 1)) {
+    std::vector<long double> cs(M), sn(M);
+    for (int q = 0; q < M; ++q) {
+      cs[q] = cosl(2.0L * pi * (long double)q / (long double)M);
+      sn[q] = sinl(2.0L * pi * (long double)q / (long double)M);
+    }
+    std::vector<long double> fr(M, 0.0L), fi(M, 0.0L);
+    for (int k = 0; k < M; ++k) {
+      long double ar = 0.0L, ai = 0.0L;
+      int q = 0;  // j k mod M
+      for (int j = 0; j < M; ++j) {
+        // (re + i im) * exp(-2 pi i q / M)
+        ar += re[j] * cs[q] + im[j] * sn[q];
+        ai += im[j] * cs[q] - re[j] * sn[q];
+        q += k;
+        if (q >= M) q -= M;
+      }
+      fr[k] = ar;
+      fi[k] = ai;
+    }
+    re.swap(fr);
+    im.swap(fi);
+  } else {
   // bit-reversal permutation, then iterative butterflies
   for (int i = 1, j = 0; i < M; ++i) {
     int bit = M >> 1;
@@ -791,6 +817,7 @@ static size_t bluestein_kernel_table(pb_plan& P, int m, int M, int inv) {
         re[a] += xr;
         im[a] += xi;
       }
+  }
   }
   std::vector<double> d(2 * (size_t)M);
   for (int k = 0; k < M; ++k) {
@@ -4445,8 +4472,7 @@ int pb_plan_step_config(const pb_plan* plan, int32_t op, int32_t step, pb_step_c
       out->nradix = mr_r2r_radices(A.m, plan->real_bytes, out->radix, 12);
     else if (A.fast == 1)
       out->nradix = pow2_radices(A.m, out->radix, 12);
-    else if (A.fast == 4)
-      out->nradix = pow2_radices(A.bs_m2, out->radix, 12);
+
     else {
       out->nradix = std::min(A.nstages, 12);
       for (int i = 0; i < out->nradix; ++i) out->radix[i] = A.radix[i];

@@ -29,12 +29,13 @@ C2C_CASES = [((2, 2), (37, 12, 41)), ((2, 3), (101, 8, 10)), ((1, 3), (9, 6, 257
 
 
 def _bluestein_steps(plan, op, kernels=("generic", "bluestein")):
-    """Launches of `op` whose radices are all powers of two although their FFT
-    length is not (the Bluestein form), on the given kernel families."""
+    """Launches of `op` in the Bluestein form on the given kernel families:
+    their radices describe the convolution length (7-smooth, >= 2m - 1), not
+    the FFT length m."""
     out = []
     for c in plan.step_configs(op):
-        n = c["fft_len"]
-        if c["kernel"] in kernels and n & (n - 1) and c["radices"] and all(r in (2, 4, 8) for r in c["radices"]):
+        n, rad = c["fft_len"], c["radices"]
+        if c["kernel"] in kernels and rad and int(np.prod(rad)) >= 2 * n - 1 and max(rad) <= 8:
             out.append(n)
     return out
 
