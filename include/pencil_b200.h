@@ -210,7 +210,7 @@ int pb_plan_steps(const pb_plan* plan, int32_t op, int32_t* kinds, int32_t capac
 /* Kernel family of each launch of one operation, in order: 0 = generic fused
  * pass (shared-memory Stockham, any length and kind), 1 = C2R spectrum check,
  * 2 = register-resident power-of-two pass, 3 = register-fed mixed-radix pass
- * (7-smooth lengths), 4 = Bluestein C2C pass on the mixed-radix kernel
+ * (7-smooth lengths), 4 = Bluestein C2C / R2C / C2R pass on the mixed-radix kernel
  * (lengths with a prime factor above 31).  A diagnostic with no counterpart
  * in the reference. */
 int pb_plan_step_kernels(const pb_plan* plan, int32_t op, int32_t* kernels, int32_t capacity, int32_t* count);

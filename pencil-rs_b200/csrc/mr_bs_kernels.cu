@@ -1,8 +1,14 @@
 // Instantiations of the Bluestein pass on the mixed-radix kernel (mr_bs.cuh):
 // the convolution lengths of kBluesteinLengths (80 .. 1024, line lengths up
-// to 512), f32 and f64.
+// to 512), f32 and f64.  Compiled once per kind, BS_KIND 1 (C2C) and 2 (R2C /
+// C2R), so the two builds run in parallel; the kind-independent entry points
+// live in the C2C object.
 #include "mr_bs.cuh"
 #include "pb_aux.hpp"
+
+#ifndef BS_KIND
+#define BS_KIND 1
+#endif
 
 namespace pb {
 
@@ -12,7 +18,7 @@ template <typename R, int I = 0>
 cudaError_t bs_launch_r(const PassArgs& A, cudaStream_t stream) {
   if constexpr (I < kBluesteinCount) {
     constexpr int N = kBluesteinLengths[I];
-    if (A.bs_m2 == N) return mr_bs_launch<R, N>(A, stream);
+    if (A.bs_m2 == N) return mr_bs_launch<R, N, BS_KIND>(A, stream);
     return bs_launch_r<R, I + 1>(A, stream);
   } else {
     return cudaErrorInvalidValue;
@@ -23,13 +29,14 @@ template <typename R, int I = 0>
 int bs_occ_r(int M) {
   if constexpr (I < kBluesteinCount) {
     constexpr int N = kBluesteinLengths[I];
-    if (M == N) return mr_bs_occ<R, N>();
+    if (M == N) return mr_bs_occ<R, N, BS_KIND>();
     return bs_occ_r<R, I + 1>(M);
   } else {
     return 1;
   }
 }
 
+#if BS_KIND == 1
 template <typename R, int I = 0>
 int bs_lines_r(int M) {
   if constexpr (I < kBluesteinCount) {
@@ -40,9 +47,21 @@ int bs_lines_r(int M) {
     return 0;
   }
 }
+#endif
 
 }  // namespace
 
+template <>
+cudaError_t launch_mr_bs_kind<BS_KIND>(const PassArgs& A, int real_bytes, cudaStream_t stream) {
+  return real_bytes == 4 ? bs_launch_r<float>(A, stream) : bs_launch_r<double>(A, stream);
+}
+
+template <>
+int mr_bs_kind_occupancy<BS_KIND>(int M, int real_bytes) {
+  return real_bytes == 4 ? bs_occ_r<float>(M) : bs_occ_r<double>(M);
+}
+
+#if BS_KIND == 1
 bool mr_bs_supported(int M, int real_bytes) {
   (void)real_bytes;
   for (int n : kBluesteinLengths)
@@ -52,12 +71,16 @@ bool mr_bs_supported(int M, int real_bytes) {
 
 int mr_bs_lines(int M, int real_bytes) { return real_bytes == 4 ? bs_lines_r<float>(M) : bs_lines_r<double>(M); }
 
-int mr_bs_occupancy(int M, int real_bytes) { return real_bytes == 4 ? bs_occ_r<float>(M) : bs_occ_r<double>(M); }
+int mr_bs_occupancy(int M, int kind, int real_bytes) {
+  return kind == P_C2C ? mr_bs_kind_occupancy<1>(M, real_bytes) : mr_bs_kind_occupancy<2>(M, real_bytes);
+}
 
 cudaError_t launch_mr_bs(const PassArgs& A, int real_bytes, cudaStream_t stream) {
   if (A.ntiles <= 0) return cudaSuccess;
   if (A.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
-  return real_bytes == 4 ? bs_launch_r<float>(A, stream) : bs_launch_r<double>(A, stream);
+  if (A.kind != P_C2C && A.kind != P_R2C && A.kind != P_C2R) return cudaErrorInvalidValue;
+  return A.kind == P_C2C ? launch_mr_bs_kind<1>(A, real_bytes, stream) : launch_mr_bs_kind<2>(A, real_bytes, stream);
 }
+#endif
 
 }  // namespace pb

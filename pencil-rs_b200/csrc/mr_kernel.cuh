@@ -660,22 +660,23 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
                                             PieceAddr* prow, const PieceAddr& my_piece, int npieces);
 
 // Bluestein lengths (mr_bs.cuh): the chirp-premultiplied load and the
-// convolution tile of an N-point (power-of-two) Bluestein pass.
-template <typename R, int N>
+// convolution tile of a Bluestein pass with an N-point (7-smooth) convolution;
+// K 1 for C2C, 2 for R2C / C2R.
+template <typename R, int N, int K>
 __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            const PassArgs& A, const TileAddr& ta);
-template <typename R, int N>
+template <typename R, int N, int K>
 __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta,
                                            typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
                                            long long* Atab, const int2* ktab, PieceAddr* prow,
                                            const PieceAddr& my_piece, int npieces);
 
-template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false, int S = 0, bool BS = false>
+template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false, int S = 0, int BS = 0>
 __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
                                        unsigned char* smem, bool setup) {
   static_assert(!R2R || S == 0, "the real-to-real kinds run the default schedule");
-  static_assert(!BS || (!R2R && !SX && !DS && S == 0), "Bluestein passes: C2C, contiguous lines");
+  static_assert(BS == 0 || (!R2R && !SX && !DS && S == 0), "Bluestein passes: contiguous lines");
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N, S>;
   constexpr int BUF = G::NSEQ * G::SEQ;
@@ -691,7 +692,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   if (tile >= end) return;
   const int tid = threadIdx.x;
   const bool direct = A.dst_k_contig == 1;  // 2 (split direct store) reads the row tables
-  const int nout = (R2R || BS) ? A.n_out : ((A.kind == P_R2C) ? N / 2 + 1 : N);
+  const int nout = (R2R || BS != 0) ? A.n_out : ((A.kind == P_R2C) ? N / 2 + 1 : N);
   const TileAddr* tiles = reinterpret_cast<const TileAddr*>(A.tile_tab);
   const PieceAddr* pieces = reinterpret_cast<const PieceAddr*>(A.piece_tab);
   const int npieces = direct ? 0 : A.npieces;
@@ -702,8 +703,8 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   }
   TileAddr ta = load_tile(tiles, tile);
   C v[G::U0][G::R0];
-  if constexpr (BS)
-    mr_load_bs<R, N>(v, A, ta);
+  if constexpr (BS != 0)
+    mr_load_bs<R, N, BS>(v, A, ta);
   else if constexpr (R2R)
     mr_load_r2r<R, N, SX>(v, A, ta);
   else
@@ -720,8 +721,8 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
     PieceAddr next_piece{0, 0};
     C nv[G::U0][G::R0];
     if (has_next) {
-      if constexpr (BS)
-        mr_load_bs<R, N>(nv, A, t1);
+      if constexpr (BS != 0)
+        mr_load_bs<R, N, BS>(nv, A, t1);
       else if constexpr (R2R)
         mr_load_r2r<R, N, SX>(nv, A, t1);
       else
@@ -729,8 +730,8 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
       if (tile + 2 * step < end) t2 = load_tile(tiles, tile + 2 * step);
       if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
-    if constexpr (BS) {
-      mr_tile_bs<R, N>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+    if constexpr (BS != 0) {
+      mr_tile_bs<R, N, BS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     } else if constexpr (R2R) {
       if (A.inv)
         mr_tile_r2r<R, N, true, SX>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);

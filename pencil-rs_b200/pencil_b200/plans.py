@@ -317,8 +317,8 @@ class _Plan:
     def step_kernels(self, op) -> list:
         """Kernel family of each launch of one operation: "generic", "check",
         "pow2" (register-resident power-of-two pass), "mixed_radix" or
-        "bluestein" (a C2C length with a prime factor above 31 on the
-        mixed-radix kernel)."""
+        "bluestein" (a C2C / R2C / C2R length with a prime factor above 31 on
+        the mixed-radix kernel)."""
         cap = 64
         ks = (C.c_int32 * cap)()
         cnt = C.c_int32()

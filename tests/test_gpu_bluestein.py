@@ -1,9 +1,9 @@
 """Lengths with a prime factor above 31 run Bluestein's chirp-z form (the
-m-point DFT as a cyclic convolution over a power-of-two FFT) instead of an
-O(p) radix: C2C passes over contiguous lines on the mixed-radix kernel
-("bluestein", convolution lengths up to 1024), everything else in the generic
-kernel's FFT core -- strided C2C lines, R2C / C2R and the real-to-real kinds
-whose FFT length has such a factor (DCT-II of 101, DST-I of 100 -> 202 =
+m-point DFT as a cyclic convolution over a 7-smooth FFT) instead of an O(p)
+radix: C2C, R2C and C2R passes over contiguous lines on the mixed-radix
+kernel ("bluestein", convolution lengths up to 1024), everything else in the
+generic kernel's FFT core -- strided lines, longer lines and the real-to-real
+kinds whose FFT length has such a factor (DCT-II of 101, DST-I of 100 -> 202 =
 2 * 101, DHT of 67, DCT-IV of 94 -> 47).  f32 and f64, against the oracle's
 float64 DFT within the usual bound."""
 
@@ -68,6 +68,9 @@ def test_r2c_prime_lengths(rb, dims, shape, extra):
     e = int(np.prod(extra)) if extra else 1
     plan = pb.R2cPlan.from_shape(pb.MpiTopology(dims), shape, extra, dtype=RDT[rb])
     assert _bluestein_steps(plan, L.FORWARD) and _bluestein_steps(plan, L.INVERSE)
+    # every Bluestein pass of these routes has contiguous lines: the mixed-radix kernel
+    for op in (L.FORWARD, L.INVERSE):
+        assert _bluestein_steps(plan, op) == _bluestein_steps(plan, op, ("bluestein",)), plan.step_configs(op)
     route = po.r2c_route(po.Topology(dims), shape)
     x = rand_field(rng, shape, extra, False, rb)
     check_transform(plan, route, x, e, rb, False, "fwd")
