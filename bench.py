@@ -506,10 +506,12 @@ def b200_arm(args):
     kinds_f = plan.step_kinds(L.FORWARD)
     kinds_i = plan.step_kinds(L.INVERSE)
     families = sorted(set(plan.step_kernels(L.FORWARD) + plan.step_kernels(L.INVERSE)) - {"check"})
-    kernel_names = ", ".join({"pow2": "pb::pow2_kernel<float, 512, kind, sign, store> (R2C, C2C), "
-                                      "pb::pow2_half_c2r_kernel<256> (C2R)",
+    n_pow2 = max(shape)
+    kernel_names = ", ".join({"pow2": f"pb::pow2_kernel<float, {n_pow2}, kind, sign, store> (R2C, C2C), "
+                                      f"pb::pow2_half_c2r_kernel<{n_pow2 // 2}> (C2R)",
                               "mixed_radix": "pb::mr_kernel<float, N, variant>",
-                              "generic": "pb::pass_kernel<float>"}[f] for f in families)
+                              "bluestein": "pb::mr_bs_kernel<float, M, kind class> (Bluestein)",
+                              "generic": "pb::pass_kernel<float>"}.get(f, f) for f in families)
     fwd_t, inv_t = [], []
     for _ in range(max(3, min(args.steps, 10))):
         fwd_t.append(plan.execute_timed(L.FORWARD, x, spec, ws, stream))
@@ -655,7 +657,7 @@ def b200_arm(args):
     if rank == 0:
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic_pow2_kernel_512cube.json")
-        if os.path.exists(tpath):
+        if shape == SHAPE and os.path.exists(tpath):  # captured on the 512^3 field only
             with open(tpath) as f:
                 traffic = json.load(f).get("bytes_per_launch")
         line = {
@@ -663,8 +665,9 @@ def b200_arm(args):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: field A uniform(-1,1) numpy default_rng(1); field B 16 random-phase cosines",
-            "config": {"workload": "R2C f32 [512,512,512] -> [512,512,257], 4x8 virtual pencil grid, fused "
-                                   "transpose-in-pass, forward + normalised inverse",
+            "config": {"workload": f"R2C f32 [{shape[0]},{shape[1]},{shape[2]}] -> "
+                                   f"[{shape[0]},{shape[1]},{shape[2] // 2 + 1}], {GRID[0]}x{GRID[1]} virtual "
+                                   "pencil grid, fused transpose-in-pass, forward + normalised inverse",
                        "grid": list(GRID), "shape": list(shape),
                        "l2": "no flush: every pass streams >= 512 MiB, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (each GPU runs the full field)"},

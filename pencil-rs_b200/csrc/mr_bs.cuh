@@ -224,11 +224,16 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
   }
 }
 
-// Resident CTAs per SM as for the C2C kernel of the same length (three in
-// f32 up to 512 points where the default schedule does not spill at 80
-// registers): a tile's ten or so barriers leave the SM idle at two.
+// Resident CTAs per SM: a tile's ten or so barriers leave the SM idle at two,
+// so three in f32 up to 640 points, where both kernel kinds fit 80 registers
+// without spilling (192 and 224 spill there and keep two); two in f64 and
+// beyond 640.
+__host__ __device__ constexpr int mr_bs_min_ctas(int real_bytes, int N) {
+  return (real_bytes == 4 && N <= 640 && N != 192 && N != 224) ? 3 : 2;
+}
+
 template <typename R, int N, int K>
-__global__ void __launch_bounds__(MR_THREADS, mr_min_ctas((int)sizeof(R), N, 0)) mr_bs_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(MR_THREADS, mr_bs_min_ctas((int)sizeof(R), N)) mr_bs_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
   mr_run<R, N, false, false, false, 0, K>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);

@@ -8,6 +8,7 @@ library is written next to this file so it travels with the source tree.
 from __future__ import annotations
 
 import os
+import re
 import subprocess
 import sys
 from concurrent.futures import ThreadPoolExecutor
@@ -31,8 +32,6 @@ SOURCES = ([("pass_kernel.cu", "pass_kernel.cu.o", [])]
            + [("mr_bs_kernels.cu", f"mr_bs_kernels_k{k}.o", [f"-DBS_KIND={k}"]) for k in (1, 2)]
            + [(s, s + ".o", []) for s in ("pow2_kernel.cu", "plan.cpp", "field_ops.cu", "aux_kernels.cu",
                                          "no_alloc.cu", "mr_dispatch.cpp")])
-HEADERS = ["pb_internal.hpp", "pb_aux.hpp", "pb_device.cuh", "pb_fft.cuh", "mr_kernel.cuh", "mr_lengths.hpp",
-           "smem_layout.hpp", "mr_r2r.cuh", "mr_bs.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -41,6 +40,27 @@ def nvcc() -> str:
         if cand and (os.path.sep not in cand or os.path.exists(cand)):
             return cand
     return "nvcc"
+
+
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _includes(path: str, seen=None) -> set:
+    """The project headers a source includes, directly or through other
+    headers (quoted includes found in csrc/ or include/)."""
+    seen = set() if seen is None else seen
+    with open(path) as f:
+        text = f.read()
+    for name in _INCLUDE_RE.findall(text):
+        for d in (os.path.dirname(path), CSRC, INCLUDE):
+            cand = os.path.join(d, name)
+            if os.path.exists(cand):
+                cand = os.path.abspath(cand)
+                if cand not in seen:
+                    seen.add(cand)
+                    _includes(cand, seen)
+                break
+    return seen
 
 
 def _stale(target: str, deps) -> bool:
@@ -52,13 +72,12 @@ def _stale(target: str, deps) -> bool:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "pencil_b200.h")]
     objs, cmds = [], []
     for src, oname, defs in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, oname)
         objs.append(obj)
-        if force or _stale(obj, [path] + hdrs):
+        if force or _stale(obj, [path, *sorted(_includes(path))]):
             cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
                    "-I", CSRC, *defs, "-c", path, "-o", obj]
             if src.endswith(".cu"):
