@@ -22,8 +22,12 @@
 namespace pb {
 
 // K: 1 C2C, 2 the real kinds (R2C / C2R by A.kind); kernels of their own so
-// that the C2C kernel carries none of the real kinds' load and store code
-template <typename R, int N, int K>
+// that the C2C kernel carries none of the real kinds' load and store code.
+// SX, strided lines (the source's innermost axis is the tile axis): item b is
+// butterfly b / NSEQ of sequence b % NSEQ, so the lanes read adjacent lines
+// at each position of the axis (element q of a line at q * srcq), the
+// mapping of the mixed-radix kernel's strided load.
+template <typename R, int N, int K, bool SX>
 __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            const PassArgs& A, const TileAddr& ta) {
   using C = typename Cx<R>::T;
@@ -37,9 +41,10 @@ __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::
 #pragma unroll
   for (int u = 0; u < G::U0; ++u) {
     const int b = threadIdx.x + u * MR_THREADS;
-    const int s = b / NB;
-    const int jb = b - s * NB;
+    const int s = SX ? b % G::NSEQ : b / NB;
+    const int jb = SX ? b / G::NSEQ : b - s * NB;
     const bool live = (G::B0 % MR_THREADS == 0) || b < G::B0;
+    const long long sq = SX ? ta.srcq : 1;  // element stride along the line
     if constexpr (K == 1) {
       const C* __restrict__ in = reinterpret_cast<const C*>(A.in);
       const bool ok = live && s < L;
@@ -47,7 +52,7 @@ __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::
 #pragma unroll
       for (int r = 0; r < R0; ++r) {
         const int q = jb + r * NB;
-        v[u][r] = (ok && q < m) ? cmul(in[base + q], chirp[q]) : mk<C, R>(zero, zero);
+        v[u][r] = (ok && q < m) ? cmul(in[base + q * sq], chirp[q]) : mk<C, R>(zero, zero);
       }
     } else if (A.kind == P_R2C) {  // real lines 2s, 2s+1 as x + iy
       const R* __restrict__ in = reinterpret_cast<const R*>(A.in);
@@ -57,7 +62,7 @@ __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::
 #pragma unroll
       for (int r = 0; r < R0; ++r) {
         const int q = jb + r * NB;
-        const C z = mk<C, R>((ok0 && q < m) ? in[b0 + q] : zero, (ok1 && q < m) ? in[b1 + q] : zero);
+        const C z = mk<C, R>((ok0 && q < m) ? in[b0 + q * sq] : zero, (ok1 && q < m) ? in[b1 + q * sq] : zero);
         v[u][r] = q < m ? cmul(z, chirp[q]) : mk<C, R>(zero, zero);
       }
     } else {  // C2R: the Hermitian extensions of half spectra 2s, 2s+1 as X + iY
@@ -76,8 +81,8 @@ __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::
         }
         const bool mirror = 2 * q > m;
         const int hq = mirror ? m - q : q;
-        C X = ok0 ? in[b0 + hq] : mk<C, R>(zero, zero);
-        C Y = ok1 ? in[b1 + hq] : mk<C, R>(zero, zero);
+        C X = ok0 ? in[b0 + hq * sq] : mk<C, R>(zero, zero);
+        C Y = ok1 ? in[b1 + hq * sq] : mk<C, R>(zero, zero);
         const bool edge = (hq == 0) || (2 * hq == m);
         if (mirror) {
           X.y = -X.y;
@@ -94,7 +99,7 @@ __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::
   }
 }
 
-template <typename R, int N, int K>
+template <typename R, int N, int K, bool SX, bool DS>
 __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta,
                                            typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
@@ -108,15 +113,20 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
   const int m = A.m;
   const R zero = R(0);
   // forward N-point FFT of the chirped lines
-  mr_stage0<R, N, false>(v, b0);
+  mr_stage0<R, N, false, SX>(v, b0);
   if (tid < npieces) prow[tid] = my_piece;
   __syncthreads();
-  if (!A.dst_k_contig) {
-    // destination row of each k of this tile (read after later barriers)
+  // DS: the split direct store (dst_k_contig 2) is compiled in; the
+  // transform axis stays innermost in the destination but is cut at its ranks
+  const bool dsplit = DS && A.dst_k_contig == 2;
+  if (A.dst_k_contig != 1) {
+    // destination row of each k of this tile (read after later barriers);
+    // split direct store: the offset of k in line 0, the line stride is the
+    // piece's
     for (int k = tid; k < A.n_out; k += MR_THREADS) {
       const int2 kp = ktab[k];
       const PieceAddr pa = prow[kp.x];
-      Atab[k] = pa.rowbase + (long long)kp.y * pa.stride;
+      Atab[k] = pa.rowbase + (dsplit ? (long long)kp.y : (long long)kp.y * pa.stride);
     }
   }
   mr_stages_upto<R, N, false, 1, G::NST>(b0, b1, W);
@@ -150,7 +160,7 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
   const C* __restrict__ chirp = reinterpret_cast<const C*>(A.bs_chirp);
   const R sc = R(A.scale);
   const int L = ta.lines;
-  const bool direct = A.dst_k_contig != 0;
+  const bool direct = A.dst_k_contig != 0;  // line-major order for both direct stores
   if constexpr (K == 1) {
     C* __restrict__ out = reinterpret_cast<C*>(A.out);
     for (int i = tid; i < G::NSEQ * m; i += MR_THREADS) {
@@ -164,7 +174,10 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
       }
       if (s >= L) continue;
       const C z = scl(cmul(Gr[s * G::SEQ + G::pad(k)], chirp[k]), sc);
-      out[direct ? ta.dst0 + (long long)s * ta.dstb + k : Atab[k] + s] = z;
+      const long long o = dsplit   ? Atab[k] + (long long)s * prow[ktab[k].x].stride
+                          : direct ? ta.dst0 + (long long)s * ta.dstb + k
+                                   : Atab[k] + s;
+      out[o] = z;
     }
   } else if (A.kind == P_C2R) {
     R* __restrict__ out = reinterpret_cast<R*>(A.out);
@@ -211,10 +224,11 @@ __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta
       if (post_weighted && k != 0 && 2 * k != m) f *= pf;
       const C v0 = mk<C, R>((a.x + b.x) * f, (a.y - b.y) * f);
       const C v1 = mk<C, R>((a.y + b.y) * f, (b.x - a.x) * f);
-      if (direct) {
-        const long long o = ta.dst0 + (long long)(2 * p) * ta.dstb + k;
+      if (direct) {  // the split direct store (R2C only) strides lines by the piece's stride
+        const long long ls = dsplit ? prow[ktab[k].x].stride : ta.dstb;
+        const long long o = dsplit ? Atab[k] + (long long)(2 * p) * ls : ta.dst0 + (long long)(2 * p) * ls + k;
         out[o] = v0;
-        if (2 * p + 1 < L) out[o + ta.dstb] = v1;
+        if (2 * p + 1 < L) out[o + ls] = v1;
       } else {
         const long long o = Atab[k] + 2 * p;
         out[o] = v0;
@@ -232,33 +246,36 @@ __host__ __device__ constexpr int mr_bs_min_ctas(int real_bytes, int N) {
   return (real_bytes == 4 && N <= 640 && N != 192 && N != 224) ? 3 : 2;
 }
 
-template <typename R, int N, int K>
+// V, the source and store layout (the mixed-radix kernel's variants):
+// 0 contiguous lines, direct or transposed store; 1 strided lines, any store;
+// 2 contiguous lines, split direct store.
+template <typename R, int N, int K, int V>
 __global__ void __launch_bounds__(MR_THREADS, mr_bs_min_ctas((int)sizeof(R), N)) mr_bs_kernel(const PassArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (A.gate != nullptr && *A.gate != 0) return;
-  mr_run<R, N, false, false, false, 0, K>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
+  mr_run<R, N, false, V == 1, V != 0, 0, K>(A, blockIdx.x, gridDim.x, A.ntiles, smem, true);
 }
 
-template <typename R, int N, int K>
+template <typename R, int N, int K, int V>
 cudaError_t mr_bs_launch(const PassArgs& A, cudaStream_t stream) {
   constexpr size_t smem = mr_smem_bytes<R, N>();
   cudaError_t err =
-      cudaFuncSetAttribute(mr_bs_kernel<R, N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(mr_bs_kernel<R, N, K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   long long grid = A.grid_ctas > 0 ? A.grid_ctas : A.ntiles;
   if (grid > A.ntiles) grid = A.ntiles;
-  mr_bs_kernel<R, N, K><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
+  mr_bs_kernel<R, N, K, V><<<dim3((unsigned)grid), MR_THREADS, smem, stream>>>(A);
   return cudaGetLastError();
 }
 
-template <typename R, int N, int K>
+template <typename R, int N, int K, int V>
 int mr_bs_occ() {
   constexpr size_t smem = mr_smem_bytes<R, N>();
   int blocks = 0;
-  if (cudaFuncSetAttribute(mr_bs_kernel<R, N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+  if (cudaFuncSetAttribute(mr_bs_kernel<R, N, K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_bs_kernel<R, N, K>, MR_THREADS, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mr_bs_kernel<R, N, K, V>, MR_THREADS, smem) !=
       cudaSuccess)
     return 1;
   return blocks > 0 ? blocks : 1;

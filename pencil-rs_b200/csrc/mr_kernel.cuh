@@ -661,11 +661,12 @@ __device__ __forceinline__ void mr_tile_r2r(const PassArgs& A, const TileAddr& t
 
 // Bluestein lengths (mr_bs.cuh): the chirp-premultiplied load and the
 // convolution tile of a Bluestein pass with an N-point (7-smooth) convolution;
-// K 1 for C2C, 2 for R2C / C2R.
-template <typename R, int N, int K>
+// K 1 for C2C, 2 for R2C / C2R; SX strided source lines; DS the split direct
+// store compiled in.
+template <typename R, int N, int K, bool SX>
 __device__ __forceinline__ void mr_load_bs(typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            const PassArgs& A, const TileAddr& ta);
-template <typename R, int N, int K>
+template <typename R, int N, int K, bool SX, bool DS>
 __device__ __forceinline__ void mr_tile_bs(const PassArgs& A, const TileAddr& ta,
                                            typename Cx<R>::T (&v)[MRGeom<R, N>::U0][MRGeom<R, N>::R0],
                                            typename Cx<R>::T* b0, typename Cx<R>::T* b1, const typename Cx<R>::T* W,
@@ -676,7 +677,7 @@ template <typename R, int N, bool R2R = false, bool SX = false, bool DS = false,
 __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long long step, long long end,
                                        unsigned char* smem, bool setup) {
   static_assert(!R2R || S == 0, "the real-to-real kinds run the default schedule");
-  static_assert(BS == 0 || (!R2R && !SX && !DS && S == 0), "Bluestein passes: contiguous lines");
+  static_assert(BS == 0 || (!R2R && S == 0), "Bluestein passes: the default schedule");
   using C = typename Cx<R>::T;
   using G = MRGeom<R, N, S>;
   constexpr int BUF = G::NSEQ * G::SEQ;
@@ -704,7 +705,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
   TileAddr ta = load_tile(tiles, tile);
   C v[G::U0][G::R0];
   if constexpr (BS != 0)
-    mr_load_bs<R, N, BS>(v, A, ta);
+    mr_load_bs<R, N, BS, SX>(v, A, ta);
   else if constexpr (R2R)
     mr_load_r2r<R, N, SX>(v, A, ta);
   else
@@ -722,7 +723,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
     C nv[G::U0][G::R0];
     if (has_next) {
       if constexpr (BS != 0)
-        mr_load_bs<R, N, BS>(nv, A, t1);
+        mr_load_bs<R, N, BS, SX>(nv, A, t1);
       else if constexpr (R2R)
         mr_load_r2r<R, N, SX>(nv, A, t1);
       else
@@ -731,7 +732,7 @@ __device__ __forceinline__ void mr_run(const PassArgs& A, long long first, long 
       if (tid < npieces) next_piece = pieces[(tile + step) * npieces + tid];
     }
     if constexpr (BS != 0) {
-      mr_tile_bs<R, N, BS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
+      mr_tile_bs<R, N, BS, SX, DS>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);
     } else if constexpr (R2R) {
       if (A.inv)
         mr_tile_r2r<R, N, true, SX>(A, ta, v, b0, b1, W, Atab, ktab, prow, my_piece, npieces);

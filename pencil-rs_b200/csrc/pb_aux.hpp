@@ -119,26 +119,47 @@ bool mr_r2r_supported(int m, int real_bytes);
 cudaError_t launch_mr_r2r(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int mr_r2r_lines(int m, int complex_data, int real_bytes);
 int mr_r2r_occupancy(int m, int real_bytes);
-// Bluestein C2C / R2C / C2R passes on the mixed-radix kernel (mr_bs.cuh):
+// Bluestein C2C / R2C / C2R passes on the mixed-radix kernel (mr_bs.cuh),
+// contiguous or strided source lines:
 // convolution length M = A.bs_m2 one of kBluesteinLengths; mr_bs_lines gives
 // the sequences per tile (lines for C2C, line pairs for the real kinds)
 bool mr_bs_supported(int M, int real_bytes);
 cudaError_t launch_mr_bs(const PassArgs& A, int real_bytes, cudaStream_t stream);
 int mr_bs_lines(int M, int real_bytes);
-int mr_bs_occupancy(int M, int kind, int real_bytes);
-// the same per kernel kind K (1 C2C, 2 R2C / C2R), one object file each
-template <int K>
+int mr_bs_occupancy(int M, int kind, int variant, int real_bytes);
+// the layout variant of a Bluestein pass: 0 contiguous lines, 1 strided
+// lines, 2 contiguous lines with a split direct store
+inline int mr_bs_variant(const PassArgs& A) { return A.src_k_contig == 0 ? 1 : (A.dst_k_contig == 2 ? 2 : 0); }
+// the same per kernel kind K (1 C2C, 2 R2C / C2R) and layout variant V, one
+// object file each
+template <int K, int V>
 cudaError_t launch_mr_bs_kind(const PassArgs& A, int real_bytes, cudaStream_t stream);
-template <int K>
+template <int K, int V>
 int mr_bs_kind_occupancy(int M, int real_bytes);
 template <>
-cudaError_t launch_mr_bs_kind<1>(const PassArgs& A, int real_bytes, cudaStream_t stream);
+cudaError_t launch_mr_bs_kind<1, 0>(const PassArgs& A, int real_bytes, cudaStream_t stream);
 template <>
-cudaError_t launch_mr_bs_kind<2>(const PassArgs& A, int real_bytes, cudaStream_t stream);
+cudaError_t launch_mr_bs_kind<1, 1>(const PassArgs& A, int real_bytes, cudaStream_t stream);
 template <>
-int mr_bs_kind_occupancy<1>(int M, int real_bytes);
+cudaError_t launch_mr_bs_kind<1, 2>(const PassArgs& A, int real_bytes, cudaStream_t stream);
 template <>
-int mr_bs_kind_occupancy<2>(int M, int real_bytes);
+cudaError_t launch_mr_bs_kind<2, 0>(const PassArgs& A, int real_bytes, cudaStream_t stream);
+template <>
+cudaError_t launch_mr_bs_kind<2, 1>(const PassArgs& A, int real_bytes, cudaStream_t stream);
+template <>
+cudaError_t launch_mr_bs_kind<2, 2>(const PassArgs& A, int real_bytes, cudaStream_t stream);
+template <>
+int mr_bs_kind_occupancy<1, 0>(int M, int real_bytes);
+template <>
+int mr_bs_kind_occupancy<1, 1>(int M, int real_bytes);
+template <>
+int mr_bs_kind_occupancy<1, 2>(int M, int real_bytes);
+template <>
+int mr_bs_kind_occupancy<2, 0>(int M, int real_bytes);
+template <>
+int mr_bs_kind_occupancy<2, 1>(int M, int real_bytes);
+template <>
+int mr_bs_kind_occupancy<2, 2>(int M, int real_bytes);
 // mixed-radix pass kernel (mr_kernel.cuh) for the lengths of mr_lengths.hpp
 bool mr_supported(int m, int real_bytes);
 cudaError_t launch_mr(const PassArgs& A, int real_bytes, cudaStream_t stream);

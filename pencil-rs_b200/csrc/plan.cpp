@@ -1123,7 +1123,7 @@ static void build_fast_tables(pb_plan& P, PassArgs& A, const Pencil& src, const 
   if (A.fast && !P.force_generic) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int occ = A.fast == 4   ? mr_bs_occupancy(A.bs_m2, A.kind, P.real_bytes)
+    const int occ = A.fast == 4   ? mr_bs_occupancy(A.bs_m2, A.kind, mr_bs_variant(A), P.real_bytes)
                     : A.fast == 3 ? mr_r2r_occupancy(A.m, P.real_bytes)
                     : A.fast == 2 ? mr_occupancy(A.m, P.real_bytes)
                     : A.half      ? pow2_half_occupancy(A.m, A.kind)
@@ -1280,15 +1280,18 @@ static Step make_pass(pb_plan& P, const Stage& st, const LocalOp& op, const Penc
   }
   // Bluestein lengths (a prime factor above 31) of C2C / R2C / C2R passes on
   // the mixed-radix kernel: the convolution's two FFTs in registers and
-  // shared memory; contiguous source lines, direct or transposed store
+  // shared memory; the mixed-radix kernel's layouts (contiguous or strided
+  // source lines, direct, transposed or, for C2C and R2C, split direct store)
   if (!A.fast && !P.force_generic && (op.kind == P_C2C || op.kind == P_R2C || op.kind == P_C2R) && A.bs_m2 &&
-      mr_bs_supported(A.bs_m2, P.real_bytes) && src.perm[N - 1] == a && src.split_of(a) < 0) {
+      mr_bs_supported(A.bs_m2, P.real_bytes) && (src.perm[N - 1] == a || src_strided) && src.split_of(a) < 0) {
     const bool direct = dst.perm[N - 1] == a && dst.split_of(a) < 0;
     const int ta = dst.split_of(a);
     const bool transposed = !direct && dst.perm[N - 1] == b && (ta < 0 || dst.grid[ta] <= 64);
-    if (direct || transposed) {
+    const bool dsplit = !direct && dst.perm[N - 1] == a && ta >= 0 && dst.grid[ta] <= 64 &&
+                        (op.kind == P_C2C || op.kind == P_R2C);
+    if (direct || transposed || dsplit) {
       A.fast = 4;
-      A.dst_k_contig = direct ? 1 : 0;
+      A.dst_k_contig = direct ? 1 : (dsplit ? 2 : 0);
       L = mr_bs_lines(A.bs_m2, P.real_bytes) * (op.kind == P_C2C ? 1 : 2);  // real kinds: two lines per sequence
       A.lines = L;
     }
@@ -4304,7 +4307,7 @@ static std::string reg_key(const PassArgs& A, int real_bytes) {
 }
 
 static int reg_occupancy(const PassArgs& A, int real_bytes, int sched) {
-  return A.fast == 4   ? mr_bs_occupancy(A.bs_m2, A.kind, real_bytes)
+  return A.fast == 4   ? mr_bs_occupancy(A.bs_m2, A.kind, mr_bs_variant(A), real_bytes)
          : A.fast == 3 ? mr_r2r_occupancy(A.m, real_bytes)
          : A.fast == 2 ? mr_occupancy(A.m, real_bytes, sched)
          : A.half      ? pow2_half_occupancy(A.m, A.kind)

@@ -22,14 +22,15 @@ LIB = os.path.join(PKG, "libpencil_b200.so")
 
 # (source, object, preprocessor definitions): mr_kernels.cu is compiled once
 # per group of lengths (MR_GROUPS in mr_lengths.hpp) and mr_bs_kernels.cu once
-# per kernel kind, so the groups build in parallel
+# per kernel kind and layout variant, so the groups build in parallel
 MR_GROUPS = 8
 # the longest compilations first, so that a full build keeps every core busy
 # to the end
 SOURCES = ([("pass_kernel.cu", "pass_kernel.cu.o", [])]
            + [("mr_kernels.cu", f"mr_kernels_g{g}.o", [f"-DMR_GROUP={g}"]) for g in range(MR_GROUPS)]
            + [("mr_r2r_kernels.cu", f"mr_r2r_kernels_g{g}.o", [f"-DMR_GROUP={g}"]) for g in range(MR_GROUPS)]
-           + [("mr_bs_kernels.cu", f"mr_bs_kernels_k{k}.o", [f"-DBS_KIND={k}"]) for k in (1, 2)]
+           + [("mr_bs_kernels.cu", f"mr_bs_kernels_k{k}v{v}.o", [f"-DBS_KIND={k}", f"-DBS_V={v}"])
+              for k in (1, 2) for v in (0, 1, 2)]
            + [(s, s + ".o", []) for s in ("pow2_kernel.cu", "plan.cpp", "field_ops.cu", "aux_kernels.cu",
                                          "no_alloc.cu", "mr_dispatch.cpp")])
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

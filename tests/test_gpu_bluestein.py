@@ -1,8 +1,8 @@
 """Lengths with a prime factor above 31 run Bluestein's chirp-z form (the
 m-point DFT as a cyclic convolution over a 7-smooth FFT) instead of an O(p)
-radix: C2C, R2C and C2R passes over contiguous lines on the mixed-radix
-kernel ("bluestein", convolution lengths up to 1024), everything else in the
-generic kernel's FFT core -- strided lines, longer lines and the real-to-real
+radix: C2C, R2C and C2R passes over contiguous or strided lines on the
+mixed-radix kernel ("bluestein", convolution lengths up to 1024), everything
+else in the generic kernel's FFT core -- longer lines and the real-to-real
 kinds whose FFT length has such a factor (DCT-II of 101, DST-I of 100 -> 202 =
 2 * 101, DHT of 67, DCT-IV of 94 -> 47).  f32 and f64, against the oracle's
 float64 DFT within the usual bound."""
@@ -44,34 +44,38 @@ def _bluestein_steps(plan, op, kernels=("generic", "bluestein")):
 @pytest.mark.parametrize("rb", [4, 8])
 @pytest.mark.parametrize("dims,shape", C2C_CASES)
 def test_c2c_prime_lengths(rb, dims, shape, permute):
-    """permute_dims = true: the contiguous C2C passes take the mixed-radix
-    Bluestein kernel (up to 512 points; 1021 needs a 2048-point convolution
-    and stays on the generic kernel); false: strided lines, the generic
-    kernel's Bluestein core."""
+    """Both layouts (permute_dims = false: strided lines) take the mixed-radix
+    Bluestein kernel up to 512 points; 1021 needs a 2048-point convolution and
+    514 = 2 * 257 a 1027-point one, which stay on the generic kernel."""
     rng = np.random.default_rng(31)
     lay = pb.DistributedLayout(permute)
     plan = pb.C2cPlan.from_shape(pb.MpiTopology(dims), shape, (), layout=lay, dtype=CDT[rb])
     assert _bluestein_steps(plan, L.FORWARD), plan.step_configs(L.FORWARD)
-    if permute and max(shape) <= 512:
+    if max(shape) <= 512:
         for op in (L.FORWARD, L.INVERSE):
-            assert _bluestein_steps(plan, op, ("bluestein",)), plan.step_configs(op)
+            assert _bluestein_steps(plan, op) == _bluestein_steps(plan, op, ("bluestein",)), plan.step_configs(op)
     route = po.c2c_route(po.Topology(dims), shape, None, permute)
     x = rand_field(rng, shape, (), True, rb)
     for d in ("fwd", "inv", "bwd"):
         check_transform(plan, route, x, 1, rb, True, d)
 
 
+@pytest.mark.parametrize("permute", [True, False])
 @pytest.mark.parametrize("rb", [4, 8])
-@pytest.mark.parametrize("dims,shape,extra", [((2, 2), (10, 12, 127), ()), ((2, 3), (53, 9, 8), (2,))])
-def test_r2c_prime_lengths(rb, dims, shape, extra):
+@pytest.mark.parametrize("dims,shape,extra", [((2, 2), (10, 12, 127), ()), ((2, 3), (53, 9, 8), (2,)),
+                                              ((2, 2), (37, 41, 20), ())])
+def test_r2c_prime_lengths(rb, dims, shape, extra, permute):
+    """R2C forward and the C2R inverse / backward; permute_dims = false
+    leaves the C2C passes (and the C2R extension) on strided lines."""
     rng = np.random.default_rng(32)
     e = int(np.prod(extra)) if extra else 1
-    plan = pb.R2cPlan.from_shape(pb.MpiTopology(dims), shape, extra, dtype=RDT[rb])
+    plan = pb.R2cPlan.from_shape(pb.MpiTopology(dims), shape, extra, layout=pb.DistributedLayout(permute),
+                                 dtype=RDT[rb])
     assert _bluestein_steps(plan, L.FORWARD) and _bluestein_steps(plan, L.INVERSE)
-    # every Bluestein pass of these routes has contiguous lines: the mixed-radix kernel
+    # every Bluestein pass of these routes (contiguous or strided lines) runs on the mixed-radix kernel
     for op in (L.FORWARD, L.INVERSE):
         assert _bluestein_steps(plan, op) == _bluestein_steps(plan, op, ("bluestein",)), plan.step_configs(op)
-    route = po.r2c_route(po.Topology(dims), shape)
+    route = po.r2c_route(po.Topology(dims), shape, None, permute)
     x = rand_field(rng, shape, extra, False, rb)
     check_transform(plan, route, x, e, rb, False, "fwd")
     spec = po.gather(oracle_pencil(plan.output_pencil),
