@@ -36,10 +36,23 @@ __host__ __device__ constexpr bool mr_two_cta_length(int N) {
   return false;
 }
 
+// Lengths above 512 whose default-schedule f32 kernel fits 80 registers, so
+// three CTAs per SM, without spilling (the strided and split-store variants
+// spill at most 16 bytes); the other long lengths spill 40-650 bytes there.
+constexpr int kMrThreeCtaLongLengths[] = {525, 540, 567, 576};
+
+__host__ __device__ constexpr bool mr_three_cta_long_length(int N) {
+  for (int n : kMrThreeCtaLongLengths)
+    if (n == N) return true;
+  return false;
+}
+
 // CTAs per SM of the mixed-radix kernel for precision `real_bytes`, length N
 // and schedule S (1: radices up to 8, fewer registers per butterfly).
 __host__ __device__ constexpr int mr_min_ctas(int real_bytes, int N, int S) {
-  return (real_bytes != 4 || N > 512) ? 2 : (S == 1 ? 3 : (mr_two_cta_length(N) ? 2 : 3));
+  return real_bytes != 4 ? 2
+         : N > 512       ? ((S == 0 && mr_three_cta_long_length(N)) ? 3 : 2)
+                         : (S == 1 ? 3 : (mr_two_cta_length(N) ? 2 : 3));
 }
 
 // The same for the real-to-real kinds (default schedule only).  The 770-point
