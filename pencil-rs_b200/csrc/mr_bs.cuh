@@ -1,6 +1,7 @@
 // Bluestein passes on the mixed-radix kernel: C2C, R2C and C2R lines whose FFT
-// length m has a prime factor above 31, contiguous in the source, direct or
-// transposed store (the real kinds two lines per complex sequence, as x + iy).
+// length m has a prime factor above 31, in the mixed-radix kernel's layouts
+// (contiguous or strided source lines; direct, transposed or, for C2C and R2C,
+// split direct store); the real kinds two lines per complex sequence, as x + iy.
 // The m-point DFT is X_k = w_k * sum_j (x_j w_j) conj(w)_{k-j} with
 // w_j = exp(-+i pi j^2 / m) (the pass's sign, A.bs_chirp); the sum is a cyclic
 // convolution of length N = A.bs_m2 (the smallest of kBluesteinLengths
@@ -14,7 +15,7 @@
 //   * the post-chirp and the store (C2C outputs k < m, C2R the two real
 //     lines, R2C the split half spectra of the pair).
 // The generic kernel's FFT core (pass_kernel.cu, fft_run) computes the same
-// convolution for the other kinds and layouts.
+// convolution for the real-to-real kinds and for longer lines.
 #pragma once
 
 #include "mr_kernel.cuh"
